@@ -1,0 +1,595 @@
+// Krylov solvers as persistent cooperative kernels.
+//
+// The reference calls PETSc (KSPBCGS + PCSOR, src/Math/SparseMatrix.cpp:86-106) once
+// per system, from a zero initial guess, and returns the iteration count.  PETSc's
+// lexicographic SOR sweep is sequential, so the device solvers use Jacobi
+// preconditioning (BASELINE's plain FP64 GPU path) with the published algorithms:
+//   * BiCGStab (van der Vorst 1992), right-preconditioned, for the momentum system
+//     (three right-hand sides sharing one operator sweep) and for non-symmetric
+//     pressure-correction systems (immersed-boundary ghost rows);
+//   * CG (Hestenes-Stiefel), for the symmetric pressure-correction system.
+// Every solve is one kernel launch: all blocks stay resident (cooperative launch) and
+// meet at grid barriers between the phases of an iteration; the dot products are summed
+// per block and then, in every block, over the block partials in a fixed order, so all
+// blocks take the same convergence decision and the result is bit-reproducible.  The
+// loop ends on the true residual ||b - A x|| <= rtol ||b|| (checked when the recursive
+// residual meets it; the iteration restarts from the true residual otherwise) or at
+// maxit, so no launch can run unbounded.
+//
+// Neighbour values written earlier in the same launch by other blocks are read with
+// ld.global.cg (L2 only), never through the incoherent L1.  Vectors that can be formed
+// from others are not stored: CG's search direction p = z + beta p_old and BiCGStab's
+// p = r + beta (p_old - omega v) and s = r - alpha v are recomputed at the stencil
+// neighbours instead of costing an extra pass and barrier.
+#include <cooperative_groups.h>
+#include "krylov.cuh"
+
+namespace cg = cooperative_groups;
+
+namespace cb {
+
+constexpr int KB = 256;   // threads per block
+constexpr int KP = 8;     // partial slots per block
+
+__device__ __forceinline__ double ldcg(const double* p) { return __ldcg(p); }
+
+template <int K>
+__device__ __forceinline__ void warp_sum(double (&v)[K]) {
+#pragma unroll
+    for (int q = 0; q < K; ++q)
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) v[q] += __shfl_xor_sync(0xffffffffu, v[q], off);
+}
+
+// block sums of v[0..K) into partials[blockIdx.x*KP + q]
+template <int K>
+__device__ void block_partials(double (&v)[K], double* partials) {
+    __shared__ double sm[KP][32];
+    warp_sum(v);
+    int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    if (lane == 0)
+#pragma unroll
+        for (int q = 0; q < K; ++q) sm[q][w] = v[q];
+    __syncthreads();
+    if (w == 0) {
+        double t[K];
+#pragma unroll
+        for (int q = 0; q < K; ++q) t[q] = lane < nw ? sm[q][lane] : 0.;
+        warp_sum(t);
+        if (lane == 0)
+#pragma unroll
+            for (int q = 0; q < K; ++q) partials[blockIdx.x * KP + q] = t[q];
+    }
+    __syncthreads();
+}
+
+// sum of all blocks' partials, computed identically in every block
+template <int K>
+__device__ void grid_totals(const double* partials, double (&out)[K]) {
+    __shared__ double sm[KP][32];
+    double v[K];
+#pragma unroll
+    for (int q = 0; q < K; ++q) v[q] = 0.;
+    for (int g = threadIdx.x; g < (int)gridDim.x; g += blockDim.x)
+#pragma unroll
+        for (int q = 0; q < K; ++q) v[q] += ldcg(partials + (long long)g * KP + q);
+    warp_sum(v);
+    int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    if (lane == 0)
+#pragma unroll
+        for (int q = 0; q < K; ++q) sm[q][w] = v[q];
+    __syncthreads();
+    if (w == 0) {
+        double t[K];
+#pragma unroll
+        for (int q = 0; q < K; ++q) t[q] = lane < nw ? sm[q][lane] : 0.;
+        warp_sum(t);
+        __syncwarp();
+        if (lane == 0)
+#pragma unroll
+            for (int q = 0; q < K; ++q) sm[q][0] = t[q];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < K; ++q) out[q] = sm[q][0];
+    __syncthreads();
+}
+
+// Block partials, grid barrier, totals.  Partials alternate between two buffers: a block
+// that races ahead to the next reduction cannot overwrite a slot another block is still
+// summing, because it must first pass the barrier of the reduction in between.
+template <int K>
+__device__ __forceinline__ void grid_reduce(cg::grid_group& grid, double (&v)[K], double* partials, int& parity, double (&out)[K]) {
+    double* buf = partials + (long long)(parity & 1) * gridDim.x * KP;
+    block_partials<K>(v, buf);
+    grid.sync();
+    grid_totals<K>(buf, out);
+    ++parity;
+}
+
+// ------------------------------------------------------------------ operators
+__device__ __forceinline__ int ghost_index(const GhostRows& gh, long long c) {
+    int lo = 0, hi = gh.n;
+    while (lo < hi) {
+        int mid = (lo + hi) >> 1;
+        if (__ldg(gh.cell + mid) < c) lo = mid + 1; else hi = mid;
+    }
+    return lo;
+}
+
+template <int NR, class X>
+__device__ __forceinline__ void ghost_fix(const GhostRows& gh, long long c, X&& x, double (&y)[NR]) {
+    uint32_t w = __ldg(gh.bits + (c >> 5));
+    if ((w >> (c & 31)) & 1u) {
+        int g = ghost_index(gh, c);
+#pragma unroll
+        for (int q = 0; q < NR; ++q) {
+            double s = 0.;
+            for (int m = 0; m < 9; ++m) {
+                int col = __ldg(gh.col + 9 * g + m);
+                if (col >= 0) s += __ldg(gh.val + 9 * g + m) * x(q, (long long)col);
+            }
+            y[q] = s;
+        }
+    }
+}
+
+template <int NR, class X>
+__device__ __forceinline__ void apply(const Op7& A, long long c, X&& x, double (&y)[NR]) {
+    double aP = __ldg(A.a[0] + c), aE = __ldg(A.a[1] + c), aW = __ldg(A.a[2] + c), aN = __ldg(A.a[3] + c);
+    double aS = __ldg(A.a[4] + c), aT = __ldg(A.a[5] + c), aB = __ldg(A.a[6] + c);
+#pragma unroll
+    for (int q = 0; q < NR; ++q)
+        y[q] = aP * x(q, c) + aE * x(q, c + 1) + aW * x(q, c - 1) + aN * x(q, c + A.nI) + aS * x(q, c - A.nI)
+               + aT * x(q, c + A.nIJ) + aB * x(q, c - A.nIJ);
+    if (A.gh.n > 0) ghost_fix<NR>(A.gh, c, x, y);
+}
+
+template <int NR, class X>
+__device__ __forceinline__ void apply(const OpSym& A, long long c, X&& x, double (&y)[NR]) {
+    double aP = __ldg(A.aP + c), aE = __ldg(A.aE + c), aW = __ldg(A.aE + c - 1), aN = __ldg(A.aN + c);
+    double aS = __ldg(A.aN + c - A.nI), aT = __ldg(A.aT + c), aB = __ldg(A.aT + c - A.nIJ);
+#pragma unroll
+    for (int q = 0; q < NR; ++q)
+        y[q] = aP * x(q, c) + aE * x(q, c + 1) + aW * x(q, c - 1) + aN * x(q, c + A.nI) + aS * x(q, c - A.nI)
+               + aT * x(q, c + A.nIJ) + aB * x(q, c - A.nIJ);
+    if (A.gh.n > 0) ghost_fix<NR>(A.gh, c, x, y);
+}
+
+__device__ __forceinline__ double diag_of(const Op7& A, long long c) { return A.a[0][c]; }
+__device__ __forceinline__ double diag_of(const OpSym& A, long long c) { return A.aP[c]; }
+
+template <class Op>
+__global__ void inv_diag_kernel(Op A, long long N, double* invD) {
+    long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (c >= N) return;
+    double dg = diag_of(A, c);
+    invD[c] = dg != 0. ? 1. / dg : 1.;
+}
+
+struct KArgs {
+    const double* b;
+    double* x;
+    double* r;
+    double* rp;
+    double* p[2];
+    double* v[2];
+    double* t;
+    const double* invD;
+    double* partials;
+    KspOut* out;
+    long long N, PS;
+    double rtol;
+    int maxit;
+    int project;   // remove the mean of b first (singular all-Neumann pressure systems)
+};
+
+// Remove the mean of b (one plane), in place; every block computes the same mean.
+__device__ __forceinline__ void project_mean(cg::grid_group& grid, double* b, long long N, long long t0, long long T,
+                                             double* partials, int& par) {
+    double s[1] = {0.};
+    for (long long c = t0; c < N; c += T) s[0] += b[c];
+    double tot[1];
+    grid_reduce<1>(grid, s, partials, par, tot);
+    double mean = tot[0] / (double)N;
+    for (long long c = t0; c < N; c += T) b[c] = b[c] - mean;
+}
+
+// ------------------------------------------------------------------ BiCGStab
+template <int NR, class Op>
+__global__ void __launch_bounds__(KB) bicgstab_kernel(Op A, KArgs a) {
+    cg::grid_group grid = cg::this_grid();
+    const long long N = a.N, PS = a.PS;
+    const long long T = (long long)gridDim.x * blockDim.x;
+    const long long t0 = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const double* invD = a.invD;
+
+    double acc[2 * NR];
+    int par = 0;
+    if (NR == 1 && a.project) project_mean(grid, const_cast<double*>(a.b), N, t0, T, a.partials, par);
+    // ---- initial state: x = 0, r = rp = b
+#pragma unroll
+    for (int q = 0; q < NR; ++q) acc[q] = 0.;
+    for (long long c = t0; c < N; c += T) {
+#pragma unroll
+        for (int q = 0; q < NR; ++q) {
+            double bv = a.b[q * PS + c];
+            a.x[q * PS + c] = 0.;
+            a.r[q * PS + c] = bv;
+            a.rp[q * PS + c] = bv;
+            acc[q] += bv * bv;
+        }
+    }
+    double bb[NR];
+    {
+        double tmp[NR];
+#pragma unroll
+        for (int q = 0; q < NR; ++q) tmp[q] = acc[q];
+        grid_reduce<NR>(grid, tmp, a.partials, par, bb);
+    }
+
+    double rho[NR], rho_old[NR], alpha[NR], omega[NR], tol2[NR];
+    int it[NR], status[NR];
+    bool done[NR], fresh[NR], needT[NR];
+    double relres[NR];
+#pragma unroll
+    for (int q = 0; q < NR; ++q) {
+        done[q] = !(bb[q] > 0.);
+        if (bb[q] != bb[q]) status[q] = 3; else status[q] = 0;
+        rho[q] = bb[q]; rho_old[q] = 1.; alpha[q] = 1.; omega[q] = 1.;
+        tol2[q] = a.rtol * a.rtol * bb[q];
+        it[q] = 0; fresh[q] = true; needT[q] = false; relres[q] = 0.;
+    }
+    int cur = 0;
+    while (true) {
+        bool run[NR], any = false;
+#pragma unroll
+        for (int q = 0; q < NR; ++q) { run[q] = !done[q]; any |= run[q]; }
+        if (!any) break;
+        double beta[NR];
+#pragma unroll
+        for (int q = 0; q < NR; ++q) beta[q] = fresh[q] ? 0. : (rho[q] / rho_old[q]) * (alpha[q] / omega[q]);
+        const double* po = a.p[cur];
+        const double* vo = a.v[cur];
+        double* pn = a.p[cur ^ 1];
+        double* vn = a.v[cur ^ 1];
+        // ---- phase 1: p = r + beta (p_old - omega v_old);  v = A D^-1 p;  (rp, v)
+#pragma unroll
+        for (int q = 0; q < NR; ++q) acc[q] = 0.;
+        for (long long c = t0; c < N; c += T) {
+            auto pnew = [&](int q, long long e) -> double {
+                double rv = ldcg(a.r + q * PS + e);
+                if (fresh[q]) return rv;
+                return rv + beta[q] * (ldcg(po + q * PS + e) - omega[q] * ldcg(vo + q * PS + e));
+            };
+            double y[NR];
+            apply<NR>(A, c, [&](int q, long long e) { return __ldg(invD + e) * pnew(q, e); }, y);
+#pragma unroll
+            for (int q = 0; q < NR; ++q) {
+                if (!run[q]) continue;
+                double pc = pnew(q, c);
+                pn[q * PS + c] = pc;
+                vn[q * PS + c] = y[q];
+                double rpv;
+                if (fresh[q]) { rpv = ldcg(a.r + q * PS + c); a.rp[q * PS + c] = rpv; }
+                else rpv = a.rp[q * PS + c];
+                acc[q] += rpv * y[q];
+            }
+        }
+        double rv[NR];
+        {
+            double tmp[NR];
+#pragma unroll
+            for (int q = 0; q < NR; ++q) tmp[q] = acc[q];
+            grid_reduce<NR>(grid, tmp, a.partials, par, rv);
+        }
+#pragma unroll
+        for (int q = 0; q < NR; ++q) {
+            if (!run[q]) continue;
+            if (rv[q] == 0. || rv[q] != rv[q]) { needT[q] = true; run[q] = false; }
+            else alpha[q] = rho[q] / rv[q];
+        }
+        // ---- phase 2: s = r - alpha v;  t = A D^-1 s;  (t, s), (t, t)
+#pragma unroll
+        for (int q = 0; q < 2 * NR; ++q) acc[q] = 0.;
+        for (long long c = t0; c < N; c += T) {
+            double y[NR];
+            apply<NR>(A, c, [&](int q, long long e) {
+                return __ldg(invD + e) * (ldcg(a.r + q * PS + e) - alpha[q] * ldcg(vn + q * PS + e));
+            }, y);
+#pragma unroll
+            for (int q = 0; q < NR; ++q) {
+                if (!run[q]) continue;
+                double s = ldcg(a.r + q * PS + c) - alpha[q] * ldcg(vn + q * PS + c);
+                a.t[q * PS + c] = y[q];
+                acc[2 * q] += y[q] * s;
+                acc[2 * q + 1] += y[q] * y[q];
+            }
+        }
+        double tot[2 * NR];
+        {
+            double tmp[2 * NR];
+#pragma unroll
+            for (int q = 0; q < 2 * NR; ++q) tmp[q] = acc[q];
+            grid_reduce<2 * NR>(grid, tmp, a.partials, par, tot);
+        }
+#pragma unroll
+        for (int q = 0; q < NR; ++q) {
+            if (!run[q]) continue;
+            omega[q] = tot[2 * q + 1] == 0. ? 0. : tot[2 * q] / tot[2 * q + 1];
+        }
+        // ---- phase 3: x += alpha D^-1 p + omega D^-1 s;  r = s - omega t;  (r, rp), (r, r)
+#pragma unroll
+        for (int q = 0; q < 2 * NR; ++q) acc[q] = 0.;
+        for (long long c = t0; c < N; c += T) {
+            double id = __ldg(invD + c);
+#pragma unroll
+            for (int q = 0; q < NR; ++q) {
+                if (!run[q]) continue;
+                double s = ldcg(a.r + q * PS + c) - alpha[q] * ldcg(vn + q * PS + c);
+                double ph = id * ldcg(pn + q * PS + c);
+                double sh = id * s;
+                a.x[q * PS + c] = a.x[q * PS + c] + (alpha[q] * ph + omega[q] * sh);
+                double rn = s - omega[q] * ldcg(a.t + q * PS + c);
+                a.r[q * PS + c] = rn;
+                acc[2 * q] += rn * a.rp[q * PS + c];
+                acc[2 * q + 1] += rn * rn;
+            }
+        }
+        {
+            double tmp[2 * NR];
+#pragma unroll
+            for (int q = 0; q < 2 * NR; ++q) tmp[q] = acc[q];
+            grid_reduce<2 * NR>(grid, tmp, a.partials, par, tot);
+        }
+        bool anyT = false;
+#pragma unroll
+        for (int q = 0; q < NR; ++q) {
+            if (run[q]) {
+                it[q] += 1;
+                fresh[q] = false;
+                rho_old[q] = rho[q];
+                rho[q] = tot[2 * q];
+                double rr = tot[2 * q + 1];
+                if (rr <= tol2[q] || omega[q] == 0. || it[q] >= a.maxit || rr != rr) needT[q] = true;
+            }
+            anyT |= needT[q];
+        }
+        cur ^= 1;
+        if (anyT) {
+            // ---- true residual r = b - A x for the components being checked
+#pragma unroll
+            for (int q = 0; q < NR; ++q) acc[q] = 0.;
+            for (long long c = t0; c < N; c += T) {
+                double y[NR];
+                apply<NR>(A, c, [&](int q, long long e) { return ldcg(a.x + q * PS + e); }, y);
+#pragma unroll
+                for (int q = 0; q < NR; ++q) {
+                    if (!needT[q]) continue;
+                    double rt = a.b[q * PS + c] - y[q];
+                    a.r[q * PS + c] = rt;
+                    acc[q] += rt * rt;
+                }
+            }
+            double rrT[NR];
+            {
+                double tmp[NR];
+#pragma unroll
+                for (int q = 0; q < NR; ++q) tmp[q] = acc[q];
+                grid_reduce<NR>(grid, tmp, a.partials, par, rrT);
+            }
+#pragma unroll
+            for (int q = 0; q < NR; ++q) {
+                if (!needT[q]) continue;
+                needT[q] = false;
+                relres[q] = sqrt(rrT[q] / bb[q]);
+                if (rrT[q] <= tol2[q]) { done[q] = true; status[q] = 0; }
+                else if (rrT[q] != rrT[q]) { done[q] = true; status[q] = 3; }
+                else if (it[q] >= a.maxit) { done[q] = true; status[q] = 1; }
+                else { fresh[q] = true; rho[q] = rrT[q]; rho_old[q] = 1.; alpha[q] = 1.; omega[q] = 1.; }
+            }
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        for (int q = 0; q < NR; ++q) { a.out->iters[q] = it[q]; a.out->relres[q] = relres[q]; a.out->status[q] = status[q]; }
+    }
+}
+
+// ------------------------------------------------------------------ CG
+template <class Op>
+__global__ void __launch_bounds__(KB) cg_kernel(Op A, KArgs a) {
+    cg::grid_group grid = cg::this_grid();
+    const long long N = a.N;
+    const long long T = (long long)gridDim.x * blockDim.x;
+    const long long t0 = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const double* invD = a.invD;
+    double* z = a.rp;     // preconditioned residual
+    double* q = a.t;      // A p
+    int par = 0;
+    if (a.project) project_mean(grid, const_cast<double*>(a.b), N, t0, T, a.partials, par);
+    double acc[2];
+    acc[0] = acc[1] = 0.;
+    for (long long c = t0; c < N; c += T) {
+        double bv = a.b[c];
+        a.x[c] = 0.;
+        a.r[c] = bv;
+        double zv = __ldg(invD + c) * bv;
+        z[c] = zv;
+        acc[0] += bv * zv;
+        acc[1] += bv * bv;
+    }
+    double tot[2];
+    grid_reduce<2>(grid, acc, a.partials, par, tot);
+    double rz = tot[0], bb = tot[1];
+    double tol2 = a.rtol * a.rtol * bb;
+    int it = 0, status = 0;
+    double relres = 0.;
+    bool done = !(bb > 0.), fresh = true;
+    if (bb != bb) status = 3;
+    double beta = 0.;
+    int cur = 0;
+    while (!done) {
+        const double* po = a.p[cur];
+        double* pn = a.p[cur ^ 1];
+        // ---- phase 1: p = z + beta p_old;  q = A p;  (p, q)
+        double pq = 0.;
+        for (long long c = t0; c < N; c += T) {
+            auto pnew = [&](long long e) -> double {
+                double zv = ldcg(z + e);
+                return fresh ? zv : zv + beta * ldcg(po + e);
+            };
+            double y[1];
+            apply<1>(A, c, [&](int, long long e) { return pnew(e); }, y);
+            double pc = pnew(c);
+            pn[c] = pc;
+            q[c] = y[0];
+            pq += pc * y[0];
+        }
+        double t1[1];
+        {
+            double tmp[1] = {pq};
+            grid_reduce<1>(grid, tmp, a.partials, par, t1);
+        }
+        bool needT = false;
+        if (t1[0] == 0. || t1[0] != t1[0]) {
+            needT = true;
+        } else {
+            double alpha = rz / t1[0];
+            // ---- phase 2: x += alpha p;  r -= alpha q;  z = D^-1 r;  (r, z), (r, r)
+            acc[0] = acc[1] = 0.;
+            for (long long c = t0; c < N; c += T) {
+                double pc = ldcg(pn + c);
+                a.x[c] = a.x[c] + alpha * pc;
+                double rn = a.r[c] - alpha * ldcg(q + c);
+                a.r[c] = rn;
+                double zv = __ldg(invD + c) * rn;
+                z[c] = zv;
+                acc[0] += rn * zv;
+                acc[1] += rn * rn;
+            }
+            grid_reduce<2>(grid, acc, a.partials, par, tot);
+            it += 1;
+            fresh = false;
+            double rr = tot[1];
+            if (rr <= tol2 || it >= a.maxit || rr != rr) needT = true;
+            beta = tot[0] / rz;
+            rz = tot[0];
+            cur ^= 1;
+        }
+        if (needT) {
+            // ---- true residual r = b - A x, z = D^-1 r
+            acc[0] = acc[1] = 0.;
+            for (long long c = t0; c < N; c += T) {
+                double y[1];
+                apply<1>(A, c, [&](int, long long e) { return ldcg(a.x + e); }, y);
+                double rt = a.b[c] - y[0];
+                a.r[c] = rt;
+                double zv = __ldg(invD + c) * rt;
+                z[c] = zv;
+                acc[0] += rt * zv;
+                acc[1] += rt * rt;
+            }
+            grid_reduce<2>(grid, acc, a.partials, par, tot);
+            relres = sqrt(tot[1] / bb);
+            if (tot[1] <= tol2) { done = true; status = 0; }
+            else if (tot[1] != tot[1]) { done = true; status = 3; }
+            else if (it >= a.maxit) { done = true; status = 1; }
+            else { fresh = true; rz = tot[0]; beta = 0.; }
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) { a.out->iters[0] = it; a.out->relres[0] = relres; a.out->status[0] = status; }
+}
+
+// ------------------------------------------------------------------ host side
+static int g_numSM = 0;
+
+static int sm_count() {
+    if (g_numSM == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&g_numSM, cudaDevAttrMultiProcessorCount, dev);
+    }
+    return g_numSM;
+}
+
+template <class K>
+static int coop_grid(K kernel) {
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, KB, 0) != cudaSuccess || nb < 1) nb = 1;
+    if (nb > 4) nb = 4;
+    return nb * sm_count();
+}
+
+template <class K>
+static int launch_coop(K kernel, int grid, KArgs& args, const void* op, cudaStream_t st) {
+    void* params[2] = {const_cast<void*>(op), &args};
+    CB_CUDA(cudaLaunchCooperativeKernel((const void*)kernel, dim3(grid), dim3(KB), params, 0, st));
+    return 0;
+}
+
+static KArgs make_args(const Lat& L, const KspWork& w, const double* b, double* x, double rtol, int maxit) {
+    KArgs a;
+    a.b = b; a.x = x; a.r = w.r; a.rp = w.rp;
+    a.p[0] = w.p[0]; a.p[1] = w.p[1]; a.v[0] = w.v[0]; a.v[1] = w.v[1];
+    a.t = w.t; a.invD = w.invD; a.partials = w.partials; a.out = w.out;
+    a.N = L.N; a.PS = L.PS; a.rtol = rtol; a.maxit = maxit;
+    a.project = 0;
+    return a;
+}
+
+int ksp_bicgstab(const Op7& A, int nr, const double* b, double* x, const Lat& L, const KspWork& w, double rtol, int maxit,
+                 cudaStream_t st) {
+    inv_diag_kernel<Op7><<<grid_for(L.N, 256), 256, 0, st>>>(A, L.N, w.invD);
+    CB_CHECK_LAUNCH();
+    KArgs a = make_args(L, w, b, x, rtol, maxit);
+    if (nr == 3) {
+        static int G = 0;
+        if (!G) G = coop_grid(bicgstab_kernel<3, Op7>);
+        return launch_coop(bicgstab_kernel<3, Op7>, G, a, &A, st);
+    }
+    static int G1 = 0;
+    if (!G1) G1 = coop_grid(bicgstab_kernel<1, Op7>);
+    return launch_coop(bicgstab_kernel<1, Op7>, G1, a, &A, st);
+}
+
+int ksp_bicgstab_sym(const OpSym& A, const double* b, double* x, const Lat& L, const KspWork& w, double rtol, int maxit,
+                     cudaStream_t st, int project) {
+    inv_diag_kernel<OpSym><<<grid_for(L.N, 256), 256, 0, st>>>(A, L.N, w.invD);
+    CB_CHECK_LAUNCH();
+    KArgs a = make_args(L, w, b, x, rtol, maxit);
+    a.project = project;
+    static int G = 0;
+    if (!G) G = coop_grid(bicgstab_kernel<1, OpSym>);
+    return launch_coop(bicgstab_kernel<1, OpSym>, G, a, &A, st);
+}
+
+int ksp_cg(const OpSym& A, const double* b, double* x, const Lat& L, const KspWork& w, double rtol, int maxit, cudaStream_t st,
+           int project) {
+    inv_diag_kernel<OpSym><<<grid_for(L.N, 256), 256, 0, st>>>(A, L.N, w.invD);
+    CB_CHECK_LAUNCH();
+    KArgs a = make_args(L, w, b, x, rtol, maxit);
+    a.project = project;
+    static int G = 0;
+    if (!G) G = coop_grid(cg_kernel<OpSym>);
+    return launch_coop(cg_kernel<OpSym>, G, a, &A, st);
+}
+
+int ksp_cg7(const Op7& A, const double* b, double* x, const Lat& L, const KspWork& w, double rtol, int maxit, cudaStream_t st) {
+    inv_diag_kernel<Op7><<<grid_for(L.N, 256), 256, 0, st>>>(A, L.N, w.invD);
+    CB_CHECK_LAUNCH();
+    KArgs a = make_args(L, w, b, x, rtol, maxit);
+    static int G = 0;
+    if (!G) G = coop_grid(cg_kernel<Op7>);
+    return launch_coop(cg_kernel<Op7>, G, a, &A, st);
+}
+
+int krylov_grid_size(int which) {
+    switch (which) {
+        case 0: return coop_grid(bicgstab_kernel<3, Op7>);
+        case 1: return coop_grid(bicgstab_kernel<1, OpSym>);
+        case 2: return coop_grid(cg_kernel<OpSym>);
+        default: return coop_grid(bicgstab_kernel<1, Op7>);
+    }
+}
+
+}  // namespace cb

@@ -1,0 +1,77 @@
+// Krylov solvers on the device: operators, workspace and launchers.
+#pragma once
+#include "common.cuh"
+
+namespace cb {
+
+// Immersed-boundary ghost rows in ELL-9 form, sorted by cell (IbPiso.cpp:119-190):
+// col[9g + 0] is the ghost cell itself, col[9g + 1..8] the interpolation stencil (-1 for a
+// dropped column), val[9g + m] the coefficients; bits marks ghost cells (one bit per cell).
+struct GhostRows {
+    int n;
+    const int* cell;
+    const int* col;
+    const double* val;
+    const uint32_t* bits;
+};
+
+// Non-symmetric 7-point operator: 7 per-cell coefficient arrays (momentum, Simple.cpp:162-171).
+struct Op7 {
+    const double* a[7];
+    long long nI, nIJ;
+    GhostRows gh;
+};
+
+// Symmetric 7-point operator: diagonal plus east/north/top coefficients per cell; the
+// west/south/bottom coefficient of a cell is the east/north/top one of that neighbour
+// (pressure correction, Simple.cpp:241-265).
+struct OpSym {
+    const double* aP;
+    const double* aE;
+    const double* aN;
+    const double* aT;
+    long long nI, nIJ;
+    GhostRows gh;
+};
+
+struct KspOut {
+    int iters[3];
+    double relres[3];
+    int status[3];      // 0 converged, 1 maxit, 2 breakdown, 3 non-finite
+};
+
+// Workspace for up to NR = 3 right-hand sides; every array is a halo-padded cell array of
+// 3 planes.
+struct KspWork {
+    double* r;
+    double* rp;
+    double* p[2];
+    double* v[2];
+    double* t;
+    double* invD;     // one plane
+    double* partials; // grid x 8 doubles
+    KspOut* out;      // device
+    // single precision copies for the mixed-precision inner solver
+    float* fr;
+    float* fp[2];
+    float* fq;
+    float* fz;
+    float* fx;
+    float* fA[4];     // aP aE aN aT
+    float* finvD;
+};
+
+int ksp_bicgstab(const Op7& A, int nr, const double* b, double* x, const Lat& L, const KspWork& w, double rtol, int maxit,
+                 cudaStream_t st);
+// project != 0: remove the mean of b first (b is modified), for singular all-Neumann systems
+int ksp_bicgstab_sym(const OpSym& A, const double* b, double* x, const Lat& L, const KspWork& w, double rtol, int maxit,
+                     cudaStream_t st, int project = 0);
+int ksp_cg(const OpSym& A, const double* b, double* x, const Lat& L, const KspWork& w, double rtol, int maxit, cudaStream_t st,
+           int project = 0);
+int ksp_cg7(const Op7& A, const double* b, double* x, const Lat& L, const KspWork& w, double rtol, int maxit, cudaStream_t st);
+// FP32 CG / BiCGStab inside FP64 iterative refinement on the symmetric operator.
+int ksp_mixed_sym(const OpSym& A, int method, const double* b, double* x, const Lat& L, const KspWork& w, double rtol, int maxit,
+                  double inner_rtol, cudaStream_t st, int* outer_iters);
+int krylov_grid_size(int which);
+
+}  // namespace cb

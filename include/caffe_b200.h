@@ -1,0 +1,136 @@
+/*
+ * caffe_b200.h -- C ABI of the B200 device library for CAFFE's finite-volume hot path.
+ *
+ * One handle holds one structured hexahedral mesh and the solver state of one
+ * Simple / Piso / IbPiso instance, resident in HBM, plus one CUDA stream on which
+ * every kernel of that handle runs.  All entry points return 0 on success and a
+ * non-zero status otherwise; caffe_last_error() gives the message of the last
+ * failure on the calling thread.  Plain pointers and sizes only: host arrays are
+ * float64, i-fastest (index (k*nJ + j)*nI + i), the layout of Array3D
+ * (src/DataStructures/Array3D.tpp:41-48 in the reference).
+ *
+ * Face order in every 6-array is east, west, north, south, top, bottom
+ * (HexaFvmMesh::Direction, src/Domains/HexaFvmMesh/HexaFvmMesh.h:44).
+ */
+#ifndef CAFFE_B200_H
+#define CAFFE_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Boundary types: FlowBoundaryConditions::Type (src/Domains/Field/FlowBoundaryConditions.h:10). */
+enum caffe_flow_bc { CAFFE_INLET = 0, CAFFE_OUTLET = 1, CAFFE_WALL = 2, CAFFE_EMPTY = 3, CAFFE_ZERO_GRADIENT = 4 };
+/* Solver classes: Simple (src/Solvers/Simple.h:33), Piso (Piso.h:6), IbPiso (IbPiso.h:33). */
+enum caffe_solver_kind { CAFFE_SIMPLE = 0, CAFFE_PISO = 1, CAFFE_IBPISO = 2 };
+/* Krylov methods.  The reference uses PETSc KSPBCGS + PCSOR (src/Math/SparseMatrix.cpp:95-100);
+ * the device implements BiCGStab and CG with Jacobi preconditioning. */
+enum caffe_ksp { CAFFE_KSP_BICGSTAB_SGS = 0, CAFFE_KSP_BICGSTAB_JACOBI = 1, CAFFE_KSP_CG_JACOBI = 2 };
+/* Form of the pressure-correction solve: plain FP64, FP32 inner solves inside FP64
+ * iterative refinement, learned preconditioner, or both. */
+enum caffe_p_form { CAFFE_P_FP64 = 0, CAFFE_P_MIXED = 1, CAFFE_P_LEARNED = 2, CAFFE_P_LEARNED_MIXED = 3 };
+
+/* Case parameters: the keys Simple / Piso / IbPiso read from case/case.info
+ * (Solver.cpp:8, Simple.cpp:61-67,104-108, Piso.cpp:9, FlowBoundaryConditions.cpp:25-40,
+ * IbPiso.cpp:37-38) plus the linear-solver settings the reference leaves to PETSc. */
+typedef struct caffe_case {
+    int kind;               /* caffe_solver_kind */
+    int bc_type[6];         /* caffe_flow_bc per face */
+    double ref_vec[6][3];   /* Boundaries.<face>.refVector */
+    double ref_val[6];      /* Boundaries.<face>.refValue */
+    double rho, mu;         /* Solver.rho, Solver.mu */
+    int time_accurate;      /* Solver.timeAccurate ON (1) / OFF (0) */
+    double omega_u, omega_p;/* Solver.relaxationFactorMomentum / relaxationFactorPCorr */
+    int n_inner, n_pcorr;   /* Solver.numberOfInnerIterations / numberOfPressureCorrections */
+    int convection;         /* 0 upwind (the reference), 1 volume-weighted central */
+    int nonorth;            /* 0 off (the reference), 1 non-orthogonal diffusion correction */
+    int mom_method, p_method;   /* caffe_ksp */
+    double mom_rtol, p_rtol;    /* relative true-residual tolerance ||b - Ax|| / ||b|| */
+    int maxit;
+    double ib_radius;       /* ImmersedBoundaries.Sphere.radius */
+    double ib_center[3];    /* ImmersedBoundaries.Sphere.center */
+    double u_init[3];       /* uniform initial u (InitialConditions, uniform) */
+    double p_init;          /* uniform initial p */
+    int p_form;             /* caffe_p_form */
+} caffe_case;
+
+/* Per-step statistics (what Simple::displayUpdateMessage prints, Simple.cpp:93-100, plus
+ * solver diagnostics). */
+typedef struct caffe_step_stats {
+    double continuity;      /* return value of Solver::solve: max continuity error */
+    double courant;         /* max Courant number (not computed by IbPiso) */
+    int mom_iters[3];       /* Krylov iterations of the last momentum solve, per component */
+    int p_iters_last;       /* iterations of the last pressure-correction solve */
+    int p_iters_total;      /* summed over all pressure-correction solves of the step */
+    int p_solves;
+    double p_res_max;       /* worst true relative residual of the step's p' solves */
+    double mom_res_max;     /* worst true relative residual of the step's momentum solves */
+    int status;             /* 0 ok; 1 a solve hit maxit; 2 breakdown; 3 non-finite residual */
+    int fallbacks;          /* p' solves that fell back to the plain FP64 method */
+    int n_ghost;            /* immersed-boundary ghost cells */
+    int n_rows;             /* unknowns per system (active + ghost cells) */
+    double p_ms, mom_ms, step_ms;   /* device time of the step's phases (CUDA events) */
+} caffe_step_stats;
+
+typedef struct caffe_dev caffe_dev;
+
+/* Last error message of the calling thread (empty when none). */
+const char* caffe_last_error(void);
+
+/* Build the device state: mesh metrics from the node array, fields, matrices and solver
+ * workspaces.  nodes: (nNodesK, nNodesJ, nNodesI, 3) float64 host array, i fastest.
+ * Replaces HexaFvmMesh::initialize (src/Domains/HexaFvmMesh/HexaFvmMesh.cpp:51-58,
+ * 615-624) followed by the Simple / Piso / IbPiso constructors (Simple.cpp:34-74,
+ * Piso.cpp:3-10, IbPiso.cpp:32-39).  device: CUDA ordinal to use. */
+int caffe_dev_create(const double* nodes, int nNodesI, int nNodesJ, int nNodesK,
+                     const caffe_case* cs, int device, caffe_dev** out);
+int caffe_dev_destroy(caffe_dev* h);
+
+/* One call of Solver::solve(timeStep) (src/Solvers/Solver.h:20): Simple::solve
+ * (Simple.cpp:78-91), Piso::solve (Piso.cpp:12-29) or IbPiso::solve (IbPiso.cpp:43-61).
+ * Asynchronous on the handle's stream unless stats != NULL, in which case it waits for
+ * the step and fills stats. */
+int caffe_dev_solve(caffe_dev* h, double dt, caffe_step_stats* stats);
+
+/* Run one named phase of the solver on the device (for tests and fine-grained callers):
+ * "save_u0", "assemble_momentum", "solve_momentum", "momentum_post" (BCs + face
+ * interpolation + Rhie-Chow), "assemble_pcorr", "solve_pcorr", "correct", "continuity",
+ * "courant", "ib_field", "ib_coeffs".  Names follow Simple.h:44-51 and IbPiso.h:46-47. */
+int caffe_dev_phase(caffe_dev* h, const char* name, double dt);
+
+/* Copy a named array between host and device (dir 0: device -> host, 1: host -> device),
+ * synchronously.  Returns the element count of the array in doubles (so a call with
+ * host == NULL queries the size), or -1 for an unknown name.  Names: "u", "p", "pCorr",
+ * "d", "h", "gradP", "gradPCorr", "massFlow", "massFlowI/J/K", "pPatch0".."pPatch5",
+ * metrics "vol", "cc", "SI/SJ/SK", "fcI/fcJ/fcK", "DI/DJ/DK", "momA" (7 x N), "momB" (N x 3),
+ * "pcA" (7 x N), "pcB", "status", ...  Vectors are N x 3 interleaved on the host.
+ * Field access of the reference: Field.h:53-61, HexaFvmMesh.h:66-142. */
+long caffe_dev_array(caffe_dev* h, const char* name, double* host, long count, int dir);
+
+/* Fill a copy of the last step's statistics without running anything. */
+int caffe_dev_stats(caffe_dev* h, caffe_step_stats* stats);
+
+/* The handle's CUDA stream (a cudaStream_t), so callers can order their own work and
+ * events with the solver's kernels. */
+void* caffe_dev_stream(caffe_dev* h);
+int caffe_dev_synchronize(caffe_dev* h);
+
+/* Stand-alone Krylov solve of a 7-point system on an nI x nJ x nK lattice: coef7 holds
+ * 7 host arrays of N = nI*nJ*nK doubles (aP, aE, aW, aN, aS, aT, aB; a coefficient whose
+ * neighbour lies outside the lattice must be zero), b and x are host arrays of N.
+ * x starts from zero.  Replaces SparseMatrix::solve (src/Math/SparseMatrix.cpp:86-106),
+ * which returns the iteration count. */
+int caffe_ksp7_solve(int nI, int nJ, int nK, const double* coef7, const double* b, double* x,
+                     int method, double rtol, int maxit, int* iters, double* rel_res);
+
+/* Device-pointer variant of caffe_ksp7_solve for callers that keep the system in HBM:
+ * d_coef7 (7*N), d_b, d_x are device pointers; stream is a cudaStream_t (NULL for the
+ * legacy default stream).  Workspace is allocated per call. */
+int caffe_ksp7_solve_device(int nI, int nJ, int nK, const double* d_coef7, const double* d_b, double* d_x,
+                            int method, double rtol, int maxit, void* stream, int* iters, double* rel_res);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CAFFE_B200_H */

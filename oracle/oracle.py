@@ -1,0 +1,228 @@
+"""TEST INFRASTRUCTURE ONLY -- ctypes binding of the CPU oracle (oracle.cpp).
+
+The oracle restates CAFFE's SIMPLE / PISO / IB-PISO hot path on the CPU; it is the
+checker of the CUDA library and the timed CPU baseline, never part of the product.
+Only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline / reference legs
+use this module.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "_build", "liboracle.so")
+_lib = None
+
+
+def build() -> str:
+    subprocess.run(["make", "-C", _HERE, "-s"], check=True)
+    return _LIB_PATH
+
+
+class OracleCase(ctypes.Structure):
+    _fields_ = [
+        ("kind", ctypes.c_int),
+        ("bc_type", ctypes.c_int * 6),
+        ("ref_vec", (ctypes.c_double * 3) * 6),
+        ("ref_val", ctypes.c_double * 6),
+        ("rho", ctypes.c_double), ("mu", ctypes.c_double),
+        ("time_accurate", ctypes.c_int),
+        ("omega_u", ctypes.c_double), ("omega_p", ctypes.c_double),
+        ("n_inner", ctypes.c_int), ("n_pcorr", ctypes.c_int),
+        ("convection", ctypes.c_int), ("nonorth", ctypes.c_int),
+        ("mom_method", ctypes.c_int), ("p_method", ctypes.c_int),
+        ("mom_rtol", ctypes.c_double), ("p_rtol", ctypes.c_double),
+        ("maxit", ctypes.c_int),
+        ("ib_radius", ctypes.c_double), ("ib_center", ctypes.c_double * 3),
+        ("u_init", ctypes.c_double * 3), ("p_init", ctypes.c_double),
+    ]
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        L = ctypes.CDLL(_LIB_PATH)
+        L.oracle_create.restype = ctypes.c_void_p
+        L.oracle_create.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(OracleCase)]
+        L.oracle_destroy.argtypes = [ctypes.c_void_p]
+        L.oracle_solve.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.POINTER(ctypes.c_double)]
+        L.oracle_phase.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_double]
+        L.oracle_stats.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        L.oracle_array.restype = ctypes.c_long
+        L.oracle_array.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_void_p, ctypes.c_long, ctypes.c_int]
+        L.oracle_last_error.restype = ctypes.c_char_p
+        L.oracle_ksp7.argtypes = [ctypes.c_int] * 3 + [ctypes.c_void_p] * 3 + [ctypes.c_int, ctypes.c_double, ctypes.c_int,
+                                                                              ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)]
+        L.oracle_hex_volume.restype = ctypes.c_double
+        L.oracle_hex_volume.argtypes = [ctypes.c_void_p]
+        L.oracle_quad_area.restype = ctypes.c_double
+        L.oracle_quad_area.argtypes = [ctypes.c_void_p]
+        L.oracle_hex_centroid.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        L.oracle_inside_hex.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        L.oracle_trilinear.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        L.oracle_nearest_intersect.argtypes = [ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        L.oracle_set_threads.argtypes = [ctypes.c_int]
+        L.oracle_get_threads.restype = ctypes.c_int
+        _lib = L
+    return _lib
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def make_case(spec) -> OracleCase:
+    from caffe_old_b200 import cases as C
+    spec.validate()
+    oc = OracleCase()
+    oc.kind = C.SOLVER_KINDS[spec.kind]
+    for f in range(6):
+        oc.bc_type[f] = C.FLOW_TYPES[spec.bc[f]]
+        for q in range(3):
+            oc.ref_vec[f][q] = float(spec.ref_vec[f][q])
+        oc.ref_val[f] = float(spec.ref_val[f])
+    oc.rho, oc.mu = float(spec.rho), float(spec.mu)
+    oc.time_accurate = 1 if spec.time_accurate else 0
+    oc.omega_u, oc.omega_p = float(spec.omega_u), float(spec.omega_p)
+    oc.n_inner, oc.n_pcorr = int(spec.n_inner), int(spec.n_pcorr)
+    oc.convection = C.CONVECTION[spec.convection]
+    oc.nonorth = 1 if spec.nonorth else 0
+    oc.mom_method = C.KSP_METHODS[spec.mom_method]
+    oc.p_method = C.KSP_METHODS[spec.p_method]
+    oc.mom_rtol, oc.p_rtol = float(spec.mom_rtol), float(spec.p_rtol)
+    oc.maxit = int(spec.maxit)
+    oc.ib_radius = float(spec.ib_radius)
+    for q in range(3):
+        oc.ib_center[q] = float(spec.ib_center[q])
+        oc.u_init[q] = float(spec.u_init[q])
+    oc.p_init = float(spec.p_init)
+    return oc
+
+
+def set_threads(n: int) -> None:
+    lib().oracle_set_threads(int(n))
+
+
+def get_threads() -> int:
+    return int(lib().oracle_get_threads())
+
+
+class OracleSolver:
+    """CPU restatement of Simple / Piso / IbPiso (src/Solvers/*.cpp) on one block."""
+
+    def __init__(self, nodes: np.ndarray, spec):
+        L = lib()
+        nodes = np.ascontiguousarray(nodes, dtype=np.float64)
+        nK1, nJ1, nI1, _ = nodes.shape
+        self.shape = (nI1 - 1, nJ1 - 1, nK1 - 1)
+        self.ncells = self.shape[0] * self.shape[1] * self.shape[2]
+        self._case = make_case(spec)
+        self.spec = spec
+        h = L.oracle_create(_ptr(nodes), nI1, nJ1, nK1, ctypes.byref(self._case))
+        if not h:
+            raise RuntimeError("oracle_create failed: " + L.oracle_last_error().decode())
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().oracle_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def solve(self, dt: float | None = None) -> float:
+        out = ctypes.c_double(0.0)
+        rc = lib().oracle_solve(self._h, float(self.spec.dt if dt is None else dt), ctypes.byref(out))
+        if rc != 0:
+            raise RuntimeError("oracle_solve: " + lib().oracle_last_error().decode())
+        return out.value
+
+    def phase(self, name: str, dt: float | None = None) -> None:
+        rc = lib().oracle_phase(self._h, name.encode(), float(self.spec.dt if dt is None else dt))
+        if rc != 0:
+            raise RuntimeError(f"oracle phase {name}: " + lib().oracle_last_error().decode())
+
+    def stats(self) -> dict:
+        out = np.zeros(10)
+        lib().oracle_stats(self._h, _ptr(out))
+        keys = ("continuity", "courant", "mom_iters", "p_iters_last", "p_iters_total", "p_solves",
+                "p_res_max", "mom_res_max", "ghosts", "rows")
+        return dict(zip(keys, out.tolist()))
+
+    def get(self, name: str) -> np.ndarray:
+        L = lib()
+        n = L.oracle_array(self._h, name.encode(), None, 0, 0)
+        if n < 0:
+            raise KeyError(name)
+        out = np.zeros(n, dtype=np.float64)
+        L.oracle_array(self._h, name.encode(), _ptr(out), n, 0)
+        return out
+
+    def set(self, name: str, values: np.ndarray) -> None:
+        L = lib()
+        n = L.oracle_array(self._h, name.encode(), None, 0, 0)
+        if n < 0:
+            raise KeyError(name)
+        v = np.ascontiguousarray(values, dtype=np.float64).ravel()
+        if v.size != n:
+            raise ValueError(f"{name}: expected {n} values, got {v.size}")
+        L.oracle_array(self._h, name.encode(), _ptr(v), n, 1)
+
+
+def ksp7(shape, coef7: np.ndarray, b: np.ndarray, method: str, rtol: float, maxit: int):
+    from caffe_old_b200 import cases as C
+    nI, nJ, nK = shape
+    coef7 = np.ascontiguousarray(coef7, dtype=np.float64)
+    b = np.ascontiguousarray(b, dtype=np.float64)
+    x = np.zeros_like(b)
+    it = ctypes.c_int(0)
+    rr = ctypes.c_double(0.0)
+    st = lib().oracle_ksp7(nI, nJ, nK, _ptr(coef7), _ptr(b), _ptr(x), C.KSP_METHODS[method], float(rtol), int(maxit),
+                           ctypes.byref(it), ctypes.byref(rr))
+    return x, it.value, rr.value, st
+
+
+def hex_volume(p8: np.ndarray) -> float:
+    p = np.ascontiguousarray(p8, dtype=np.float64)
+    return lib().oracle_hex_volume(_ptr(p))
+
+
+def hex_centroid(p8: np.ndarray) -> np.ndarray:
+    p = np.ascontiguousarray(p8, dtype=np.float64)
+    out = np.zeros(3)
+    lib().oracle_hex_centroid(_ptr(p), _ptr(out))
+    return out
+
+
+def quad_area(p4: np.ndarray) -> float:
+    p = np.ascontiguousarray(p4, dtype=np.float64)
+    return lib().oracle_quad_area(_ptr(p))
+
+
+def inside_hex(pt, p8) -> bool:
+    a = np.ascontiguousarray(pt, dtype=np.float64)
+    p = np.ascontiguousarray(p8, dtype=np.float64)
+    return bool(lib().oracle_inside_hex(_ptr(a), _ptr(p)))
+
+
+def trilinear(p8, ip) -> np.ndarray:
+    p = np.ascontiguousarray(p8, dtype=np.float64)
+    a = np.ascontiguousarray(ip, dtype=np.float64)
+    out = np.zeros(8)
+    lib().oracle_trilinear(_ptr(p), _ptr(a), _ptr(out))
+    return out
+
+
+def nearest_intersect(radius, center, pt) -> np.ndarray:
+    c = np.ascontiguousarray(center, dtype=np.float64)
+    a = np.ascontiguousarray(pt, dtype=np.float64)
+    out = np.zeros(3)
+    lib().oracle_nearest_intersect(float(radius), _ptr(c), _ptr(a), _ptr(out))
+    return out
