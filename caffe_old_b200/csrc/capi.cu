@@ -434,6 +434,13 @@ bool find_array(caffe_dev* h, const std::string& nm, ArrDesc& a) {
         if (f < 0 || f > 5) return false;
         return face(h->pPatch[f], h->patchN[f], 1);
     }
+    if (nm == "status") { a.kind = 3; a.n = L.N; a.planes = 1; a.stride = L.N; a.base = nullptr; a.writable = false; return h->ib; }
+    if (nm == "ibCell" || nm == "ibCol" || nm == "ibValMom" || nm == "ibValP") {
+        if (!h->ib) return false;
+        a.kind = nm == "ibCell" ? 4 : (nm == "ibCol" ? 5 : (nm == "ibValMom" ? 6 : 7));
+        a.n = (nm == "ibCell" ? 1 : 9) * (long long)h->ibs.nGhost; a.planes = 1; a.stride = a.n; a.base = nullptr; a.writable = false;
+        return true;
+    }
     if (nm == "momA") { a.kind = 1; a.n = L.N; a.planes = 7; a.stride = L.PS; a.base = h->ma[0]; a.writable = false; return true; }
     if (nm == "pcA") { a.kind = 2; a.n = L.N; a.planes = 7; a.stride = L.PS; a.base = h->paP; a.writable = false; return true; }
     return false;
@@ -601,6 +608,23 @@ long caffe_dev_array(caffe_dev* h, const char* name, double* host, long count, i
     if (toDev && (!a.writable || a.kind != 0)) { set_error(std::string("array is read-only: ") + name); return -1; }
     if (cudaSetDevice(h->device) != cudaSuccess) { set_error("cudaSetDevice failed"); return -1; }
     if (cudaStreamSynchronize(h->st) != cudaSuccess) { set_error(std::string("stream: ") + cudaGetErrorString(cudaGetLastError())); return -1; }
+    if (a.kind >= 3) {
+        // cell status (uint8) and immersed-boundary ghost rows, converted to doubles
+        if (a.kind == 3) {
+            std::vector<uint8_t> v((size_t)a.n);
+            if (cudaMemcpy(v.data(), h->status, a.n, cudaMemcpyDeviceToHost) != cudaSuccess) { set_error("copy failed"); return -1; }
+            for (long long q = 0; q < a.n; ++q) host[q] = v[q];
+        } else if (a.kind == 4 || a.kind == 5) {
+            std::vector<int> v((size_t)a.n);
+            const int* src = a.kind == 4 ? h->ibs.gCell : h->ibs.gCol;
+            if (a.n && cudaMemcpy(v.data(), src, a.n * sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) { set_error("copy failed"); return -1; }
+            for (long long q = 0; q < a.n; ++q) host[q] = v[q];
+        } else {
+            const double* src = a.kind == 6 ? h->ibs.gValMom : h->ibs.gValP;
+            if (a.n && cudaMemcpy(host, src, a.n * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess) { set_error("copy failed"); return -1; }
+        }
+        return need;
+    }
     if (a.kind != 0) {
         // coefficient matrices: host layout [N][7] in the order aP aE aW aN aS aT aB
         std::vector<double> planes((size_t)7 * a.n);
@@ -686,8 +710,10 @@ int caffe_ksp7_solve_device(int nI, int nJ, int nK, const double* d_coef7, const
     double* x = cellbuf(1);
     KspWork w;
     std::memset(&w, 0, sizeof(w));
-    w.r = cellbuf(1); w.rp = cellbuf(1); w.p[0] = cellbuf(1); w.p[1] = cellbuf(1);
-    w.v[0] = cellbuf(1); w.v[1] = cellbuf(1); w.t = cellbuf(1); w.invD = cellbuf(1);
+    // same shape as a handle's workspace: every vector has 3 planes (the CG kernel uses
+    // the second plane of r as its double buffer)
+    w.r = cellbuf(3); w.rp = cellbuf(3); w.p[0] = cellbuf(3); w.p[1] = cellbuf(3);
+    w.v[0] = cellbuf(3); w.v[1] = cellbuf(3); w.t = cellbuf(3); w.invD = cellbuf(1);
     void* part = nullptr;
     void* outp = nullptr;
     bool ok = cudaMalloc(&part, 2 * 8 * 8 * 1024 * sizeof(double)) == cudaSuccess && cudaMalloc(&outp, sizeof(KspOut)) == cudaSuccess;

@@ -345,7 +345,6 @@ __global__ void __launch_bounds__(256) correct_kernel(Geo g, Bc bc, FlowFields f
             int idx = dir == 0 ? i : (dir == 1 ? j : k);
             if (idx == 0) f.Fout[dir][fidx[2 * dir + 1]] = f.F[dir][fidx[2 * dir + 1]];
         }
-        return;
     }
     double pcP = f.pc[c], dP = f.d[c], VP = g.vol[c];
     double gsx = 0., gsy = 0., gsz = 0.;
@@ -384,6 +383,7 @@ __global__ void __launch_bounds__(256) correct_kernel(Geo g, Bc bc, FlowFields f
         double sx = g.S[dir][fi], sy = g.S[dir][fi + nF], sz = g.S[dir][fi + 2 * nF];
         if (!upper) { sx = -sx; sy = -sy; sz = -sz; }
         gsx = gsx + sx * pcF; gsy = gsy + sy * pcF; gsz = gsz + sz * pcF;
+        if (inact) continue;   // grad p' is formed for every cell; the rest only for non-inactive cells
         double Fold = f.F[dir][fi];
         double DF = g.D[dir][fi];
         double Fnew = Fold;
@@ -402,6 +402,7 @@ __global__ void __launch_bounds__(256) correct_kernel(Geo g, Bc bc, FlowFields f
     double rv = 1. / VP;
     double gx = gsx * rv, gy = gsy * rv, gz = gsz * rv;
     f.gradPC[c] = gx; f.gradPC[c + N] = gy; f.gradPC[c + 2 * N] = gz;
+    if (inact) return;
     f.mfc[c] = Fn[0] - Fn[1] + Fn[2] - Fn[3] + Fn[4] - Fn[5];
     f.p[c] = f.p[c] + omp * pcP;
     double md = -dP;

@@ -244,9 +244,11 @@ __global__ void ghost_rows_kernel(Geo g, const double* xyz, const uint8_t* statu
     vp[0] = dp;
 }
 
+// every cell inside the sphere -- ghost cells included, which IbPiso::computeIbField marks
+// SOLID before re-flagging them IB -- gets u = 0, p = 0 (IbPiso.cpp:74-80)
 __global__ void solid_reset_kernel(Lat L, const uint8_t* status, double* u, double* p) {
     long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (c >= L.N || status[c] != ST_INACTIVE) return;
+    if (c >= L.N || status[c] == ST_ACTIVE) return;
     u[c] = 0.; u[c + L.PS] = 0.; u[c + 2 * L.PS] = 0.;
     p[c] = 0.;
 }

@@ -27,7 +27,7 @@ int ib_create(IbState& s, const Lat& L, uint8_t*& status, const Alloc& alloc, cu
 // Classify cells, list ghost cells and build their stencil rows (IbPiso.cpp:65-190).
 int ib_setup(IbState& s, const Geo& g, const caffe_case& cs, const double* d_xyz, uint8_t* status, const Alloc& alloc,
              cudaStream_t st);
-// Per step: solid cells get u = 0, p = 0 (IbPiso.cpp:74-80).
+// Per step: cells inside the sphere (ghost and inactive) get u = 0, p = 0 (IbPiso.cpp:74-80).
 int ib_compute_field(IbState& s, const Geo& g, const caffe_case& cs, double* u, double* p, const uint8_t* status, cudaStream_t st);
 // Per inner iteration: ghost diagonals into both systems' diagonal arrays.
 int ib_compute_coeffs(IbState& s, const Geo& g, const caffe_case& cs, const uint8_t* status, double* momDiag, double* pDiag,

@@ -16,8 +16,9 @@
 // residual meets it; the iteration restarts from the true residual otherwise) or at
 // maxit, so no launch can run unbounded.
 //
-// Neighbour values written earlier in the same launch by other blocks are read with
-// ld.global.cg (L2 only), never through the incoherent L1.  Vectors that can be formed
+// Values written earlier in the same launch by other blocks are read with ordinary loads
+// after the grid barrier (whose device-scope fence orders them), never through the
+// read-only (non-coherent) path; only never-written inputs use __ldg.  Vectors that can be formed
 // from others are not stored: CG's search direction p = z + beta p_old and BiCGStab's
 // p = r + beta (p_old - omega v) and s = r - alpha v are recomputed at the stencil
 // neighbours instead of costing an extra pass and barrier.
@@ -31,7 +32,7 @@ namespace cb {
 constexpr int KB = 256;   // threads per block
 constexpr int KP = 8;     // partial slots per block
 
-__device__ __forceinline__ double ldcg(const double* p) { return __ldcg(p); }
+__device__ __forceinline__ double ldcg(const double* p) { return *p; }   // coherent load after a grid barrier
 
 template <int K>
 __device__ __forceinline__ void warp_sum(double (&v)[K]) {
@@ -500,6 +501,121 @@ __global__ void __launch_bounds__(KB) cg_kernel(Op A, KArgs a) {
     if (blockIdx.x == 0 && threadIdx.x == 0) { a.out->iters[0] = it; a.out->relres[0] = relres; a.out->status[0] = status; }
 }
 
+// ------------------------------------------------------------------ CG, one reduction per iteration
+// Chronopoulos & Gear (1989) form of preconditioned CG: with u = M^-1 r and w = A u the two
+// inner products (r, u) and (w, u) are taken together, so an iteration is one sweep and one
+// grid barrier:
+//   s_i = w_i + beta_i s_{i-1};  p_i = u_i + beta_i p_{i-1};  x += alpha_i p_i;
+//   r_{i+1} = r_i - alpha_i s_i;  u_{i+1} = M^-1 r_{i+1};  w_{i+1} = A u_{i+1};
+//   gamma = (r_{i+1}, u_{i+1}), delta = (w_{i+1}, u_{i+1});
+//   beta_{i+1} = gamma_{i+1} / gamma_i;  alpha_{i+1} = gamma_{i+1} / (delta - beta_{i+1} gamma_{i+1} / alpha_i).
+// u_{i+1} at the stencil neighbours is recomputed from r_i, w_i and s_{i-1}, which are
+// double-buffered (the sweep writes the other buffer).
+template <class Op>
+__global__ void __launch_bounds__(KB, 4) cg1_kernel(Op A, KArgs a) {
+    cg::grid_group grid = cg::this_grid();
+    const long long N = a.N, PS = a.PS;
+    const long long T = (long long)gridDim.x * blockDim.x;
+    const long long t0 = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const double* invD = a.invD;
+    // current (read) and next (written) buffers, swapped after every sweep
+    double *rC = a.r, *rN = a.r + PS, *wC = a.v[0], *wN = a.v[1], *sC = a.p[0], *sN = a.p[1];
+    double* p = a.t;       // u = M^-1 r is not stored: it is recomputed from r where needed
+    int par = 0;
+    if (a.project) project_mean(grid, const_cast<double*>(a.b), N, t0, T, a.partials, par);
+    // ---- start: x = 0, r = b, u = M^-1 b, w = A u, s_-1 = p_-1 = 0
+    double acc[3] = {0., 0., 0.};
+    for (long long c = t0; c < N; c += T) {
+        double bv = a.b[c];
+        double uv = __ldg(invD + c) * bv;
+        double y[1];
+        apply<1>(A, c, [&](int, long long e) { return __ldg(invD + e) * a.b[e]; }, y);
+        a.x[c] = 0.;
+        rC[c] = bv; wC[c] = y[0]; sC[c] = 0.; p[c] = 0.;
+        acc[0] += bv * uv; acc[1] += y[0] * uv; acc[2] += bv * bv;
+    }
+    double tot[3];
+    grid_reduce<3>(grid, acc, a.partials, par, tot);
+    double gamma = tot[0], bb = tot[2];
+    double tol2 = a.rtol * a.rtol * bb;
+    double alpha = tot[1] != 0. ? gamma / tot[1] : 0., beta = 0.;
+    int it = 0, status = 0;
+    double relres = 0.;
+    bool done = !(bb > 0.);
+    if (bb != bb) status = 3;
+    while (!done) {
+        const double* r0 = rC;
+        const double* w0 = wC;
+        const double* s0 = sC;
+        double* r1 = rN;
+        double* w1 = wN;
+        double* s1 = sN;
+        acc[0] = acc[1] = acc[2] = 0.;
+        for (long long c = t0; c < N; c += T) {
+            double idc = __ldg(invD + c);
+            double r0c = r0[c];
+            double si = w0[c] + beta * s0[c];
+            double pi = idc * r0c + beta * p[c];
+            a.x[c] = a.x[c] + alpha * pi;
+            double rn = r0c - alpha * si;
+            double un = idc * rn;
+            double y[1];
+            apply<1>(A, c, [&](int, long long e) {
+                return __ldg(invD + e) * (r0[e] - alpha * (w0[e] + beta * s0[e]));
+            }, y);
+            s1[c] = si; p[c] = pi; r1[c] = rn; w1[c] = y[0];
+            acc[0] += rn * un; acc[1] += y[0] * un; acc[2] += rn * rn;
+        }
+        grid_reduce<3>(grid, acc, a.partials, par, tot);
+        it += 1;
+        { double* t_ = rC; rC = rN; rN = t_; t_ = wC; wC = wN; wN = t_; t_ = sC; sC = sN; sN = t_; }
+        double gn = tot[0], dn = tot[1], rr = tot[2];
+        bool check = rr <= tol2 || it >= a.maxit || rr != rr;
+        double bn = gn / gamma;
+        double den = dn - bn * gn / alpha;
+        if (den == 0. || den != den || gamma == 0.) check = true;
+        beta = bn; alpha = gn / den; gamma = gn;
+        if (check) {
+            // ---- true residual r = b - A x (into the current buffer)
+            double* rc = rC;
+            double a2[1] = {0.};
+            for (long long c = t0; c < N; c += T) {
+                double y[1];
+                apply<1>(A, c, [&](int, long long e) { return a.x[e]; }, y);
+                double rt = a.b[c] - y[0];
+                rc[c] = rt;
+                a2[0] += rt * rt;
+            }
+            double t1[1];
+            grid_reduce<1>(grid, a2, a.partials, par, t1);
+            relres = sqrt(t1[0] / bb);
+            if (t1[0] <= tol2) { done = true; status = 0; }
+            else if (t1[0] != t1[0]) { done = true; status = 3; }
+            else if (it >= a.maxit) { done = true; status = 1; }
+            else {
+                // restart from the true residual: u = M^-1 r, w = A u, s = p = 0
+                double a3[2] = {0., 0.};
+                double* wc = wC;
+                double* sc = sC;
+                for (long long c = t0; c < N; c += T) {
+                    double uv = __ldg(invD + c) * rc[c];
+                    double y[1];
+                    apply<1>(A, c, [&](int, long long e) { return __ldg(invD + e) * rc[e]; }, y);
+                    wc[c] = y[0]; sc[c] = 0.; p[c] = 0.;
+                    a3[0] += rc[c] * uv; a3[1] += y[0] * uv;
+                }
+                double t2[2];
+                grid_reduce<2>(grid, a3, a.partials, par, t2);
+                gamma = t2[0];
+                alpha = t2[1] != 0. ? gamma / t2[1] : 0.;
+                beta = 0.;
+                if (gamma == 0.) { done = true; status = 2; }
+            }
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) { a.out->iters[0] = it; a.out->relres[0] = relres; a.out->status[0] = status; }
+}
+
 // ------------------------------------------------------------------ host side
 static int g_numSM = 0;
 
@@ -570,8 +686,8 @@ int ksp_cg(const OpSym& A, const double* b, double* x, const Lat& L, const KspWo
     KArgs a = make_args(L, w, b, x, rtol, maxit);
     a.project = project;
     static int G = 0;
-    if (!G) G = coop_grid(cg_kernel<OpSym>);
-    return launch_coop(cg_kernel<OpSym>, G, a, &A, st);
+    if (!G) G = coop_grid(cg1_kernel<OpSym>);
+    return launch_coop(cg1_kernel<OpSym>, G, a, &A, st);
 }
 
 int ksp_cg7(const Op7& A, const double* b, double* x, const Lat& L, const KspWork& w, double rtol, int maxit, cudaStream_t st) {
@@ -579,15 +695,15 @@ int ksp_cg7(const Op7& A, const double* b, double* x, const Lat& L, const KspWor
     CB_CHECK_LAUNCH();
     KArgs a = make_args(L, w, b, x, rtol, maxit);
     static int G = 0;
-    if (!G) G = coop_grid(cg_kernel<Op7>);
-    return launch_coop(cg_kernel<Op7>, G, a, &A, st);
+    if (!G) G = coop_grid(cg1_kernel<Op7>);
+    return launch_coop(cg1_kernel<Op7>, G, a, &A, st);
 }
 
 int krylov_grid_size(int which) {
     switch (which) {
         case 0: return coop_grid(bicgstab_kernel<3, Op7>);
         case 1: return coop_grid(bicgstab_kernel<1, OpSym>);
-        case 2: return coop_grid(cg_kernel<OpSym>);
+        case 2: return coop_grid(cg1_kernel<OpSym>);
         default: return coop_grid(bicgstab_kernel<1, Op7>);
     }
 }

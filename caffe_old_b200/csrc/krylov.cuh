@@ -41,7 +41,7 @@ struct KspOut {
 };
 
 // Workspace for up to NR = 3 right-hand sides; every array is a halo-padded cell array of
-// 3 planes.
+// 3 planes (the single right-hand-side CG also uses plane 1 of r as a second buffer).
 struct KspWork {
     double* r;
     double* rp;

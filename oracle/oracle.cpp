@@ -1326,6 +1326,26 @@ long oracle_array(void* hh, const char* name, double* buf, long count, int dir) 
         if (buf && count >= need && dir == 0) for (int q = 0; q < s->N; ++q) buf[q] = s->status[q];
         return need;
     }
+    if (n == "rowOfCell") {
+        long need = s->N;
+        if (buf && count >= need && dir == 0) for (int q = 0; q < s->N; ++q) buf[q] = s->row[q];
+        return need;
+    }
+    if (n == "A0coo" || n == "A1coo") {   // (row, col, value) triplets of a system matrix
+        orc::Rows& R = s->A[n[1] - '0'];
+        long nnz = 0;
+        for (int r = 0; r < R.n; ++r) nnz += R.cnt[r];
+        long need = 3 * nnz;
+        if (buf && count >= need && dir == 0) {
+            long q = 0;
+            for (int r = 0; r < R.n; ++r)
+                for (int e = 0; e < R.cnt[r]; ++e) {
+                    buf[q++] = r; buf[q++] = R.col[(size_t)r * R.width + e]; buf[q++] = R.val[(size_t)r * R.width + e];
+                }
+        }
+        return need;
+    }
+    if (n == "b0") return vecd(s->bv[0]);
     if (n == "ibStencil") {
         long need = (long)s->ibStencil.size();
         if (buf && count >= need && dir == 0) for (size_t q = 0; q < s->ibStencil.size(); ++q) buf[q] = s->ibStencil[q];

@@ -108,15 +108,37 @@ def test_steps_match_oracle(maker, steps):
 
 
 def test_ib_stencils_bit_exact():
+    """Ghost classification and image-point rows (IbPiso.cpp:65-190) equal the oracle's."""
     nodes, spec = small_channel_sphere()
     o = OracleSolver(nodes, spec)
     o.phase("ib_field")
     o.phase("ib_coeffs")
     d = make_solver(nodes, spec)
+    status = o.get("status")
+    assert np.array_equal(d.field("status"), status)
+    cells = np.flatnonzero(status == 1)
+    assert np.array_equal(d.field("ibCell"), cells)
+    beta = o.get("ibBeta").reshape(-1, 8)
+    sten = o.get("ibStencil").reshape(-1, 8).astype(int)
+    col = d.field("ibCol").reshape(-1, 9).astype(int)
+    vm = d.field("ibValMom").reshape(-1, 9)
+    vp = d.field("ibValP").reshape(-1, 9)
+    assert np.array_equal(col[:, 0], cells)
+    for g, c in enumerate(cells):
+        dm, dp = 1.0, -1.0
+        for m in range(8):
+            if sten[g, m] == c:
+                dm += beta[g, m]
+                dp = -1.0 + beta[g, m]
+                assert col[g, m + 1] == -1
+            else:
+                dp = -1.0
+                assert col[g, m + 1] == (-1 if status[sten[g, m]] == 2 else sten[g, m])
+                assert vm[g, m + 1] == beta[g, m] and vp[g, m + 1] == beta[g, m]
+        assert vm[g, 0] == dm and vp[g, 0] == dp
     d.solve()
     ost = o.stats()
-    assert d.last_stats["n_ghost"] == int(ost["ghosts"])
-    assert d.last_stats["n_rows"] == int(ost["rows"])
+    assert d.last_stats["n_ghost"] == int(ost["ghosts"]) == len(cells)
 
 
 @pytest.mark.parametrize("method", ["cg_jacobi", "bicgstab_jacobi"])
