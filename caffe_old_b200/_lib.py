@@ -64,7 +64,7 @@ class StepStats(ctypes.Structure):
 EXPORTS = (
     "caffe_last_error", "caffe_dev_create", "caffe_dev_destroy", "caffe_dev_solve", "caffe_dev_phase",
     "caffe_dev_array", "caffe_dev_stats", "caffe_dev_stream", "caffe_dev_synchronize",
-    "caffe_ksp7_solve", "caffe_ksp7_solve_device",
+    "caffe_ksp7_solve", "caffe_ksp7_solve_device", "caffe_ksp7_solve_device_noalloc",
 )
 
 
@@ -90,6 +90,8 @@ def lib():
     L.caffe_dev_synchronize.argtypes = [vp]
     L.caffe_ksp7_solve.argtypes = [ci, ci, ci, vp, vp, vp, ci, cd, ci, ctypes.POINTER(ci), ctypes.POINTER(cd)]
     L.caffe_ksp7_solve_device.argtypes = [ci, ci, ci, vp, vp, vp, ci, cd, ci, vp, ctypes.POINTER(ci), ctypes.POINTER(cd)]
+    L.caffe_ksp7_solve_device_noalloc.argtypes = [ci, ci, ci, vp, vp, vp, ci, cd, ci, vp, ctypes.POINTER(ci),
+                                                  ctypes.POINTER(cd)]
     _lib = L
     return L
 

@@ -129,6 +129,20 @@ int caffe_ksp7_solve(int nI, int nJ, int nK, const double* coef7, const double* 
 int caffe_ksp7_solve_device(int nI, int nJ, int nK, const double* d_coef7, const double* d_b, double* d_x,
                             int method, double rtol, int maxit, void* stream, int* iters, double* rel_res);
 
+/* caffe_ksp7_solve_device without any device allocation.  It has no counterpart in the
+ * reference.  For callers that cannot call cudaMalloc/cudaFree from inside a solve -- a program
+ * whose own allocator already owns nearly all of HBM, or a time loop that cannot take the
+ * device-wide synchronisation cudaFree implies -- the workspace lives in one 16 MiB __device__
+ * array inside this library (held on every GPU that loads it, until exit).  Same arguments and
+ * results as caffe_ksp7_solve_device (d_coef7, d_b, d_x are the caller's device arrays); lattices
+ * whose workspace, 11 halo-padded planes of nI*nJ*nK + 2*ceil32(nI*nJ) doubles plus 128 KiB,
+ * exceeds 16 MiB (about 180 thousand cells) are rejected with an error.  Calls share the array:
+ * each clears the part it uses on entry, and calls that overlap on the GPU race.  The first call
+ * on a device looks up the array's address (cudaGetSymbolAddress); make it before any stream
+ * capture. */
+int caffe_ksp7_solve_device_noalloc(int nI, int nJ, int nK, const double* d_coef7, const double* d_b, double* d_x,
+                                    int method, double rtol, int maxit, void* stream, int* iters, double* rel_res);
+
 #ifdef __cplusplus
 }
 #endif
