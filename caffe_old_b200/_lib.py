@@ -65,6 +65,7 @@ EXPORTS = (
     "caffe_last_error", "caffe_dev_create", "caffe_dev_destroy", "caffe_dev_solve", "caffe_dev_phase",
     "caffe_dev_array", "caffe_dev_stats", "caffe_dev_stream", "caffe_dev_synchronize",
     "caffe_ksp7_solve", "caffe_ksp7_solve_device", "caffe_ksp7_solve_device_noalloc",
+    "caffe_precond_param_count", "caffe_precond_net_apply", "caffe_precond_net_grad",
 )
 
 
@@ -92,6 +93,9 @@ def lib():
     L.caffe_ksp7_solve_device.argtypes = [ci, ci, ci, vp, vp, vp, ci, cd, ci, vp, ctypes.POINTER(ci), ctypes.POINTER(cd)]
     L.caffe_ksp7_solve_device_noalloc.argtypes = [ci, ci, ci, vp, vp, vp, ci, cd, ci, vp, ctypes.POINTER(ci),
                                                   ctypes.POINTER(cd)]
+    L.caffe_precond_param_count.restype = ci
+    L.caffe_precond_net_apply.argtypes = [ci, ci, ci, vp, vp, vp]
+    L.caffe_precond_net_grad.argtypes = [ci, ci, ci, vp, vp, vp, vp, vp]
     _lib = L
     return L
 

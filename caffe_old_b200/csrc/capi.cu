@@ -136,6 +136,10 @@ struct caffe_dev {
         double* b = dalloc<double>((size_t)L.PS * planes);
         return b ? b + L.H : nullptr;
     }
+    float* fcell() {
+        float* b = dalloc<float>((size_t)L.PS);
+        return b ? b + L.H : nullptr;
+    }
     FlowFields fields(bool forCorrect = false) {
         FlowFields f;
         f.u = u;
@@ -251,6 +255,10 @@ int fill(caffe_dev* h, double* dst, int planes, double a, double b = 0., double 
 // constant vector is its null space) and its right-hand side carries a round-off
 // component along it that no Krylov method can remove; the solver then projects the
 // right-hand side onto the range first (the CPU oracle does the same).
+// deepest relative residual reduction an FP32 inner solve of the mixed-precision form aims for
+// (later inner solves only aim for the factor still missing)
+constexpr double MIXED_INNER_RTOL = 1e-6;
+
 int p_singular(const caffe_dev* h) {
     if (h->ib) return 0;
     for (int f = 0; f < 6; ++f) if (h->bc.pType[f] == P_FIXED) return 0;
@@ -287,9 +295,19 @@ int ph_solve_pcorr(caffe_dev* h) {
     OpSym A = h->pOp();
     bool sym = !(h->ib && h->ibs.nGhost > 0);
     int method = h->cs.p_method;
+    if (method == CAFFE_KSP_CG_JACOBI && !sym) method = CAFFE_KSP_BICGSTAB_JACOBI;   // ghost rows are not symmetric
     int project = p_singular(h);
-    if (method == CAFFE_KSP_CG_JACOBI && sym) rc = ksp_cg(A, h->pb, h->pc, h->L, h->kw, h->cs.p_rtol, h->cs.maxit, h->st, project);
-    else rc = ksp_bicgstab_sym(A, h->pb, h->pc, h->L, h->kw, h->cs.p_rtol, h->cs.maxit, h->st, project);
+    if (h->cs.p_form == CAFFE_P_MIXED) {
+        // FP32 inner solves inside FP64 refinement; the plain FP64 solve re-runs on the device
+        // when the refinement does not reach the tolerance
+        rc = ksp_mixed_sym(A, method, h->pb, h->pc, h->L, h->kw, h->cs.p_rtol, h->cs.maxit, MIXED_INNER_RTOL, h->st, project);
+        if (!rc) rc = ksp_fallback_sym(A, method, h->pb, h->pc, h->L, h->kw, h->cs.p_rtol, h->cs.maxit, h->st, 0,
+                                       &h->kw.out->status[0], &h->acc->fallbacks);
+    } else if (method == CAFFE_KSP_CG_JACOBI) {
+        rc = ksp_cg(A, h->pb, h->pc, h->L, h->kw, h->cs.p_rtol, h->cs.maxit, h->st, project);
+    } else {
+        rc = ksp_bicgstab_sym(A, h->pb, h->pc, h->L, h->kw, h->cs.p_rtol, h->cs.maxit, h->st, project);
+    }
     if (rc) return rc;
     acc_kernel<<<1, 32, 0, h->st>>>(h->kw.out, h->acc, 1, 1);
     CB_CHECK_LAUNCH();
@@ -504,6 +522,15 @@ int caffe_dev_create(const double* nodes, int nNI, int nNJ, int nNK, const caffe
     h->kw.p[0] = h->cell(3); h->kw.p[1] = h->cell(3);
     h->kw.v[0] = h->cell(3); h->kw.v[1] = h->cell(3);
     h->kw.t = h->cell(3); h->kw.invD = h->cell(1);
+    if (cs->p_form == CAFFE_P_MIXED || cs->p_form == CAFFE_P_LEARNED_MIXED) {
+        for (int q = 0; q < 2; ++q) { h->kw.fr[q] = h->fcell(); h->kw.fw[q] = h->fcell(); h->kw.fs[q] = h->fcell(); h->kw.fv[q] = h->fcell(); }
+        h->kw.fp = h->fcell(); h->kw.fe = h->fcell(); h->kw.ft = h->fcell(); h->kw.finvD = h->fcell();
+        for (int q = 0; q < 4; ++q) h->kw.fA[q] = h->fcell();
+        bool ok = h->kw.fp && h->kw.fe && h->kw.ft && h->kw.finvD;
+        for (int q = 0; q < 2; ++q) ok = ok && h->kw.fr[q] && h->kw.fw[q] && h->kw.fs[q] && h->kw.fv[q];
+        for (int q = 0; q < 4; ++q) ok = ok && h->kw.fA[q];
+        if (!ok) { set_error("device allocation failed (mixed-precision workspace)"); return fail(); }
+    }
     int nsm = 0;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
     h->kw.partials = h->dalloc<double>((size_t)2 * 8 * 8 * (nsm > 0 ? nsm : 256));

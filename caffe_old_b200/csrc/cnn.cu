@@ -1,0 +1,259 @@
+// Learned preconditioner network kernels: 3x3x3 convolutions with 16 input and 16 output
+// channels as implicit GEMMs on the 5th-generation tensor cores (tcgen05, sm_100a).
+//
+// Data: activations are channel-last bf16, 16 channels (32 bytes) per cell, cell index
+// (k*nJ + j)*nI + i; zero padding outside the lattice.
+//
+// One CTA (128 threads, 4 warps) owns an 8 (i) x 16 (j) tile of output cells and marches
+// through KC consecutive k-planes.  For each output plane the tile is one UMMA problem
+// M = 128 cells, N = 16 output channels, accumulated over the 27 taps with one
+// tcgen05.mma.kind::f16 of K = 16 input channels per tap into a 128 x 16 FP32 accumulator
+// in tensor memory.  Operands are in shared memory in the canonical no-swizzle K-major
+// layout (core matrices of 8 rows x 16 bytes): the A operand of tap (dk, dj, di) is input
+// plane k+dk shifted by di along i (three i-shifted copies of each plane are staged) and
+// by dj rows of the tile (a whole-core-matrix offset in the descriptor); B is the tap's
+// 16 x 16 weight block.  Three input planes rotate as the CTA moves along k, so each input
+// plane is read from global memory once per tile.  The epilogue reads the accumulator with
+// tcgen05.ld (one TMEM lane per thread = one cell), applies bias / ReLU, or the ReLU mask
+// of the backward pass, and writes bf16 (or FP32 for the network output).
+//
+// Every wait on the MMA-completion mbarrier is bounded; a CTA that times out records an
+// error, waits once more (bounded) and frees its tensor memory before leaving.
+#include <cuda_bf16.h>
+#include <cstdint>
+
+#include "common.cuh"
+#include "cnn.cuh"
+
+namespace cb {
+
+namespace {
+
+constexpr int TI = 8, TJ = 16;          // tile: 8 cells along i, 16 along j -> M = 128
+constexpr int ROWS = TJ + 2;            // staged j-rows (one halo row each side)
+constexpr int GROUP_BYTES = 256;        // one j-row of 8 cells x 16 channels, canonical layout
+constexpr int BUF_BYTES = ROWS * GROUP_BYTES;          // 4608
+constexpr int NBUF = 9;                 // 3 planes x 3 i-shifts
+constexpr int W_BYTES = 27 * 512;       // 27 taps x 16 x 16 bf16
+constexpr uint32_t TMEM_COLS = 32;
+constexpr long long WAIT_LIMIT = 1ll << 20;   // try_wait rounds (each may block briefly): about a second at most
+
+// instruction descriptor: kind::f16, D = F32, A = B = BF16, both K-major, N = 16, M = 128
+constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((16u >> 3) << 17) | ((128u >> 4) << 24);
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// shared-memory matrix descriptor, no swizzle (sm_100 version 1)
+__device__ __forceinline__ uint64_t sdesc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
+    d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+    d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+    d |= (uint64_t)1 << 46;
+    return d;
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n"
+        :
+        : "r"(tmem_d), "l"(a), "l"(b), "r"(IDESC), "r"(acc));
+}
+
+__device__ __forceinline__ void mma_commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t phase) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred P1;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, P1;\n\t}\n"
+        : "=r"(ok)
+        : "r"(bar), "r"(phase)
+        : "memory");
+    return ok != 0;
+}
+
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t phase) {
+    for (long long t = 0; t < WAIT_LIMIT; ++t)
+        if (mbar_try(bar, phase)) return true;
+    return false;
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+          "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int q = 0; q < 16; ++q) v[q] = __uint_as_float(r[q]);
+}
+
+// Stage input plane kk into the three i-shifted canonical buffers of rotation slot `slot`.
+__device__ __forceinline__ void stage_plane(unsigned char* bufs, int slot, const __nv_bfloat16* __restrict__ in, const Lat& L,
+                                            int i0, int j0, int kk) {
+    // units of 16 bytes: 3 shifts x ROWS rows x 8 cells x 2 chunks
+    const int total = 3 * ROWS * TI * 2;
+    for (int u = threadIdx.x; u < total; u += blockDim.x) {
+        int h = u & 1;
+        int il = (u >> 1) & 7;
+        int rest = u >> 4;
+        int jr = rest % ROWS;
+        int s = rest / ROWS;        // 0,1,2 -> di = -1,0,1
+        int i = i0 + il + s - 1, j = j0 + jr - 1;
+        uint4 val = make_uint4(0u, 0u, 0u, 0u);
+        if (kk >= 0 && kk < L.nK && i >= 0 && i < L.nI && j >= 0 && j < L.nJ) {
+            long long c = ((long long)kk * L.nJ + j) * L.nI + i;
+            val = *reinterpret_cast<const uint4*>(in + c * 16 + h * 8);
+        }
+        unsigned char* dst = bufs + (size_t)(slot * 3 + s) * BUF_BYTES + jr * GROUP_BYTES + h * 128 + il * 16;
+        *reinterpret_cast<uint4*>(dst) = val;
+    }
+}
+
+}  // namespace
+
+// EPI: 0 bias + ReLU -> bf16; 1 bias -> FP32 channel 0 (network output); 2 backward data:
+// multiply by (mask_act > 0) -> bf16.  Weights: packed canonical blocks, 27 x 512 bytes.
+template <int EPI>
+__global__ void __launch_bounds__(128) conv3d_tc_kernel(Lat L, const __nv_bfloat16* __restrict__ in,
+                                                        const __nv_bfloat16* __restrict__ wpack, const float* __restrict__ bias,
+                                                        __nv_bfloat16* out_bf, float* out_f, long long out_stride,
+                                                        const __nv_bfloat16* __restrict__ mask_act, int KC, int* err) {
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    // 1 KiB-align the dynamic region
+    unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    unsigned char* wsm = smem;                                // W_BYTES
+    unsigned char* bufs = smem + W_BYTES;                     // NBUF x BUF_BYTES
+    __shared__ __align__(8) uint64_t mbar;
+    __shared__ uint32_t tmem_base_sh;
+    __shared__ float bias_sh[16];
+
+    const int i0 = blockIdx.x * TI, j0 = blockIdx.y * TJ;
+    const int k0 = blockIdx.z * KC;
+    const int k1 = min(k0 + KC, L.nK);
+    const int warp = threadIdx.x >> 5;
+
+    // weights and bias to shared memory
+    for (int u = threadIdx.x; u < W_BYTES / 16; u += blockDim.x)
+        reinterpret_cast<uint4*>(wsm)[u] = reinterpret_cast<const uint4*>(wpack)[u];
+    if (threadIdx.x < 16) bias_sh[threadIdx.x] = bias ? bias[threadIdx.x] : 0.f;
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar)));
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base_sh)),
+                     "r"(TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    // planes k0-1 and k0 into rotation slots 0 and 1
+    stage_plane(bufs, 0, in, L, i0, j0, k0 - 1);
+    stage_plane(bufs, 1, in, L, i0, j0, k0);
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    const uint32_t tmem = tmem_base_sh;
+    const uint32_t bar = smem_u32(&mbar);
+    uint32_t phase = 0;
+    bool failed = false;
+    int slotM = 0, slotC = 1, slotP = 2;   // planes k-1, k, k+1
+    for (int k = k0; k < k1; ++k) {
+        stage_plane(bufs, slotP, in, L, i0, j0, k + 1);
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        asm volatile("tcgen05.fence::before_thread_sync;");
+        __syncthreads();
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        if (threadIdx.x == 0) {
+            const uint32_t wbase = smem_u32(wsm);
+            const uint32_t bbase = smem_u32(bufs);
+            int slots[3] = {slotM, slotC, slotP};
+            int t = 0;
+#pragma unroll 1
+            for (int dk = 0; dk < 3; ++dk)
+#pragma unroll 1
+                for (int dj = 0; dj < 3; ++dj)
+#pragma unroll 1
+                    for (int di = 0; di < 3; ++di, ++t) {
+                        uint32_t a_addr = bbase + (uint32_t)((slots[dk] * 3 + di) * BUF_BYTES + dj * GROUP_BYTES);
+                        uint64_t ad = sdesc(a_addr, 128, 256);
+                        uint64_t bd = sdesc(wbase + (uint32_t)(t * 512), 128, 256);
+                        mma_bf16(tmem, ad, bd, t > 0 ? 1u : 0u);
+                    }
+            mma_commit(bar);
+        }
+        bool ok = mbar_wait_bounded(bar, phase);
+        phase ^= 1u;
+        // the decision to stop must be the same in every thread (barriers follow)
+        if (__syncthreads_or(ok ? 0 : 1)) { failed = true; break; }
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        // epilogue: thread = TMEM lane = output cell
+        float v[16];
+        tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16), v);
+        int m = threadIdx.x;
+        int i = i0 + (m & 7), j = j0 + (m >> 3);
+        if (i < L.nI && j < L.nJ) {
+            long long c = ((long long)k * L.nJ + j) * L.nI + i;
+            if (EPI == 1) {
+                out_f[c] = v[0] + bias_sh[0];
+            } else {
+                float o[16];
+                if (EPI == 0) {
+#pragma unroll
+                    for (int q = 0; q < 16; ++q) o[q] = fmaxf(v[q] + bias_sh[q], 0.f);
+                } else {
+                    const __nv_bfloat16* mp = mask_act + c * 16;
+#pragma unroll
+                    for (int q = 0; q < 16; ++q) o[q] = __bfloat162float(mp[q]) > 0.f ? v[q] : 0.f;
+                }
+                __align__(16) __nv_bfloat16 ob[16];
+#pragma unroll
+                for (int q = 0; q < 16; ++q) ob[q] = __float2bfloat16_rn(o[q]);
+                uint4* dst = reinterpret_cast<uint4*>(out_bf + c * out_stride);
+                dst[0] = reinterpret_cast<uint4*>(ob)[0];
+                dst[1] = reinterpret_cast<uint4*>(ob)[1];
+            }
+        }
+        // rotate planes; the accumulator is re-written by the next plane's first MMA only
+        // after every thread has finished reading it (barrier at the top of the loop)
+        int tmp = slotM; slotM = slotC; slotC = slotP; slotP = tmp;
+        asm volatile("tcgen05.fence::before_thread_sync;");
+    }
+    if (failed) {
+        if (threadIdx.x == 0) atomicExch(err, 1);
+        mbar_wait_bounded(bar, phase ^ 1u);   // let any MMA in flight finish before freeing TMEM
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
+}
+
+size_t conv_smem_bytes() { return 1024 + W_BYTES + NBUF * BUF_BYTES; }
+
+int launch_conv3d(const Lat& L, int epi, const __nv_bfloat16* in, const __nv_bfloat16* wpack, const float* bias, __nv_bfloat16* out_bf,
+                  float* out_f, const __nv_bfloat16* mask_act, int* err, cudaStream_t st) {
+    const int KC = 16;
+    dim3 grid((L.nI + TI - 1) / TI, (L.nJ + TJ - 1) / TJ, (L.nK + KC - 1) / KC);
+    size_t smem = conv_smem_bytes();
+    static bool attr = false;
+    if (!attr) {
+        CB_CUDA(cudaFuncSetAttribute(conv3d_tc_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        CB_CUDA(cudaFuncSetAttribute(conv3d_tc_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        CB_CUDA(cudaFuncSetAttribute(conv3d_tc_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        attr = true;
+    }
+    if (epi == 0) conv3d_tc_kernel<0><<<grid, 128, smem, st>>>(L, in, wpack, bias, out_bf, out_f, 16, mask_act, KC, err);
+    else if (epi == 1) conv3d_tc_kernel<1><<<grid, 128, smem, st>>>(L, in, wpack, bias, out_bf, out_f, 16, mask_act, KC, err);
+    else conv3d_tc_kernel<2><<<grid, 128, smem, st>>>(L, in, wpack, bias, out_bf, out_f, 16, mask_act, KC, err);
+    CB_CHECK_LAUNCH();
+    return 0;
+}
+
+}  // namespace cb

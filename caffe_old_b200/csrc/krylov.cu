@@ -25,6 +25,8 @@
 #include <cooperative_groups.h>
 #include "krylov.cuh"
 
+#define CAFFE_KSP_CG_JACOBI_INT 2   // caffe_ksp value of Jacobi-CG (include/caffe_b200.h)
+
 namespace cg = cooperative_groups;
 
 namespace cb {
@@ -183,6 +185,10 @@ struct KArgs {
     double rtol;
     int maxit;
     int project;   // remove the mean of b first (singular all-Neumann pressure systems)
+    // fallback mode: when skip_if_ok is set the launch returns at once unless the status
+    // it points to (the previous solve's) is non-zero; fallbacks counts the launches that ran
+    const int* skip_if_ok;
+    int* fallbacks;
 };
 
 // Remove the mean of b (one plane), in place; every block computes the same mean.
@@ -199,6 +205,8 @@ __device__ __forceinline__ void project_mean(cg::grid_group& grid, double* b, lo
 // ------------------------------------------------------------------ BiCGStab
 template <int NR, class Op>
 __global__ void __launch_bounds__(KB) bicgstab_kernel(Op A, KArgs a) {
+    if (a.skip_if_ok && *a.skip_if_ok == 0) return;   // uniform across the grid: no barrier is reached
+    if (a.skip_if_ok && blockIdx.x == 0 && threadIdx.x == 0 && a.fallbacks) atomicAdd(a.fallbacks, 1);
     cg::grid_group grid = cg::this_grid();
     const long long N = a.N, PS = a.PS;
     const long long T = (long long)gridDim.x * blockDim.x;
@@ -513,6 +521,8 @@ __global__ void __launch_bounds__(KB) cg_kernel(Op A, KArgs a) {
 // double-buffered (the sweep writes the other buffer).
 template <class Op>
 __global__ void __launch_bounds__(KB, 4) cg1_kernel(Op A, KArgs a) {
+    if (a.skip_if_ok && *a.skip_if_ok == 0) return;   // uniform across the grid: no barrier is reached
+    if (a.skip_if_ok && blockIdx.x == 0 && threadIdx.x == 0 && a.fallbacks) atomicAdd(a.fallbacks, 1);
     cg::grid_group grid = cg::this_grid();
     const long long N = a.N, PS = a.PS;
     const long long T = (long long)gridDim.x * blockDim.x;
@@ -616,6 +626,237 @@ __global__ void __launch_bounds__(KB, 4) cg1_kernel(Op A, KArgs a) {
     if (blockIdx.x == 0 && threadIdx.x == 0) { a.out->iters[0] = it; a.out->relres[0] = relres; a.out->status[0] = status; }
 }
 
+// ------------------------------------------------------------------ mixed precision
+// FP64 iterative refinement around FP32 inner solves (the precision form of the pressure
+// correction): the true residual r = b - A x, the update x += e, and every dot product and
+// norm stay FP64; the matrix copy, the Jacobi preconditioner, the inner Krylov vectors and
+// the inner operator sweeps are FP32.  One launch runs the whole solve:
+//   repeat: r = b - A x (FP64, reduced) -> stop at ||r|| <= rtol ||b||;
+//           A32 e = float(r) by FP32 CG or BiCGStab to inner_rtol (relative);  x += e.
+struct OpSymF {
+    const float* aP;
+    const float* aE;
+    const float* aN;
+    const float* aT;
+    long long nI, nIJ;
+    GhostRows gh;
+};
+
+template <class X>
+__device__ __forceinline__ float applyf(const OpSymF& A, long long c, X&& x) {
+    float aP = __ldg(A.aP + c), aE = __ldg(A.aE + c), aW = __ldg(A.aE + c - 1), aN = __ldg(A.aN + c);
+    float aS = __ldg(A.aN + c - A.nI), aT = __ldg(A.aT + c), aB = __ldg(A.aT + c - A.nIJ);
+    float y = aP * x(c) + aE * x(c + 1) + aW * x(c - 1) + aN * x(c + A.nI) + aS * x(c - A.nI) + aT * x(c + A.nIJ)
+              + aB * x(c - A.nIJ);
+    if (A.gh.n > 0) {
+        uint32_t wbits = __ldg(A.gh.bits + (c >> 5));
+        if ((wbits >> (c & 31)) & 1u) {
+            int g = ghost_index(A.gh, c);
+            float sum = 0.f;
+            for (int m = 0; m < 9; ++m) {
+                int col = __ldg(A.gh.col + 9 * g + m);
+                if (col >= 0) sum += (float)__ldg(A.gh.val + 9 * g + m) * x((long long)col);
+            }
+            y = sum;
+        }
+    }
+    return y;
+}
+
+__global__ void cast_sym_kernel(OpSym A, long long N, float* aP, float* aE, float* aN, float* aT, float* invD) {
+    long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (c >= N) return;
+    double d = A.aP[c];
+    aP[c] = (float)d; aE[c] = (float)A.aE[c]; aN[c] = (float)A.aN[c]; aT[c] = (float)A.aT[c];
+    invD[c] = d != 0. ? (float)(1. / d) : 1.f;
+}
+
+struct MxArgs {
+    const double* b;
+    double* x;
+    float* r[2];
+    float* w[2];
+    float* s[2];
+    float* p;
+    float* e;
+    float* v[2];
+    float* t;
+    const float* invD;
+    double* partials;
+    KspOut* out;
+    long long N;
+    double rtol;
+    int maxit;
+    double eta;
+    int project;
+    int inner_max;
+};
+
+template <class Op64, int INNER_BICG>
+__global__ void __launch_bounds__(KB, 4) mixed_kernel(Op64 A, OpSymF Af, MxArgs a) {
+    cg::grid_group grid = cg::this_grid();
+    const long long N = a.N;
+    const long long T = (long long)gridDim.x * blockDim.x;
+    const long long t0 = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const float* invD = a.invD;
+    int par = 0;
+    if (a.project) project_mean(grid, const_cast<double*>(a.b), N, t0, T, a.partials, par);
+    double acc1[1] = {0.};
+    for (long long c = t0; c < N; c += T) {
+        double bv = a.b[c];
+        a.x[c] = 0.;
+        acc1[0] += bv * bv;
+    }
+    double tot1[1];
+    grid_reduce<1>(grid, acc1, a.partials, par, tot1);
+    double bb = tot1[0], tol2 = a.rtol * a.rtol * bb;
+    int status = 0, inner_total = 0, outer = 0;
+    double relres = 0.;
+    bool done = !(bb > 0.);
+    if (bb != bb) { status = 3; done = true; }
+    float* rC = a.r[0];
+    float* rN = a.r[1];
+    while (!done) {
+        // ---- FP64 true residual, handed to the inner solver in FP32
+        acc1[0] = 0.;
+        for (long long c = t0; c < N; c += T) {
+            double y[1];
+            apply<1>(A, c, [&](int, long long e_) { return a.x[e_]; }, y);
+            double rt = a.b[c] - y[0];
+            rC[c] = (float)rt;
+            acc1[0] += rt * rt;
+        }
+        grid_reduce<1>(grid, acc1, a.partials, par, tot1);
+        double rr = tot1[0];
+        relres = sqrt(rr / bb);
+        if (rr <= tol2) { status = 0; break; }
+        if (rr != rr) { status = 3; break; }
+        if (inner_total >= a.maxit) { status = 1; break; }
+        ++outer;
+        // inner target: as deep as FP32 allows on the first pass, then only the factor still
+        // missing to the outer tolerance (with a safety margin)
+        double eta = 0.25 * a.rtol * sqrt(bb / rr);
+        if (eta < a.eta) eta = a.eta;
+        if (eta > 0.5) eta = 0.5;
+        // ---- FP32 inner solve A32 e = r (e from zero), dots and norms in FP64
+        int inner = 0;
+        if (!INNER_BICG) {
+            // Chronopoulos-Gear CG, as cg1_kernel, in FP32 storage
+            float* wC = a.w[0]; float* wN = a.w[1]; float* sC = a.s[0]; float* sN = a.s[1];
+            double acc[3] = {0., 0., 0.};
+            for (long long c = t0; c < N; c += T) {
+                float r0 = rC[c];
+                float u0 = __ldg(invD + c) * r0;
+                float y = applyf(Af, c, [&](long long e_) { return __ldg(invD + e_) * rC[e_]; });
+                a.e[c] = 0.f; wC[c] = y; sC[c] = 0.f; a.p[c] = 0.f;
+                acc[0] += (double)r0 * u0; acc[1] += (double)y * u0; acc[2] += (double)r0 * r0;
+            }
+            double tot[3];
+            grid_reduce<3>(grid, acc, a.partials, par, tot);
+            double gamma = tot[0], rr0 = tot[2];
+            double alpha = tot[1] != 0. ? gamma / tot[1] : 0., beta = 0.;
+            double tin2 = eta * eta * rr0;
+            bool stop = !(gamma != 0.);
+            while (!stop) {
+                float al = (float)alpha, be = (float)beta;
+                acc[0] = acc[1] = acc[2] = 0.;
+                for (long long c = t0; c < N; c += T) {
+                    float idc = __ldg(invD + c);
+                    float r0 = rC[c];
+                    float si = wC[c] + be * sC[c];
+                    float pi = idc * r0 + be * a.p[c];
+                    a.e[c] = a.e[c] + al * pi;
+                    float rn = r0 - al * si;
+                    float un = idc * rn;
+                    float y = applyf(Af, c, [&](long long e_) { return __ldg(invD + e_) * (rC[e_] - al * (wC[e_] + be * sC[e_])); });
+                    sN[c] = si; a.p[c] = pi; rN[c] = rn; wN[c] = y;
+                    acc[0] += (double)rn * un; acc[1] += (double)y * un; acc[2] += (double)rn * rn;
+                }
+                grid_reduce<3>(grid, acc, a.partials, par, tot);
+                ++inner;
+                { float* t_ = rC; rC = rN; rN = t_; t_ = wC; wC = wN; wN = t_; t_ = sC; sC = sN; sN = t_; }
+                double gn = tot[0], dn = tot[1], rri = tot[2];
+                double bn = gn / gamma;
+                double den = dn - bn * gn / alpha;
+                if (rri <= tin2 || inner >= a.inner_max || inner_total + inner >= a.maxit || den == 0. || den != den || gn == 0.) stop = true;
+                beta = bn; alpha = gn / den; gamma = gn;
+            }
+        } else {
+            // BiCGStab, right-preconditioned with Jacobi, in FP32 storage
+            float* rp = a.s[0];
+            float* pO = a.p;  float* pNn = a.s[1];
+            float* vO = a.v[0]; float* vNn = a.v[1];
+            double acc[1] = {0.};
+            for (long long c = t0; c < N; c += T) {
+                float r0 = rC[c];
+                a.e[c] = 0.f; rp[c] = r0; pO[c] = 0.f; vO[c] = 0.f;
+                acc[0] += (double)r0 * r0;
+            }
+            double tot[1];
+            grid_reduce<1>(grid, acc, a.partials, par, tot);
+            double rr0 = tot[0], tin2 = eta * eta * rr0;
+            double rho = rr0, rho_old = 1., alpha = 1., omega = 1.;
+            bool fresh = true, stop = !(rr0 > 0.);
+            float* rcur = rC;
+            while (!stop) {
+                double beta = fresh ? 0. : (rho / rho_old) * (alpha / omega);
+                float be = (float)beta, om = (float)omega;
+                double a1[1] = {0.};
+                for (long long c = t0; c < N; c += T) {
+                    auto pn_at = [&](long long e_) -> float {
+                        float rv = rcur[e_];
+                        return fresh ? rv : rv + be * (pO[e_] - om * vO[e_]);
+                    };
+                    float y = applyf(Af, c, [&](long long e_) { return __ldg(invD + e_) * pn_at(e_); });
+                    pNn[c] = pn_at(c); vNn[c] = y;
+                    a1[0] += (double)rp[c] * y;
+                }
+                double t1[1];
+                grid_reduce<1>(grid, a1, a.partials, par, t1);
+                if (t1[0] == 0. || t1[0] != t1[0]) break;
+                alpha = rho / t1[0];
+                float al = (float)alpha;
+                double a2[2] = {0., 0.};
+                for (long long c = t0; c < N; c += T) {
+                    float y = applyf(Af, c, [&](long long e_) { return __ldg(invD + e_) * (rcur[e_] - al * vNn[e_]); });
+                    float sv = rcur[c] - al * vNn[c];
+                    a.t[c] = y;
+                    a2[0] += (double)y * sv; a2[1] += (double)y * y;
+                }
+                double t2[2];
+                grid_reduce<2>(grid, a2, a.partials, par, t2);
+                omega = t2[1] == 0. ? 0. : t2[0] / t2[1];
+                om = (float)omega;
+                double a3[2] = {0., 0.};
+                for (long long c = t0; c < N; c += T) {
+                    float idc = __ldg(invD + c);
+                    float sv = rcur[c] - al * vNn[c];
+                    a.e[c] = a.e[c] + (al * (idc * pNn[c]) + om * (idc * sv));
+                    float rn = sv - om * a.t[c];
+                    rcur[c] = rn;
+                    a3[0] += (double)rn * rp[c]; a3[1] += (double)rn * rn;
+                }
+                double t3[2];
+                grid_reduce<2>(grid, a3, a.partials, par, t3);
+                ++inner;
+                fresh = false;
+                rho_old = rho; rho = t3[0];
+                { float* t_ = pO; pO = pNn; pNn = t_; t_ = vO; vO = vNn; vNn = t_; }
+                if (t3[1] <= tin2 || omega == 0. || inner >= a.inner_max || inner_total + inner >= a.maxit || t3[1] != t3[1]) stop = true;
+            }
+            rC = rcur;
+        }
+        inner_total += inner;
+        // ---- x += e (FP64); the next residual reads x at the neighbours
+        for (long long c = t0; c < N; c += T) a.x[c] = a.x[c] + (double)a.e[c];
+        grid.sync();
+        if (outer > 60) { status = 1; break; }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        a.out->iters[0] = inner_total; a.out->iters[1] = outer; a.out->relres[0] = relres; a.out->status[0] = status;
+    }
+}
+
 // ------------------------------------------------------------------ host side
 static int g_numSM = 0;
 
@@ -650,6 +891,8 @@ static KArgs make_args(const Lat& L, const KspWork& w, const double* b, double* 
     a.t = w.t; a.invD = w.invD; a.partials = w.partials; a.out = w.out;
     a.N = L.N; a.PS = L.PS; a.rtol = rtol; a.maxit = maxit;
     a.project = 0;
+    a.skip_if_ok = nullptr;
+    a.fallbacks = nullptr;
     return a;
 }
 
@@ -706,6 +949,52 @@ int krylov_grid_size(int which) {
         case 2: return coop_grid(cg1_kernel<OpSym>);
         default: return coop_grid(bicgstab_kernel<1, Op7>);
     }
+}
+
+
+int ksp_mixed_sym(const OpSym& A, int method, const double* b, double* x, const Lat& L, const KspWork& w, double rtol, int maxit,
+                  double inner_rtol, cudaStream_t st, int project) {
+    cast_sym_kernel<<<grid_for(L.N, 256), 256, 0, st>>>(A, L.N, w.fA[0], w.fA[1], w.fA[2], w.fA[3], w.finvD);
+    CB_CHECK_LAUNCH();
+    OpSymF Af;
+    Af.aP = w.fA[0]; Af.aE = w.fA[1]; Af.aN = w.fA[2]; Af.aT = w.fA[3];
+    Af.nI = A.nI; Af.nIJ = A.nIJ; Af.gh = A.gh;
+    MxArgs m;
+    m.b = b; m.x = x;
+    m.r[0] = w.fr[0]; m.r[1] = w.fr[1]; m.w[0] = w.fw[0]; m.w[1] = w.fw[1]; m.s[0] = w.fs[0]; m.s[1] = w.fs[1];
+    m.p = w.fp; m.e = w.fe; m.v[0] = w.fv[0]; m.v[1] = w.fv[1]; m.t = w.ft; m.invD = w.finvD;
+    m.partials = w.partials; m.out = w.out; m.N = L.N; m.rtol = rtol; m.maxit = maxit; m.eta = inner_rtol;
+    m.project = project; m.inner_max = 100000;
+    void* params[3] = {const_cast<OpSym*>(&A), &Af, &m};
+    if (method == CAFFE_KSP_CG_JACOBI_INT) {
+        static int G = 0;
+        if (!G) { int nb = 0; cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, mixed_kernel<OpSym, 0>, KB, 0); G = (nb < 1 ? 1 : (nb > 4 ? 4 : nb)) * sm_count(); }
+        CB_CUDA(cudaLaunchCooperativeKernel((const void*)mixed_kernel<OpSym, 0>, dim3(G), dim3(KB), params, 0, st));
+    } else {
+        static int G = 0;
+        if (!G) { int nb = 0; cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, mixed_kernel<OpSym, 1>, KB, 0); G = (nb < 1 ? 1 : (nb > 4 ? 4 : nb)) * sm_count(); }
+        CB_CUDA(cudaLaunchCooperativeKernel((const void*)mixed_kernel<OpSym, 1>, dim3(G), dim3(KB), params, 0, st));
+    }
+    return 0;
+}
+
+int ksp_fallback_sym(const OpSym& A, int method, const double* b, double* x, const Lat& L, const KspWork& w, double rtol, int maxit,
+                     cudaStream_t st, int project, const int* status, int* fallbacks) {
+    // plain FP64 re-solve from zero, executed only when *status (the previous solve's) is non-zero
+    inv_diag_kernel<OpSym><<<grid_for(L.N, 256), 256, 0, st>>>(A, L.N, w.invD);
+    CB_CHECK_LAUNCH();
+    KArgs a = make_args(L, w, b, x, rtol, maxit);
+    a.project = project;
+    a.skip_if_ok = status;
+    a.fallbacks = fallbacks;
+    if (method == CAFFE_KSP_CG_JACOBI_INT) {
+        static int G = 0;
+        if (!G) G = coop_grid(cg1_kernel<OpSym>);
+        return launch_coop(cg1_kernel<OpSym>, G, a, &A, st);
+    }
+    static int G = 0;
+    if (!G) G = coop_grid(bicgstab_kernel<1, OpSym>);
+    return launch_coop(bicgstab_kernel<1, OpSym>, G, a, &A, st);
 }
 
 }  // namespace cb

@@ -51,14 +51,16 @@ struct KspWork {
     double* invD;     // one plane
     double* partials; // grid x 8 doubles
     KspOut* out;      // device
-    // single precision copies for the mixed-precision inner solver
-    float* fr;
-    float* fp[2];
-    float* fq;
-    float* fz;
-    float* fx;
-    float* fA[4];     // aP aE aN aT
+    // single-precision workspace of the mixed-precision solver (halo-padded float cell arrays)
+    float* fr[2];
+    float* fw[2];
+    float* fs[2];
+    float* fp;
+    float* fe;
     float* finvD;
+    float* fA[4];     // aP aE aN aT in FP32
+    float* fv[2];     // extra vectors of the FP32 BiCGStab inner solver
+    float* ft;
 };
 
 int ksp_bicgstab(const Op7& A, int nr, const double* b, double* x, const Lat& L, const KspWork& w, double rtol, int maxit,
@@ -69,9 +71,16 @@ int ksp_bicgstab_sym(const OpSym& A, const double* b, double* x, const Lat& L, c
 int ksp_cg(const OpSym& A, const double* b, double* x, const Lat& L, const KspWork& w, double rtol, int maxit, cudaStream_t st,
            int project = 0);
 int ksp_cg7(const Op7& A, const double* b, double* x, const Lat& L, const KspWork& w, double rtol, int maxit, cudaStream_t st);
-// FP32 CG / BiCGStab inside FP64 iterative refinement on the symmetric operator.
+// FP64 iterative refinement around FP32 inner solves on the symmetric p' operator: CG inner
+// (method CAFFE_KSP_CG_JACOBI, symmetric systems) or BiCGStab inner (ghost rows).
+// inner_rtol: relative reduction each inner solve aims for.  out->iters counts inner
+// iterations; the outer count goes to *outer_iters (device int, may be null).
 int ksp_mixed_sym(const OpSym& A, int method, const double* b, double* x, const Lat& L, const KspWork& w, double rtol, int maxit,
-                  double inner_rtol, cudaStream_t st, int* outer_iters);
+                  double inner_rtol, cudaStream_t st, int project);
+// Plain FP64 re-solve that runs only when *status is non-zero (the fallback of a mixed or
+// learned solve), decided on the device without a host round trip.
+int ksp_fallback_sym(const OpSym& A, int method, const double* b, double* x, const Lat& L, const KspWork& w, double rtol, int maxit,
+                     cudaStream_t st, int project, const int* status, int* fallbacks);
 int krylov_grid_size(int which);
 
 }  // namespace cb

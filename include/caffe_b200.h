@@ -129,6 +129,19 @@ int caffe_ksp7_solve(int nI, int nJ, int nK, const double* coef7, const double* 
 int caffe_ksp7_solve_device(int nI, int nJ, int nK, const double* d_coef7, const double* d_b, double* d_x,
                             int method, double rtol, int maxit, void* stream, int* iters, double* rel_res);
 
+/* Learned preconditioner network (an extension; the reference has no learned component):
+ * a 4-layer 3-D convolutional network with 3x3x3 kernels and 16 channels, BF16 weights and
+ * activations, FP32 accumulation on the tensor cores.  Parameters are FP32, layer by layer:
+ * W[27 taps][16 out][16 in] then b[16]; tap = 9*(dk+1) + 3*(dj+1) + (di+1).  Layer 1 reads
+ * input channels 0 and 1, layer 4 writes output channel 0. */
+int caffe_precond_param_count(void);
+/* Apply the network to a 2-channel input x2 (host, nI*nJ*nK x 2 floats); y receives the
+ * output channel (host, nI*nJ*nK floats). */
+int caffe_precond_net_apply(int nI, int nJ, int nK, const float* params, const float* x2, float* y);
+/* Forward plus backward: y as above and dparams = d(sum dy*y)/d(params) (host arrays). */
+int caffe_precond_net_grad(int nI, int nJ, int nK, const float* params, const float* x2, const float* dy,
+                           float* y, float* dparams);
+
 /* caffe_ksp7_solve_device without any device allocation.  It has no counterpart in the
  * reference.  For callers that cannot call cudaMalloc/cudaFree from inside a solve -- a program
  * whose own allocator already owns nearly all of HBM, or a time loop that cannot take the
