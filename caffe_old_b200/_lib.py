@@ -66,6 +66,9 @@ EXPORTS = (
     "caffe_dev_array", "caffe_dev_stats", "caffe_dev_stream", "caffe_dev_synchronize",
     "caffe_ksp7_solve", "caffe_ksp7_solve_device", "caffe_ksp7_solve_device_noalloc",
     "caffe_precond_param_count", "caffe_precond_net_apply", "caffe_precond_net_grad",
+    "caffe_dev_set_precond", "caffe_dev_get_precond", "caffe_dev_set_precond_mode", "caffe_dev_set_precond_options",
+    "caffe_dev_record_pairs", "caffe_dev_pair_count", "caffe_dev_add_pairs", "caffe_dev_copy_pairs", "caffe_dev_train_precond",
+    "caffe_dev_eval_precond",
 )
 
 
@@ -96,6 +99,16 @@ def lib():
     L.caffe_precond_param_count.restype = ci
     L.caffe_precond_net_apply.argtypes = [ci, ci, ci, vp, vp, vp]
     L.caffe_precond_net_grad.argtypes = [ci, ci, ci, vp, vp, vp, vp, vp]
+    L.caffe_dev_set_precond.argtypes = [vp, vp]
+    L.caffe_dev_get_precond.argtypes = [vp, vp]
+    L.caffe_dev_set_precond_mode.argtypes = [vp, ci]
+    L.caffe_dev_set_precond_options.argtypes = [vp, ci, ci]
+    L.caffe_dev_record_pairs.argtypes = [vp, ci, ci]
+    L.caffe_dev_pair_count.argtypes = [vp]
+    L.caffe_dev_add_pairs.argtypes = [vp, vp, vp, ci]
+    L.caffe_dev_copy_pairs.argtypes = [vp, vp]
+    L.caffe_dev_train_precond.argtypes = [vp, ci, ci, ctypes.c_float, ctypes.c_uint, vp, vp]
+    L.caffe_dev_eval_precond.argtypes = [vp, ci, vp]
     _lib = L
     return L
 

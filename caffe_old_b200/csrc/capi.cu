@@ -11,6 +11,8 @@
 #include "flow.cuh"
 #include "krylov.cuh"
 #include "ib.cuh"
+#include "cnn.cuh"
+#include "learned.cuh"
 
 namespace cb {
 
@@ -33,6 +35,12 @@ struct StepAcc {
     double continuity;
     unsigned long long courant_bits;
 };
+
+// one training pair (b, x) of a p' solve, rounded to FP32
+__global__ void pair_cast_kernel(long long N, const double* b, const double* x, float* pb, float* px) {
+    long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (c < N) { pb[c] = (float)b[c]; px[c] = (float)x[c]; }
+}
 
 __global__ void acc_kernel(const KspOut* o, StepAcc* acc, int kind, int nr) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
@@ -112,6 +120,17 @@ struct caffe_dev {
     double* pb = nullptr;
     KspWork kw;
     IbState ibs;
+    // learned preconditioner of the p' solve
+    LearnedWork lw;
+    bool haveLearned = false;
+    int netMode = NET_MODE_NETWORK;
+    // training pairs (b, x) of p' solves, FP32 halo-padded planes
+    float* pairB = nullptr;
+    float* pairX = nullptr;
+    int pairCap = 0, pairCount = 0;
+    int pairSnapshots = 0;       // intermediate-iterate pairs per recorded solve
+    double* snapX = nullptr;     // iterate of a truncated re-solve (one FP64 cell plane)
+    bool recording = false;
     // reductions and statistics
     double* chunkMax = nullptr;
     StepAcc* acc = nullptr;
@@ -135,6 +154,33 @@ struct caffe_dev {
     double* cell(int planes) {
         double* b = dalloc<double>((size_t)L.PS * planes);
         return b ? b + L.H : nullptr;
+    }
+    static void* alloc_cb(size_t bytes, void* ctx) { return static_cast<caffe_dev*>(ctx)->dalloc<char>(bytes); }
+    int ensure_learned() {
+        if (haveLearned) return 0;
+        if (learned_alloc(lw, L, &caffe_dev::alloc_cb, this)) return 1;
+        haveLearned = true;
+        return 0;
+    }
+    int ensure_pairs(int cap) {
+        if (cap <= pairCap) return 0;
+        size_t plane = (size_t)L.PS;
+        float *nb = nullptr, *nx = nullptr;
+        if (cudaMalloc(&nb, sizeof(float) * plane * cap) != cudaSuccess || cudaMalloc(&nx, sizeof(float) * plane * cap) != cudaSuccess) {
+            cudaFree(nb); cudaFree(nx);
+            set_error("training-pair allocation failed");
+            return 1;
+        }
+        cudaMemsetAsync(nb, 0, sizeof(float) * plane * cap, st);
+        cudaMemsetAsync(nx, 0, sizeof(float) * plane * cap, st);
+        if (pairCount > 0) {
+            cudaMemcpyAsync(nb, pairB, sizeof(float) * plane * pairCount, cudaMemcpyDeviceToDevice, st);
+            cudaMemcpyAsync(nx, pairX, sizeof(float) * plane * pairCount, cudaMemcpyDeviceToDevice, st);
+        }
+        cudaStreamSynchronize(st);
+        cudaFree(pairB); cudaFree(pairX);
+        pairB = nb; pairX = nx; pairCap = cap;
+        return 0;
     }
     float* fcell() {
         float* b = dalloc<float>((size_t)L.PS);
@@ -188,6 +234,8 @@ struct caffe_dev {
         for (auto& e : ev) if (e) cudaEventDestroy(e);
         for (auto& e : evP) if (e) cudaEventDestroy(e);
         for (auto& e : evM) if (e) cudaEventDestroy(e);
+        learned_free_host(lw);
+        cudaFree(pairB); cudaFree(pairX);
         if (accHost) cudaFreeHost(accHost);
         if (st) cudaStreamDestroy(st);
     }
@@ -258,6 +306,7 @@ int fill(caffe_dev* h, double* dst, int planes, double a, double b = 0., double 
 // deepest relative residual reduction an FP32 inner solve of the mixed-precision form aims for
 // (later inner solves only aim for the factor still missing)
 constexpr double MIXED_INNER_RTOL = 1e-6;
+constexpr double LEARNED_INNER_RTOL = 1e-5;
 
 int p_singular(const caffe_dev* h) {
     if (h->ib) return 0;
@@ -297,7 +346,16 @@ int ph_solve_pcorr(caffe_dev* h) {
     int method = h->cs.p_method;
     if (method == CAFFE_KSP_CG_JACOBI && !sym) method = CAFFE_KSP_BICGSTAB_JACOBI;   // ghost rows are not symmetric
     int project = p_singular(h);
-    if (h->cs.p_form == CAFFE_P_MIXED) {
+    if (h->cs.p_form == CAFFE_P_LEARNED || h->cs.p_form == CAFFE_P_LEARNED_MIXED) {
+        // FP64 refinement around an FP32 flexible Krylov solve preconditioned through the level
+        // pyramid and the network; the plain FP64 solve re-runs on the device if it does not
+        // reach the tolerance
+        if (h->ensure_learned()) return 1;
+        rc = learned_solve(h->lw, A, h->ib ? h->status : nullptr, h->pb, h->pc, h->L, h->cs.p_rtol, h->cs.maxit, LEARNED_INNER_RTOL,
+                           project, h->netMode, h->kw.out, h->st);
+        if (!rc) rc = ksp_fallback_sym(A, method, h->pb, h->pc, h->L, h->kw, h->cs.p_rtol, h->cs.maxit, h->st, 0,
+                                       &h->kw.out->status[0], &h->acc->fallbacks);
+    } else if (h->cs.p_form == CAFFE_P_MIXED) {
         // FP32 inner solves inside FP64 refinement; the plain FP64 solve re-runs on the device
         // when the refinement does not reach the tolerance
         rc = ksp_mixed_sym(A, method, h->pb, h->pc, h->L, h->kw, h->cs.p_rtol, h->cs.maxit, MIXED_INNER_RTOL, h->st, project);
@@ -311,6 +369,24 @@ int ph_solve_pcorr(caffe_dev* h) {
     if (rc) return rc;
     acc_kernel<<<1, 32, 0, h->st>>>(h->kw.out, h->acc, 1, 1);
     CB_CHECK_LAUNCH();
+    if (h->recording && h->pairCount < h->pairCap) {
+        // (b, x*) of this solve, then (b - A x_k, x* - x_k) for iterates x_k of truncated plain
+        // re-solves after 8, 32, 128, ... iterations
+        size_t slot = (size_t)h->pairCount * h->L.PS + h->L.H;
+        pair_cast_kernel<<<grid_for(h->L.N, 256), 256, 0, h->st>>>(h->L.N, h->pb, h->pc, h->pairB + slot, h->pairX + slot);
+        CB_CHECK_LAUNCH();
+        ++h->pairCount;
+        int kIt = 8;
+        for (int q = 0; q < h->pairSnapshots && h->pairCount < h->pairCap; ++q, kIt *= 4) {
+            if (!h->snapX && !(h->snapX = h->cell(1))) { set_error("allocation failed"); return 1; }
+            rc = method == CAFFE_KSP_CG_JACOBI ? ksp_cg(A, h->pb, h->snapX, h->L, h->kw, 0., kIt, h->st, 0)
+                                               : ksp_bicgstab_sym(A, h->pb, h->snapX, h->L, h->kw, 0., kIt, h->st, 0);
+            if (rc) return rc;
+            slot = (size_t)h->pairCount * h->L.PS + h->L.H;
+            if (learned_snapshot_pair(A, h->L, h->pb, h->pc, h->snapX, h->pairB + slot, h->pairX + slot, h->st)) return 1;
+            ++h->pairCount;
+        }
+    }
     return 0;
 }
 int ph_correct(caffe_dev* h) {
@@ -712,6 +788,125 @@ int caffe_dev_synchronize(caffe_dev* h) {
     if (!h) { set_error("handle is NULL"); return 1; }
     CB_CUDA(cudaStreamSynchronize(h->st));
     return 0;
+}
+
+int caffe_dev_set_precond(caffe_dev* h, const float* params) {
+    g_err.clear();
+    if (!h) { set_error("handle is NULL"); return 1; }
+    CB_CUDA(cudaSetDevice(h->device));
+    if (h->ensure_learned()) return 1;
+    if (!params) { h->lw.haveParams = false; return 0; }
+    if (!h->lw.weights) { set_error("lattice too small for the level pyramid of the learned preconditioner"); return 1; }
+    CB_CUDA(cudaMemcpyAsync(h->lw.weights->params, params, sizeof(float) * NET_PARAMS, cudaMemcpyHostToDevice, h->st));
+    if (net_pack_weights(*h->lw.weights, h->st)) return 1;
+    CB_CUDA(cudaStreamSynchronize(h->st));
+    h->lw.haveParams = true;
+    return 0;
+}
+
+int caffe_dev_get_precond(caffe_dev* h, float* params) {
+    g_err.clear();
+    if (!h || !params) { set_error("NULL argument"); return 1; }
+    if (!h->haveLearned || !h->lw.haveParams || !h->lw.weights) { set_error("no preconditioner parameters on this handle"); return 1; }
+    CB_CUDA(cudaMemcpyAsync(params, h->lw.weights->params, sizeof(float) * NET_PARAMS, cudaMemcpyDeviceToHost, h->st));
+    CB_CUDA(cudaStreamSynchronize(h->st));
+    return 0;
+}
+
+int caffe_dev_set_precond_mode(caffe_dev* h, int mode) {
+    g_err.clear();
+    if (!h) { set_error("handle is NULL"); return 1; }
+    if (mode < NET_MODE_JACOBI || mode > NET_MODE_LEVELS) { set_error("unknown preconditioner mode"); return 1; }
+    h->netMode = mode;
+    return 0;
+}
+
+int caffe_dev_set_precond_options(caffe_dev* h, int inner_method, int net_from_level) {
+    g_err.clear();
+    if (!h) { set_error("handle is NULL"); return 1; }
+    if (inner_method < LEARN_INNER_AUTO || inner_method > LEARN_INNER_BICGSTAB || net_from_level < 1) { set_error("invalid options"); return 1; }
+    CB_CUDA(cudaSetDevice(h->device));
+    if (h->ensure_learned()) return 1;
+    h->lw.inner = inner_method;
+    h->lw.netFrom = net_from_level;
+    return 0;
+}
+
+int caffe_dev_record_pairs(caffe_dev* h, int capacity, int snapshots) {
+    g_err.clear();
+    if (!h || capacity < 0 || snapshots < 0 || snapshots > 8) { set_error("invalid arguments"); return 1; }
+    CB_CUDA(cudaSetDevice(h->device));
+    h->pairSnapshots = snapshots;
+    if (capacity == 0) { h->recording = false; return 0; }
+    if (h->ensure_pairs(capacity)) return 1;
+    h->recording = true;
+    return 0;
+}
+
+int caffe_dev_pair_count(caffe_dev* h) {
+    if (!h) { set_error("handle is NULL"); return -1; }
+    return h->pairCount;
+}
+
+int caffe_dev_add_pairs(caffe_dev* h, const float* b_pairs, const float* x_pairs, int n_pairs) {
+    g_err.clear();
+    if (!h || !b_pairs || !x_pairs || n_pairs < 0) { set_error("invalid arguments"); return 1; }
+    CB_CUDA(cudaSetDevice(h->device));
+    if (h->ensure_pairs(h->pairCount + n_pairs)) return 1;
+    const Lat& L = h->L;
+    for (int q = 0; q < n_pairs; ++q) {
+        size_t slot = (size_t)h->pairCount * L.PS + L.H;
+        CB_CUDA(cudaMemcpyAsync(h->pairB + slot, b_pairs + (size_t)q * L.N, sizeof(float) * L.N, cudaMemcpyHostToDevice, h->st));
+        CB_CUDA(cudaMemcpyAsync(h->pairX + slot, x_pairs + (size_t)q * L.N, sizeof(float) * L.N, cudaMemcpyHostToDevice, h->st));
+        ++h->pairCount;
+    }
+    CB_CUDA(cudaStreamSynchronize(h->st));
+    return 0;
+}
+
+int caffe_dev_copy_pairs(caffe_dev* dst, caffe_dev* src) {
+    g_err.clear();
+    if (!dst || !src) { set_error("handle is NULL"); return 1; }
+    if (dst->device != src->device || dst->L.nI != src->L.nI || dst->L.nJ != src->L.nJ || dst->L.nK != src->L.nK) {
+        set_error("pairs can only be copied between handles with the same lattice on the same device");
+        return 1;
+    }
+    if (src->pairCount == 0) return 0;
+    CB_CUDA(cudaSetDevice(dst->device));
+    CB_CUDA(cudaStreamSynchronize(src->st));
+    if (dst->ensure_pairs(dst->pairCount + src->pairCount)) return 1;
+    size_t plane = (size_t)dst->L.PS;
+    CB_CUDA(cudaMemcpyAsync(dst->pairB + (size_t)dst->pairCount * plane, src->pairB, sizeof(float) * plane * src->pairCount,
+                            cudaMemcpyDeviceToDevice, dst->st));
+    CB_CUDA(cudaMemcpyAsync(dst->pairX + (size_t)dst->pairCount * plane, src->pairX, sizeof(float) * plane * src->pairCount,
+                            cudaMemcpyDeviceToDevice, dst->st));
+    CB_CUDA(cudaStreamSynchronize(dst->st));
+    dst->pairCount += src->pairCount;
+    return 0;
+}
+
+int caffe_dev_train_precond(caffe_dev* h, int steps, int batch, float lr, unsigned seed, float* params_inout, float* loss_hist) {
+    g_err.clear();
+    if (!h || !params_inout || steps < 0 || batch < 1) { set_error("invalid arguments"); return 1; }
+    if (h->pairCount < 1) { set_error("no training pairs on this handle"); return 1; }
+    CB_CUDA(cudaSetDevice(h->device));
+    if (h->ensure_learned()) return 1;
+    if (!h->lw.weights) { set_error("lattice too small for the level pyramid of the learned preconditioner"); return 1; }
+    CB_CUDA(cudaMemcpyAsync(h->lw.weights->params, params_inout, sizeof(float) * NET_PARAMS, cudaMemcpyHostToDevice, h->st));
+    int rc = learned_train(h->lw, h->pOp(), h->ib ? h->status : nullptr, h->L, h->pairB, h->pairX, h->pairCount, steps, batch, lr, seed,
+                           loss_hist, h->st);
+    if (rc) return rc;
+    CB_CUDA(cudaMemcpy(params_inout, h->lw.weights->params, sizeof(float) * NET_PARAMS, cudaMemcpyDeviceToHost));
+    return 0;
+}
+
+int caffe_dev_eval_precond(caffe_dev* h, int mode, float* loss) {
+    g_err.clear();
+    if (!h || !loss) { set_error("NULL argument"); return 1; }
+    if (mode < NET_MODE_JACOBI || mode > NET_MODE_LEVELS) { set_error("unknown preconditioner mode"); return 1; }
+    CB_CUDA(cudaSetDevice(h->device));
+    if (h->ensure_learned()) return 1;
+    return learned_eval(h->lw, h->pOp(), h->ib ? h->status : nullptr, h->L, h->pairB, h->pairX, h->pairCount, mode, loss, h->st);
 }
 
 int caffe_ksp7_solve_device(int nI, int nJ, int nK, const double* d_coef7, const double* d_b, double* d_x, int method, double rtol,

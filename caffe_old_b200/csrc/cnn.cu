@@ -126,7 +126,10 @@ template <int EPI>
 __global__ void __launch_bounds__(128) conv3d_tc_kernel(Lat L, const __nv_bfloat16* __restrict__ in,
                                                         const __nv_bfloat16* __restrict__ wpack, const float* __restrict__ bias,
                                                         __nv_bfloat16* out_bf, float* out_f, long long out_stride,
-                                                        const __nv_bfloat16* __restrict__ mask_act, int KC, int* err) {
+                                                        const __nv_bfloat16* __restrict__ mask_act, int KC, int* err,
+                                                        const int* __restrict__ skip) {
+    // a solve that has already converged turns its remaining launches into no-ops (uniform)
+    if (skip && *skip) return;
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     // 1 KiB-align the dynamic region
     unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -238,8 +241,12 @@ __global__ void __launch_bounds__(128) conv3d_tc_kernel(Lat L, const __nv_bfloat
 size_t conv_smem_bytes() { return 1024 + W_BYTES + NBUF * BUF_BYTES; }
 
 int launch_conv3d(const Lat& L, int epi, const __nv_bfloat16* in, const __nv_bfloat16* wpack, const float* bias, __nv_bfloat16* out_bf,
-                  float* out_f, const __nv_bfloat16* mask_act, int* err, cudaStream_t st) {
-    const int KC = 16;
+                  float* out_f, const __nv_bfloat16* mask_act, int* err, cudaStream_t st, const int* skip) {
+    // k-planes per CTA: up to 16 (one staged plane serves three output planes), fewer on small
+    // lattices so that the grid still covers the SMs twice
+    const long long gxy = (long long)((L.nI + TI - 1) / TI) * ((L.nJ + TJ - 1) / TJ);
+    const long long kc = gxy * L.nK / 296;
+    const int KC = (int)(kc < 1 ? 1 : (kc > 16 ? 16 : kc));
     dim3 grid((L.nI + TI - 1) / TI, (L.nJ + TJ - 1) / TJ, (L.nK + KC - 1) / KC);
     size_t smem = conv_smem_bytes();
     static bool attr = false;
@@ -249,9 +256,9 @@ int launch_conv3d(const Lat& L, int epi, const __nv_bfloat16* in, const __nv_bfl
         CB_CUDA(cudaFuncSetAttribute(conv3d_tc_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         attr = true;
     }
-    if (epi == 0) conv3d_tc_kernel<0><<<grid, 128, smem, st>>>(L, in, wpack, bias, out_bf, out_f, 16, mask_act, KC, err);
-    else if (epi == 1) conv3d_tc_kernel<1><<<grid, 128, smem, st>>>(L, in, wpack, bias, out_bf, out_f, 16, mask_act, KC, err);
-    else conv3d_tc_kernel<2><<<grid, 128, smem, st>>>(L, in, wpack, bias, out_bf, out_f, 16, mask_act, KC, err);
+    if (epi == 0) conv3d_tc_kernel<0><<<grid, 128, smem, st>>>(L, in, wpack, bias, out_bf, out_f, 16, mask_act, KC, err, skip);
+    else if (epi == 1) conv3d_tc_kernel<1><<<grid, 128, smem, st>>>(L, in, wpack, bias, out_bf, out_f, 16, mask_act, KC, err, skip);
+    else conv3d_tc_kernel<2><<<grid, 128, smem, st>>>(L, in, wpack, bias, out_bf, out_f, 16, mask_act, KC, err, skip);
     CB_CHECK_LAUNCH();
     return 0;
 }

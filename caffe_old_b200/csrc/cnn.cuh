@@ -18,8 +18,9 @@ constexpr int NET_PARAMS = NET_LAYERS * NET_LAYER_PARAMS;
 
 size_t conv_smem_bytes();
 // epi 0: bias + ReLU -> bf16;  1: bias -> FP32 channel 0;  2: times (mask_act > 0) -> bf16
+// skip: optional device flag; while it holds non-zero the launch does nothing
 int launch_conv3d(const Lat& L, int epi, const __nv_bfloat16* in, const __nv_bfloat16* wpack, const float* bias, __nv_bfloat16* out_bf,
-                  float* out_f, const __nv_bfloat16* mask_act, int* err, cudaStream_t st);
+                  float* out_f, const __nv_bfloat16* mask_act, int* err, cudaStream_t st, const int* skip = nullptr);
 
 // Device buffers of one network applied on one lattice.
 struct NetBuffers {
@@ -35,9 +36,13 @@ struct NetBuffers {
 };
 
 int net_alloc(NetBuffers& nb, const Lat& L, void* (*alloc)(size_t, void*), void* ctx);
+// activations of another lattice that share the weights, gradient and error flag of `owner`
+int net_alloc_shared(NetBuffers& nb, const Lat& L, const NetBuffers& owner, void* (*alloc)(size_t, void*), void* ctx);
 int net_pack_weights(NetBuffers& nb, cudaStream_t st);
 // forward from the packed 16-channel input already in act[0]; output in nb.y
 int net_forward(NetBuffers& nb, cudaStream_t st);
+// same, every launch a no-op while *skip is non-zero
+int net_forward_if(NetBuffers& nb, const int* skip, cudaStream_t st);
 // backward for dL/dy (FP32, N): accumulates dL/dparams into nb.grad
 int net_backward(NetBuffers& nb, const float* dy, cudaStream_t st);
 // act[0] from a 2-channel FP32 input laid out [N][2]

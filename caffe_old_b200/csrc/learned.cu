@@ -1,0 +1,1159 @@
+// Learned preconditioner in a flexible Krylov solve, and its training on the device.
+//
+// Preconditioner (additive multilevel with a learned level operator):
+//   M(r) = D^-1 r + P_1 w_1,   w_l = gain_l s y_l + P_(l+1) w_(l+1),   y_l = net(u_l / s, mask_l, l),
+//   u_1 = R_1 (D^-1 r),  u_(l+1) = R_(l+1) u_l,
+// on active cells (D^-1 r on ghost rows, 0 on inactive cells).  Level l halves every
+// direction of level l-1 that is longer than one cell; P is cell-centred trilinear
+// prolongation and R = P^T scaled to a cell average; gain_l = 4^l is the factor by which the
+// inverse of the Jacobi-scaled operator grows per halving for the modes that level
+// resolves; s is the RMS of D^-1 r over the active cells.  One set of network weights (the
+// 4-layer tensor-core CNN of cnn.cu) serves every level; its input carries the restricted
+// residual, the fraction of active cells and a constant level channel.  The network never
+// runs on the cell lattice itself: on the 25M-cell lattice level 1 holds 1/8 of the cells, so
+// the network costs a fraction of one fine-lattice sweep while the pyramid reaches the
+// smooth error that a 9^3 receptive field cannot.  Two reference forms use the same code:
+// JACOBI (no levels: M = D^-1, the method without the network) and LEVELS (y_l = u_l / s,
+// the pyramid with an identity in place of the network).
+//
+// Solve (learned + mixed precision): FP64 iterative refinement (true residual, update and
+// convergence test in FP64) around an FP32 flexible Krylov solve that tolerates a
+// preconditioner that changes from one application to the next:
+//  * flexible CG (Notay 2000, truncated to one previous direction) for the symmetric p' matrix:
+//      p_k = z_k - beta_k p_{k-1},  beta_k = (z_k, q_{k-1}) / (p_{k-1}, q_{k-1}),
+//      q_k = A p_k,  alpha_k = (p_k, r_k) / (p_k, q_k),  x += alpha p,  r -= alpha q;
+//  * right-preconditioned BiCGStab when immersed-boundary ghost rows make the matrix
+//    non-symmetric (x and r stay consistent for any M).
+// Each iteration is a short fixed sequence of kernels; their dot products go through block
+// partials and a one-block finaliser into a device-side scalar record, so the host never
+// waits inside an iteration.  Once the record's `done` flag is set every later kernel returns
+// at entry; the host looks at the flag every few iterations.
+//
+// Training: pairs (b, x*) with A x* = b from the plain solver; loss per pair
+//   L = ||M(b) - x*||^2_E / ||x*||^2_E
+// in the energy norm of -A (the p' matrix is negative definite; with immersed-boundary cells,
+// of its active-cell block), gradient dL/dz = 2 (-A)(z - x*) / ||x*||^2_E, carried through the
+// prolongations (adjoint: P^T) to every level's network output and back-propagated by the
+// tensor-core backward pass; Adam update.
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/caffe_b200.h"
+#include "common.cuh"
+#include "cnn.cuh"
+#include "krylov.cuh"
+#include "learned.cuh"
+
+namespace cb {
+
+namespace {
+
+constexpr int LB = 256;
+constexpr int MAXP = 2048;   // partial slots (blocks) per reduction
+
+struct Scal {
+    double rr0, rr, tin2;       // inner: initial and current ||r||^2, stop threshold
+    double s;                   // RMS of D^-1 r over active cells
+    double zq, pq, pr;          // (z, q_prev), (p, q), (p, r)
+    double alpha, beta;
+    double bb, tol2, rr64;      // outer: ||b||^2, tolerance, current true ||r||^2
+    double nact;
+    double loss;
+    double rho, omega, rv, ts, tt;   // flexible BiCGStab: (rhat, r), omega, (rhat, v), (t, s), (t, t)
+    int done;                   // inner solve finished
+    int odone;                  // outer solve finished
+    int iters, outer, status, first;
+};
+
+__device__ __forceinline__ void block_sums(double* v, int K, double* part) {
+    __shared__ double sm[4][LB / 32];
+    for (int q = 0; q < K; ++q)
+        for (int off = 16; off > 0; off >>= 1) v[q] += __shfl_xor_sync(0xffffffffu, v[q], off);
+    int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0)
+        for (int q = 0; q < K; ++q) sm[q][w] = v[q];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int q = 0; q < K; ++q) {
+            double t = 0.;
+            for (int u = 0; u < LB / 32; ++u) t += sm[q][u];
+            part[(size_t)blockIdx.x * 4 + q] = t;
+        }
+    }
+}
+
+// one block: totals of K partial streams over nblk blocks, in a fixed order
+__device__ __forceinline__ void totals(const double* part, int nblk, int K, double* out) {
+    __shared__ double sm[4][LB];
+    for (int q = 0; q < K; ++q) {
+        double t = 0.;
+        for (int b = threadIdx.x; b < nblk; b += blockDim.x) t += part[(size_t)b * 4 + q];
+        sm[q][threadIdx.x] = t;
+    }
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s)
+            for (int q = 0; q < K; ++q) sm[q][threadIdx.x] += sm[q][threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int q = 0; q < K; ++q) out[q] = sm[q][0];
+    __syncthreads();
+}
+
+inline int nblocks(long long N) {
+    long long b = (N + LB - 1) / LB;
+    return (int)(b < MAXP ? b : MAXP);
+}
+
+__device__ __forceinline__ bool is_active(const uint8_t* st, long long c) { return st == nullptr || st[c] == ST_ACTIVE; }
+__device__ __forceinline__ bool is_inactive(const uint8_t* st, long long c) { return st != nullptr && st[c] == ST_INACTIVE; }
+
+// 4-cell vector access (cell arrays start 16-byte aligned: the halo H is a multiple of 32)
+__device__ __forceinline__ float4 ld4(const float* p, long long q) { return reinterpret_cast<const float4*>(p)[q]; }
+__device__ __forceinline__ void st4(float* p, long long q, const float (&v)[4]) {
+    reinterpret_cast<float4*>(p)[q] = make_float4(v[0], v[1], v[2], v[3]);
+}
+__device__ __forceinline__ void un4(const float4& v, float (&a)[4]) { a[0] = v.x; a[1] = v.y; a[2] = v.z; a[3] = v.w; }
+__device__ __forceinline__ void st_flags4(const uint8_t* st, long long q, uint8_t (&f)[4]) {
+    if (!st) { f[0] = f[1] = f[2] = f[3] = ST_ACTIVE; return; }
+    uchar4 v = reinterpret_cast<const uchar4*>(st)[q];
+    f[0] = v.x; f[1] = v.y; f[2] = v.z; f[3] = v.w;
+}
+
+// ---------------------------------------------------------------- outer (FP64) kernels
+// r = b - A x (FP64), r32 = float(r), partial ||r||^2
+__global__ void __launch_bounds__(LB) outer_residual_kernel(OpSym A, long long N, const double* b, const double* x, float* r32,
+                                                            double* part, const Scal* S) {
+    if (S->odone) return;
+    double v[1] = {0.};
+    for (long long c = blockIdx.x * (long long)LB + threadIdx.x; c < N; c += (long long)gridDim.x * LB) {
+        double y = __ldg(A.aP + c) * x[c] + __ldg(A.aE + c) * x[c + 1] + __ldg(A.aE + c - 1) * x[c - 1]
+                   + __ldg(A.aN + c) * x[c + A.nI] + __ldg(A.aN + c - A.nI) * x[c - A.nI]
+                   + __ldg(A.aT + c) * x[c + A.nIJ] + __ldg(A.aT + c - A.nIJ) * x[c - A.nIJ];
+        if (A.gh.n > 0) {
+            uint32_t w = __ldg(A.gh.bits + (c >> 5));
+            if ((w >> (c & 31)) & 1u) {
+                int lo = 0, hi = A.gh.n;
+                while (lo < hi) { int mid = (lo + hi) >> 1; if (__ldg(A.gh.cell + mid) < c) lo = mid + 1; else hi = mid; }
+                double s = 0.;
+                for (int m = 0; m < 9; ++m) { int col = __ldg(A.gh.col + 9 * lo + m); if (col >= 0) s += __ldg(A.gh.val + 9 * lo + m) * x[col]; }
+                y = s;
+            }
+        }
+        double r = b[c] - y;
+        r32[c] = (float)r;
+        v[0] += r * r;
+    }
+    block_sums(v, 1, part);
+}
+
+__global__ void outer_check_kernel(const double* part, int nblk, Scal* S, int max_outer) {
+    if (S->odone) return;
+    double t[1];
+    totals(part, nblk, 1, t);
+    if (threadIdx.x == 0) {
+        S->rr64 = t[0];
+        if (S->outer == 0 && S->first) { S->bb = t[0]; S->first = 0; }
+        bool conv = t[0] <= S->tol2 || !(S->bb > 0.);
+        if (t[0] != t[0]) { S->status = 3; conv = true; }
+        if (!conv && S->outer >= max_outer) { S->status = 1; conv = true; }
+        if (conv) S->odone = 1;
+        S->done = S->odone;   // no inner solve when the outer one is finished
+        S->outer += conv ? 0 : 1;
+    }
+}
+
+__global__ void outer_update_kernel(long long N, double* x, const float* e, const Scal* S) {
+    if (S->odone) return;
+    long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (c < N) x[c] = x[c] + (double)e[c];
+}
+
+// ---------------------------------------------------------------- inner flexible CG (FP32)
+// start of an inner solve: e = 0, p = q = 0, ||r||^2 and ||D^-1 r||^2 over active cells
+__global__ void __launch_bounds__(LB) inner_start_kernel(long long N, const float* r, const float* invD, const uint8_t* st, float* e,
+                                                         float* p, float* q, double* part, const Scal* S) {
+    if (S->done) return;
+    double v[3] = {0., 0., 0.};
+    for (long long c = blockIdx.x * (long long)LB + threadIdx.x; c < N; c += (long long)gridDim.x * LB) {
+        float rv = r[c];
+        e[c] = 0.f; p[c] = 0.f; q[c] = 0.f;
+        double u = (double)__ldg(invD + c) * rv;
+        v[0] += (double)rv * rv;
+        if (is_active(st, c)) { v[1] += u * u; v[2] += 1.; }
+    }
+    block_sums(v, 3, part);
+}
+
+__global__ void inner_start_finish_kernel(const double* part, int nblk, Scal* S, double eta) {
+    if (S->done) return;
+    double t[3];
+    totals(part, nblk, 3, t);
+    if (threadIdx.x == 0) {
+        S->rr0 = t[0]; S->rr = t[0];
+        S->tin2 = eta * eta * t[0];
+        S->nact = t[2];
+        S->s = t[2] > 0. ? sqrt(t[1] / t[2]) : 1.;
+        if (!(S->s > 0.)) S->s = 1.;
+        S->alpha = 0.; S->beta = 0.; S->pq = 1.;
+        S->done = !(t[0] > 0.);
+    }
+}
+
+// ---------------------------------------------------------------- level pyramid
+// Cell-centred trilinear prolongation, per direction: fine cell f takes 3/4 of coarse cell
+// f/2 and 1/4 of its other neighbour (f/2 - 1 for even f, f/2 + 1 for odd f), clamped to the
+// lattice.  A direction of one cell is not coarsened (both weights land on cell 0).
+struct Dims3 {
+    int n0, n1, n2;
+};
+__device__ __forceinline__ int pclamp(int v, int n) { return v < 0 ? 0 : (v >= n ? n - 1 : v); }
+__device__ __forceinline__ float rweight(int f, int I, int nc) {
+    int J = pclamp((f & 1) ? (f >> 1) + 1 : (f >> 1) - 1, nc);
+    return ((f >> 1) == I ? 0.75f : 0.f) + (J == I ? 0.25f : 0.f);
+}
+__device__ __forceinline__ float rweight_in(int f, int nf, int I, int nc) { return (f >= 0 && f < nf) ? rweight(f, I, nc) : 0.f; }
+
+// out[I] = scale * (P^T v)[I],  v(f) = (fin ? fin[f] : 1) * (invD ? invD[f] : 1) * (active(f) if st)
+// optional: out2 = mul2 * s * out; act0 row (out / s, mask, level channel) for the network.
+// One CTA owns RCI x RCJ x RCK coarse cells: it stages the (2 RCI + 2) x (2 RCJ + 2) x
+// (2 RCK + 2) fine cells they draw on in shared memory once, then applies the separable
+// weights along i, j and k in three passes.
+constexpr int RCI = 32, RCJ = 4, RCK = 4;
+constexpr int RFI = 2 * RCI + 2, RFJ = 2 * RCJ + 2, RFK = 2 * RCK + 2;
+
+__global__ void __launch_bounds__(256) restrict_kernel(Dims3 fd, Dims3 cd, const float* fin, const float* invD, const uint8_t* st,
+                                                       float scale, float* out, float* out2, float mul2, __nv_bfloat16* act0,
+                                                       const float* maskc, float chan, const Scal* S) {
+    if (S && S->done) return;
+    __shared__ float s0[RFK][RFJ][RFI];
+    __shared__ float t1[RFK][RFJ][RCI];
+    __shared__ float t2[RFK][RCJ][RCI];
+    const int I0 = blockIdx.x * RCI, J0 = blockIdx.y * RCJ, K0 = blockIdx.z * RCK;
+    const int fi0 = 2 * I0 - 1, fj0 = 2 * J0 - 1, fk0 = 2 * K0 - 1;
+    const unsigned fsJ = (unsigned)fd.n0, fsK = (unsigned)fd.n0 * (unsigned)fd.n1;
+    for (int u = threadIdx.x; u < RFI * RFJ * RFK; u += blockDim.x) {
+        int li = u % RFI, lj = (u / RFI) % RFJ, lk = u / (RFI * RFJ);
+        int fi = fi0 + li, fj = fj0 + lj, fk = fk0 + lk;
+        float v = 0.f;
+        if (fi >= 0 && fi < fd.n0 && fj >= 0 && fj < fd.n1 && fk >= 0 && fk < fd.n2) {
+            unsigned f = (unsigned)fk * fsK + (unsigned)fj * fsJ + (unsigned)fi;
+            if (!st || st[f] == ST_ACTIVE) {
+                v = fin ? fin[f] : 1.f;
+                if (invD) v *= __ldg(invD + f);
+            }
+        }
+        s0[lk][lj][li] = v;
+    }
+    __syncthreads();
+    for (int u = threadIdx.x; u < RFK * RFJ * RCI; u += blockDim.x) {
+        int ci = u % RCI, lj = (u / RCI) % RFJ, lk = u / (RCI * RFJ);
+        int I = I0 + ci;
+        float a = 0.f;
+#pragma unroll
+        for (int m = 0; m < 4; ++m) a += rweight_in(2 * I - 1 + m, fd.n0, I, cd.n0) * s0[lk][lj][2 * ci + m];
+        t1[lk][lj][ci] = a;
+    }
+    __syncthreads();
+    for (int u = threadIdx.x; u < RFK * RCJ * RCI; u += blockDim.x) {
+        int ci = u % RCI, cj = (u / RCI) % RCJ, lk = u / (RCI * RCJ);
+        int J = J0 + cj;
+        float a = 0.f;
+#pragma unroll
+        for (int m = 0; m < 4; ++m) a += rweight_in(2 * J - 1 + m, fd.n1, J, cd.n1) * t1[lk][2 * cj + m][ci];
+        t2[lk][cj][ci] = a;
+    }
+    __syncthreads();
+    for (int u = threadIdx.x; u < RCK * RCJ * RCI; u += blockDim.x) {
+        int ci = u % RCI, cj = (u / RCI) % RCJ, ck = u / (RCI * RCJ);
+        int I = I0 + ci, J = J0 + cj, K = K0 + ck;
+        if (I >= cd.n0 || J >= cd.n1 || K >= cd.n2) continue;
+        float acc = 0.f;
+#pragma unroll
+        for (int m = 0; m < 4; ++m) acc += rweight_in(2 * K - 1 + m, fd.n2, K, cd.n2) * t2[2 * ck + m][cj][ci];
+        acc *= scale;
+        unsigned c = ((unsigned)K * (unsigned)cd.n1 + (unsigned)J) * (unsigned)cd.n0 + (unsigned)I;
+        out[c] = acc;
+        if (out2) out2[c] = mul2 * (float)S->s * acc;
+        if (act0) {
+            __align__(16) __nv_bfloat16 v[16];
+            v[0] = __float2bfloat16_rn(acc * (float)(1. / S->s));
+            v[1] = __float2bfloat16_rn(maskc[c]);
+            v[2] = __float2bfloat16_rn(chan);
+            for (int q = 3; q < 16; ++q) v[q] = __float2bfloat16_rn(0.f);
+            uint4* dst = reinterpret_cast<uint4*>(act0 + (size_t)c * 16);
+            dst[0] = reinterpret_cast<uint4*>(v)[0];
+            dst[1] = reinterpret_cast<uint4*>(v)[1];
+        }
+    }
+}
+
+inline dim3 restrict_grid(const Dims3& cd) {
+    return dim3((unsigned)((cd.n0 + RCI - 1) / RCI), (unsigned)((cd.n1 + RCJ - 1) / RCJ), (unsigned)((cd.n2 + RCK - 1) / RCK));
+}
+
+// (P wc)[f] on the fine lattice fd from the coarse lattice cd (32-bit index arithmetic:
+// lattices stay below 2^32 cells)
+__device__ __forceinline__ float prolong_at(const Dims3& fd, const Dims3& cd, const float* wc, long long f) {
+    const unsigned uf = (unsigned)f, n0 = (unsigned)fd.n0, n1 = (unsigned)fd.n1;
+    const unsigned t = uf / n0;
+    const int fi = (int)(uf - t * n0);
+    const int fk = (int)(t / n1);
+    const int fj = (int)(t - (unsigned)fk * n1);
+    int I0 = fi >> 1, I1 = pclamp((fi & 1) ? I0 + 1 : I0 - 1, cd.n0);
+    int J0 = fj >> 1, J1 = pclamp((fj & 1) ? J0 + 1 : J0 - 1, cd.n1);
+    int K0 = fk >> 1, K1 = pclamp((fk & 1) ? K0 + 1 : K0 - 1, cd.n2);
+    const unsigned sJ = (unsigned)cd.n0, sK = (unsigned)cd.n0 * (unsigned)cd.n1;
+    auto row = [&](int K, int J) {
+        const float* w = wc + (unsigned)K * sK + (unsigned)J * sJ;
+        return 0.75f * __ldg(w + I0) + 0.25f * __ldg(w + I1);
+    };
+    float k0 = 0.75f * row(K0, J0) + 0.25f * row(K0, J1);
+    float k1 = 0.75f * row(K1, J0) + 0.25f * row(K1, J1);
+    return 0.75f * k0 + 0.25f * k1;
+}
+
+// w_l = gain * (ydiv ? y : s y) + P w_{l+1}   (wc null on the coarsest level)
+__global__ void __launch_bounds__(256) prolong_kernel(Dims3 fd, Dims3 cd, const float* wc, const float* y, int ydiv, float gain,
+                                                      float* out, const Scal* S) {
+    if (S->done) return;
+    long long Nf = (long long)fd.n0 * fd.n1 * fd.n2;
+    long long f = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (f >= Nf) return;
+    float sy = ydiv ? 1.f : (float)S->s;
+    float v = gain * sy * y[f];
+    if (wc) v += prolong_at(fd, cd, wc, f);
+    out[f] = v;
+}
+
+// z = D^-1 r + P w_1 (active), D^-1 r (ghost), 0 (inactive); partial (z, q_prev)
+__global__ void __launch_bounds__(LB) precond_z_kernel(long long N, Dims3 fd, Dims3 cd, const float* r, const float* invD,
+                                                       const uint8_t* st, const float* w1, float* z, const float* qprev, double* part,
+                                                       const Scal* S) {
+    if (S->done) return;
+    const long long T = (long long)gridDim.x * LB, t0 = blockIdx.x * (long long)LB + threadIdx.x, NQ = N >> 2;
+    double v[1] = {0.};
+    for (long long q = t0; q < NQ; q += T) {
+        float R[4], D[4], Z[4], Q[4];
+        uint8_t F[4];
+        un4(ld4(r, q), R); un4(ld4(invD, q), D); un4(ld4(qprev, q), Q); st_flags4(st, q, F);
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+            if (F[m] == ST_INACTIVE) Z[m] = 0.f;
+            else {
+                Z[m] = D[m] * R[m];
+                if (w1 && F[m] == ST_ACTIVE) Z[m] += prolong_at(fd, cd, w1, 4 * q + m);
+            }
+            v[0] += (double)Z[m] * Q[m];
+        }
+        st4(z, q, Z);
+    }
+    for (long long c = 4 * NQ + t0; c < N; c += T) {
+        float zv;
+        if (is_inactive(st, c)) zv = 0.f;
+        else {
+            zv = __ldg(invD + c) * r[c];
+            if (w1 && is_active(st, c)) zv += prolong_at(fd, cd, w1, c);
+        }
+        z[c] = zv;
+        v[0] += (double)zv * qprev[c];
+    }
+    block_sums(v, 1, part);
+}
+
+__global__ void beta_kernel(const double* part, int nblk, Scal* S) {
+    if (S->done) return;
+    double t[1];
+    totals(part, nblk, 1, t);
+    if (threadIdx.x == 0) { S->zq = t[0]; S->beta = S->pq != 0. ? t[0] / S->pq : 0.; }
+}
+
+// FP32 operator row (7-point, or the ghost row's 9 entries)
+template <class X>
+__device__ __forceinline__ float applyF(const OpSymF32& A, long long c, X&& x) {
+    float y = __ldg(A.aP + c) * x(c) + __ldg(A.aE + c) * x(c + 1) + __ldg(A.aE + c - 1) * x(c - 1) + __ldg(A.aN + c) * x(c + A.nI)
+              + __ldg(A.aN + c - A.nI) * x(c - A.nI) + __ldg(A.aT + c) * x(c + A.nIJ) + __ldg(A.aT + c - A.nIJ) * x(c - A.nIJ);
+    if (A.gh.n > 0) {
+        uint32_t w = __ldg(A.gh.bits + (c >> 5));
+        if ((w >> (c & 31)) & 1u) {
+            int lo = 0, hi = A.gh.n;
+            while (lo < hi) { int mid = (lo + hi) >> 1; if (__ldg(A.gh.cell + mid) < c) lo = mid + 1; else hi = mid; }
+            float s = 0.f;
+            for (int m = 0; m < 9; ++m) { int col = __ldg(A.gh.col + 9 * lo + m); if (col >= 0) s += (float)__ldg(A.gh.val + 9 * lo + m) * x(col); }
+            y = s;
+        }
+    }
+    return y;
+}
+
+// p_new = z - beta p_old, q_new = A p_new (neighbours recomputed), partials (p, q), (p, r)
+__global__ void __launch_bounds__(LB) direction_kernel(OpSymF32 A, long long N, const float* z, const float* pold, float* pnew, float* qnew,
+                                                       const float* r, double* part, const Scal* S) {
+    if (S->done) return;
+    float be = (float)S->beta;
+    double v[2] = {0., 0.};
+    for (long long c = blockIdx.x * (long long)LB + threadIdx.x; c < N; c += (long long)gridDim.x * LB) {
+        float pc = z[c] - be * pold[c];
+        float qc = applyF(A, c, [&](long long e_) { return z[e_] - be * pold[e_]; });
+        pnew[c] = pc; qnew[c] = qc;
+        v[0] += (double)pc * qc;
+        v[1] += (double)pc * r[c];
+    }
+    block_sums(v, 2, part);
+}
+
+__global__ void alpha_kernel(const double* part, int nblk, Scal* S) {
+    if (S->done) return;
+    double t[2];
+    totals(part, nblk, 2, t);
+    if (threadIdx.x == 0) {
+        S->pq = t[0];
+        S->pr = t[1];
+        S->alpha = t[0] != 0. ? t[1] / t[0] : 0.;
+        if (!(t[0] != 0.) || t[0] != t[0]) S->done = 1;
+    }
+}
+
+// e += alpha p, r -= alpha q, partial ||r||^2 and ||D^-1 r||^2 (next network scale)
+__global__ void __launch_bounds__(LB) step_kernel(long long N, float* e, float* r, const float* p, const float* q, const float* invD,
+                                                  const uint8_t* st, double* part, const Scal* S) {
+    if (S->done) return;
+    const float al = (float)S->alpha;
+    const long long T = (long long)gridDim.x * LB, t0 = blockIdx.x * (long long)LB + threadIdx.x, NQ = N >> 2;
+    double v[2] = {0., 0.};
+    for (long long qd = t0; qd < NQ; qd += T) {
+        float E[4], R[4], P4[4], Q[4], D[4];
+        uint8_t F[4];
+        un4(ld4(e, qd), E); un4(ld4(r, qd), R); un4(ld4(p, qd), P4); un4(ld4(q, qd), Q); un4(ld4(invD, qd), D); st_flags4(st, qd, F);
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+            E[m] = E[m] + al * P4[m];
+            R[m] = R[m] - al * Q[m];
+            v[0] += (double)R[m] * R[m];
+            if (F[m] == ST_ACTIVE) { double u = (double)D[m] * R[m]; v[1] += u * u; }
+        }
+        st4(e, qd, E);
+        st4(r, qd, R);
+    }
+    for (long long c = 4 * NQ + t0; c < N; c += T) {
+        e[c] = e[c] + al * p[c];
+        float rn = r[c] - al * q[c];
+        r[c] = rn;
+        v[0] += (double)rn * rn;
+        if (is_active(st, c)) { double u = (double)__ldg(invD + c) * rn; v[1] += u * u; }
+    }
+    block_sums(v, 2, part);
+}
+
+__global__ void step_finish_kernel(const double* part, int nblk, Scal* S, int max_iters) {
+    if (S->done) return;
+    double t[2];
+    totals(part, nblk, 2, t);
+    if (threadIdx.x == 0) {
+        S->rr = t[0];
+        S->iters += 1;
+        S->s = S->nact > 0. ? sqrt(t[1] / S->nact) : 1.;
+        if (!(S->s > 0.)) S->s = 1.;
+        if (t[0] <= S->tin2 || S->iters >= max_iters || t[0] != t[0]) S->done = 1;
+    }
+}
+
+// ---------------------------------------------------------------- inner flexible BiCGStab (FP32)
+// For operators with immersed-boundary ghost rows (not symmetric): right-preconditioned
+// BiCGStab, each half step preconditioned by the same M; x and r stay consistent for any M.
+//   p = r + beta (p - omega v);  ph = M(p);  v = A ph;  alpha = rho / (rhat, v)
+//   s = r - alpha v;  sh = M(s);  t = A sh;  omega = (t, s) / (t, t)
+//   e += alpha ph + omega sh;  r = s - omega t;  rho' = (rhat, r);  beta = rho'/rho alpha/omega
+__global__ void __launch_bounds__(LB) bs_start_kernel(long long N, const float* r, float* rh, float* e, float* p, float* v, double* part,
+                                                      const Scal* S) {
+    if (S->done) return;
+    double a[1] = {0.};
+    for (long long c = blockIdx.x * (long long)LB + threadIdx.x; c < N; c += (long long)gridDim.x * LB) {
+        float rv = r[c];
+        rh[c] = rv; e[c] = 0.f; p[c] = 0.f; v[c] = 0.f;
+        a[0] += (double)rv * rv;
+    }
+    block_sums(a, 1, part);
+}
+__global__ void bs_start_finish(const double* part, int nblk, Scal* S, double eta, const double* nact) {
+    if (S->done) return;
+    double t[1];
+    totals(part, nblk, 1, t);
+    if (threadIdx.x == 0) {
+        S->rr0 = t[0]; S->rr = t[0];
+        S->tin2 = eta * eta * t[0];
+        S->nact = *nact;
+        S->rho = t[0]; S->alpha = 1.; S->omega = 1.; S->beta = 0.;
+        S->done = !(t[0] > 0.);
+    }
+}
+// p = r + beta (p - omega v); partial sum of (D^-1 p)^2 over active cells (scale of M(p))
+__global__ void __launch_bounds__(LB) bs_dir_kernel(long long N, const float* r, const float* v, const float* invD, const uint8_t* st,
+                                                    float* p, double* part, const Scal* S) {
+    if (S->done) return;
+    const float be = (float)S->beta, om = (float)S->omega;
+    const long long T = (long long)gridDim.x * LB, t0 = blockIdx.x * (long long)LB + threadIdx.x, NQ = N >> 2;
+    double a[1] = {0.};
+    for (long long q = t0; q < NQ; q += T) {
+        float R[4], V[4], P4[4], D[4];
+        uint8_t F[4];
+        un4(ld4(r, q), R); un4(ld4(v, q), V); un4(ld4(p, q), P4); un4(ld4(invD, q), D); st_flags4(st, q, F);
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+            P4[m] = R[m] + be * (P4[m] - om * V[m]);
+            if (F[m] == ST_ACTIVE) { double u = (double)D[m] * P4[m]; a[0] += u * u; }
+        }
+        st4(p, q, P4);
+    }
+    for (long long c = 4 * NQ + t0; c < N; c += T) {
+        float pv = r[c] + be * (p[c] - om * v[c]);
+        p[c] = pv;
+        if (is_active(st, c)) { double u = (double)__ldg(invD + c) * pv; a[0] += u * u; }
+    }
+    block_sums(a, 1, part);
+}
+__global__ void scale_finish(const double* part, int nblk, Scal* S) {
+    if (S->done) return;
+    double t[1];
+    totals(part, nblk, 1, t);
+    if (threadIdx.x == 0) {
+        double sc = S->nact > 0. ? sqrt(t[0] / S->nact) : 1.;
+        S->s = sc > 0. ? sc : 1.;
+    }
+}
+// y = M(x) on the cell lattice: D^-1 x + P w_1 on active cells, D^-1 x on ghost rows, 0 on inactive cells
+__global__ void __launch_bounds__(LB) bs_z_kernel(long long N, Dims3 fd, Dims3 cd, const float* x, const float* invD, const uint8_t* st,
+                                                  const float* w1, float* y, const Scal* S) {
+    if (S->done) return;
+    const long long T = (long long)gridDim.x * LB, t0 = blockIdx.x * (long long)LB + threadIdx.x, NQ = N >> 2;
+    for (long long q = t0; q < NQ; q += T) {
+        float X[4], D[4], Y[4];
+        uint8_t F[4];
+        un4(ld4(x, q), X); un4(ld4(invD, q), D); st_flags4(st, q, F);
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+            if (F[m] == ST_INACTIVE) Y[m] = 0.f;
+            else {
+                Y[m] = D[m] * X[m];
+                if (w1 && F[m] == ST_ACTIVE) Y[m] += prolong_at(fd, cd, w1, 4 * q + m);
+            }
+        }
+        st4(y, q, Y);
+    }
+    for (long long c = 4 * NQ + t0; c < N; c += T) {
+        float zv;
+        if (is_inactive(st, c)) zv = 0.f;
+        else {
+            zv = __ldg(invD + c) * x[c];
+            if (w1 && is_active(st, c)) zv += prolong_at(fd, cd, w1, c);
+        }
+        y[c] = zv;
+    }
+}
+// out = A x; partial (a1, out), or with b2: (b2, out) and (out, out)
+__global__ void __launch_bounds__(LB) bs_spmv_kernel(OpSymF32 A, long long N, const float* x, float* out, const float* a1, const float* b2,
+                                                     double* part, const Scal* S) {
+    if (S->done) return;
+    double a[2] = {0., 0.};
+    for (long long c = blockIdx.x * (long long)LB + threadIdx.x; c < N; c += (long long)gridDim.x * LB) {
+        float y = applyF(A, c, [&](long long e_) { return x[e_]; });
+        out[c] = y;
+        if (b2) { a[0] += (double)b2[c] * y; a[1] += (double)y * y; }
+        else a[0] += (double)a1[c] * y;
+    }
+    block_sums(a, b2 ? 2 : 1, part);
+}
+__global__ void bs_alpha_finish(const double* part, int nblk, Scal* S) {
+    if (S->done) return;
+    double t[1];
+    totals(part, nblk, 1, t);
+    if (threadIdx.x == 0) {
+        S->rv = t[0];
+        if (t[0] != 0. && t[0] == t[0]) S->alpha = S->rho / t[0];
+        else { S->alpha = 0.; S->done = 1; }
+    }
+}
+// s = r - alpha v; partial sum of (D^-1 s)^2 over active cells
+__global__ void __launch_bounds__(LB) bs_s_kernel(long long N, const float* r, const float* v, const float* invD, const uint8_t* st, float* s,
+                                                  double* part, const Scal* S) {
+    if (S->done) return;
+    const float al = (float)S->alpha;
+    const long long T = (long long)gridDim.x * LB, t0 = blockIdx.x * (long long)LB + threadIdx.x, NQ = N >> 2;
+    double a[1] = {0.};
+    for (long long q = t0; q < NQ; q += T) {
+        float R[4], V[4], D[4], O[4];
+        uint8_t F[4];
+        un4(ld4(r, q), R); un4(ld4(v, q), V); un4(ld4(invD, q), D); st_flags4(st, q, F);
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+            O[m] = R[m] - al * V[m];
+            if (F[m] == ST_ACTIVE) { double u = (double)D[m] * O[m]; a[0] += u * u; }
+        }
+        st4(s, q, O);
+    }
+    for (long long c = 4 * NQ + t0; c < N; c += T) {
+        float sv = r[c] - al * v[c];
+        s[c] = sv;
+        if (is_active(st, c)) { double u = (double)__ldg(invD + c) * sv; a[0] += u * u; }
+    }
+    block_sums(a, 1, part);
+}
+__global__ void bs_omega_finish(const double* part, int nblk, Scal* S) {
+    if (S->done) return;
+    double t[2];
+    totals(part, nblk, 2, t);
+    if (threadIdx.x == 0) {
+        S->ts = t[0]; S->tt = t[1];
+        S->omega = t[1] > 0. ? t[0] / t[1] : 0.;
+    }
+}
+// e += alpha ph + omega sh; r = s - omega t; partials ||r||^2, (rhat, r)
+__global__ void __launch_bounds__(LB) bs_update_kernel(long long N, float* e, float* r, const float* ph, const float* sh, const float* s,
+                                                       const float* t, const float* rh, double* part, const Scal* S) {
+    if (S->done) return;
+    const float al = (float)S->alpha, om = (float)S->omega;
+    const long long T = (long long)gridDim.x * LB, t0 = blockIdx.x * (long long)LB + threadIdx.x, NQ = N >> 2;
+    double a[2] = {0., 0.};
+    for (long long q = t0; q < NQ; q += T) {
+        float E[4], PH[4], SH[4], S4[4], T4[4], RH[4], RN[4];
+        un4(ld4(e, q), E); un4(ld4(ph, q), PH); un4(ld4(sh, q), SH); un4(ld4(s, q), S4); un4(ld4(t, q), T4); un4(ld4(rh, q), RH);
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+            E[m] = E[m] + al * PH[m] + om * SH[m];
+            RN[m] = S4[m] - om * T4[m];
+            a[0] += (double)RN[m] * RN[m];
+            a[1] += (double)RH[m] * RN[m];
+        }
+        st4(e, q, E);
+        st4(r, q, RN);
+    }
+    for (long long c = 4 * NQ + t0; c < N; c += T) {
+        e[c] = e[c] + al * ph[c] + om * sh[c];
+        float rn = s[c] - om * t[c];
+        r[c] = rn;
+        a[0] += (double)rn * rn;
+        a[1] += (double)rh[c] * rn;
+    }
+    block_sums(a, 2, part);
+}
+__global__ void bs_update_finish(const double* part, int nblk, Scal* S, int max_iters) {
+    if (S->done) return;
+    double t[2];
+    totals(part, nblk, 2, t);
+    if (threadIdx.x == 0) {
+        S->rr = t[0];
+        S->iters += 1;
+        double rho_new = t[1];
+        bool breakdown = !(S->omega != 0.) || !(S->rho != 0.) || t[1] != t[1];
+        S->beta = breakdown ? 0. : (rho_new / S->rho) * (S->alpha / S->omega);
+        S->rho = rho_new;
+        if (t[0] <= S->tin2 || S->iters >= max_iters || t[0] != t[0] || breakdown) S->done = 1;
+    }
+}
+
+// active-cell count (the scale of the preconditioner input is an RMS over active cells)
+__global__ void __launch_bounds__(LB) count_active_kernel(long long N, const uint8_t* st, double* part) {
+    double a[1] = {0.};
+    for (long long c = blockIdx.x * (long long)LB + threadIdx.x; c < N; c += (long long)gridDim.x * LB) a[0] += is_active(st, c) ? 1. : 0.;
+    block_sums(a, 1, part);
+}
+__global__ void count_finish(const double* part, int nblk, double* out) {
+    double t[1];
+    totals(part, nblk, 1, t);
+    if (threadIdx.x == 0) *out = t[0];
+}
+
+// ---------------------------------------------------------------- small kernels
+__global__ void mean_kernel(long long N, const double* b, double* part) {
+    double v[1] = {0.};
+    for (long long c = blockIdx.x * (long long)LB + threadIdx.x; c < N; c += (long long)gridDim.x * LB) v[0] += b[c];
+    block_sums(v, 1, part);
+}
+__global__ void mean_finish_kernel(const double* part, int nblk, double* out, long long N) {
+    double t[1];
+    totals(part, nblk, 1, t);
+    if (threadIdx.x == 0) *out = t[0] / (double)N;
+}
+__global__ void sub_mean_kernel(long long N, double* b, const double* mean) {
+    long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (c < N) b[c] = b[c] - *mean;
+}
+__global__ void zero_kernel(long long N, double* x) {
+    long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (c < N) x[c] = 0.;
+}
+__global__ void cast_kernel(OpSym A, long long N, float* aP, float* aE, float* aN, float* aT, float* invD) {
+    long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (c >= N) return;
+    double d = A.aP[c];
+    aP[c] = (float)d; aE[c] = (float)A.aE[c]; aN[c] = (float)A.aN[c]; aT[c] = (float)A.aT[c];
+    invD[c] = d != 0. ? (float)(1. / d) : 1.f;
+}
+__global__ void publish_kernel(const Scal* S, KspOut* out) {
+    if (threadIdx.x != 0) return;
+    out->iters[0] = S->iters;
+    out->iters[1] = S->outer;
+    out->relres[0] = S->bb > 0. ? sqrt(S->rr64 / S->bb) : 0.;
+    out->status[0] = S->status;
+}
+
+// ---------------------------------------------------------------- pyramid host side
+Dims3 dims_of(const Level& l) { return Dims3{l.n[0], l.n[1], l.n[2]}; }
+
+// Restriction chain, the network (or the identity) on every coarse level, prolongation chain
+// (result in lev[1].w).  Every kernel is a no-op while S->done is set.
+int apply_levels(LearnedWork& lw, const float* rfine, const uint8_t* status, int mode, Scal* S, cudaStream_t st) {
+    if (mode == NET_MODE_JACOBI || lw.nLev < 2) return 0;
+    auto netAt = [&](int l) { return mode == NET_MODE_NETWORK && l >= lw.netFrom; };
+    for (int l = 1; l < lw.nLev; ++l) {
+        Level& c = lw.lev[l];
+        const Level& f = lw.lev[l - 1];
+        restrict_kernel<<<restrict_grid(dims_of(c)), 256, 0, st>>>(dims_of(f), dims_of(c), l == 1 ? rfine : f.u, l == 1 ? lw.invD : nullptr,
+                                                                   l == 1 ? status : nullptr, c.rscale, c.u, nullptr, 0.f,
+                                                                   netAt(l) ? c.net.act[0] : nullptr, c.mask, c.chan, S);
+    }
+    CB_CHECK_LAUNCH();
+    for (int l = 1; l < lw.nLev; ++l)
+        if (netAt(l) && net_forward_if(lw.lev[l].net, &S->done, st)) return 1;
+    for (int l = lw.nLev - 1; l >= 1; --l) {
+        Level& f = lw.lev[l];
+        const bool top = l + 1 >= lw.nLev;
+        prolong_kernel<<<grid_for(f.N, 256), 256, 0, st>>>(dims_of(f), top ? dims_of(f) : dims_of(lw.lev[l + 1]),
+                                                           top ? nullptr : lw.lev[l + 1].w, netAt(l) ? f.net.y : f.u, netAt(l) ? 0 : 1,
+                                                           f.gain, f.w, S);
+    }
+    CB_CHECK_LAUNCH();
+    return 0;
+}
+
+const float* level_w1(const LearnedWork& lw, int mode) { return (mode == NET_MODE_JACOBI || lw.nLev < 2) ? nullptr : lw.lev[1].w; }
+Dims3 level1_dims(const LearnedWork& lw) { return lw.nLev >= 2 ? dims_of(lw.lev[1]) : dims_of(lw.lev[0]); }
+
+// masks of the coarse levels: fraction of active fine cells
+int level_masks(LearnedWork& lw, const uint8_t* status, cudaStream_t st) {
+    for (int l = 1; l < lw.nLev; ++l) {
+        Level& c = lw.lev[l];
+        const Level& f = lw.lev[l - 1];
+        restrict_kernel<<<restrict_grid(dims_of(c)), 256, 0, st>>>(dims_of(f), dims_of(c), l == 1 ? nullptr : f.mask, nullptr,
+                                                                   l == 1 ? status : nullptr, c.rscale, c.mask, nullptr, 0.f, nullptr,
+                                                                   nullptr, 0.f, nullptr);
+    }
+    CB_CHECK_LAUNCH();
+    lw.masksReady = true;
+    return 0;
+}
+
+OpSymF32 cast_operator(LearnedWork& lw, const OpSym& A, const Lat& L, cudaStream_t st) {
+    cast_kernel<<<grid_for(L.N, 256), 256, 0, st>>>(A, L.N, lw.A[0], lw.A[1], lw.A[2], lw.A[3], lw.invD);
+    OpSymF32 Af;
+    Af.aP = lw.A[0]; Af.aE = lw.A[1]; Af.aN = lw.A[2]; Af.aT = lw.A[3]; Af.nI = A.nI; Af.nIJ = A.nIJ; Af.gh = A.gh;
+    return Af;
+}
+
+}  // namespace
+
+int learned_alloc(LearnedWork& lw, const Lat& L, void* (*alloc)(size_t, void*), void* ctx) {
+    lw.L = L;
+    auto fcell = [&]() -> float* {
+        float* b = static_cast<float*>(alloc(sizeof(float) * (size_t)L.PS, ctx));
+        return b ? b + L.H : nullptr;
+    };
+    lw.r = fcell(); lw.z = fcell(); lw.e = fcell();
+    lw.p[0] = fcell(); lw.p[1] = fcell(); lw.q[0] = fcell(); lw.q[1] = fcell();
+    lw.t = fcell(); lw.rh = fcell();
+    lw.invD = fcell();
+    for (int q = 0; q < 4; ++q) lw.A[q] = fcell();
+    lw.part = static_cast<double*>(alloc(sizeof(double) * 4 * MAXP, ctx));
+    lw.scal = alloc(sizeof(Scal), ctx);
+    lw.mean = static_cast<double*>(alloc(sizeof(double) * 2, ctx));
+    bool ok = lw.r && lw.z && lw.e && lw.p[0] && lw.p[1] && lw.q[0] && lw.q[1] && lw.t && lw.rh && lw.invD && lw.part && lw.scal && lw.mean;
+    for (int q = 0; q < 4; ++q) ok = ok && lw.A[q];
+    if (!ok) { set_error("learned-solver allocation failed"); return 1; }
+    if (cudaMallocHost(&lw.hostScal, sizeof(Scal)) != cudaSuccess) { set_error("pinned allocation failed"); return 1; }
+    // level pyramid: halve every direction longer than one cell until about 64 cells remain
+    Level& l0 = lw.lev[0];
+    l0.n[0] = L.nI; l0.n[1] = L.nJ; l0.n[2] = L.nK; l0.N = L.N; l0.rscale = 1.f; l0.gain = 1.f; l0.chan = 0.f;
+    lw.nLev = 1;
+    while (lw.nLev < LEARN_MAX_LEVELS) {
+        const Level& f = lw.lev[lw.nLev - 1];
+        if (f.N <= 64 || (f.n[0] == 1 && f.n[1] == 1 && f.n[2] == 1)) break;
+        Level& c = lw.lev[lw.nLev];
+        int coarsened = 0;
+        for (int d = 0; d < 3; ++d) {
+            c.n[d] = f.n[d] > 1 ? (f.n[d] + 1) / 2 : 1;
+            coarsened += f.n[d] > 1;
+        }
+        c.N = (long long)c.n[0] * c.n[1] * c.n[2];
+        c.rscale = 1.f / (float)(1 << coarsened);
+        c.gain = f.gain * 4.f;
+        c.chan = (float)lw.nLev / 8.f;
+        c.u = static_cast<float*>(alloc(sizeof(float) * (size_t)c.N, ctx));
+        c.w = static_cast<float*>(alloc(sizeof(float) * (size_t)c.N, ctx));
+        c.mask = static_cast<float*>(alloc(sizeof(float) * (size_t)c.N, ctx));
+        if (!c.u || !c.w || !c.mask) { set_error("learned-solver allocation failed"); return 1; }
+        Lat Lc = make_lat(c.n[0], c.n[1], c.n[2]);
+        int rc = lw.nLev == 1 ? net_alloc(c.net, Lc, alloc, ctx) : net_alloc_shared(c.net, Lc, lw.lev[1].net, alloc, ctx);
+        if (rc) return 1;
+        ++lw.nLev;
+    }
+    lw.weights = lw.nLev >= 2 ? &lw.lev[1].net : nullptr;
+    lw.masksReady = false;
+    return 0;
+}
+
+void learned_free_host(LearnedWork& lw) {
+    if (lw.hostScal) cudaFreeHost(lw.hostScal);
+    lw.hostScal = nullptr;
+}
+
+int learned_solve(LearnedWork& lw, const OpSym& A, const uint8_t* status, const double* b, double* x, const Lat& L, double rtol, int maxit,
+                  double eta, int project, int mode, KspOut* out, cudaStream_t st) {
+    const long long N = L.N;
+    const int nb = nblocks(N);
+    const int G = grid_for(N, 256);
+    Scal* S = static_cast<Scal*>(lw.scal);
+    if (mode == NET_MODE_NETWORK && (!lw.haveParams || lw.nLev < 2)) mode = NET_MODE_JACOBI;
+    if (mode != NET_MODE_JACOBI && !lw.masksReady && level_masks(lw, status, st)) return 1;
+    OpSymF32 Af = cast_operator(lw, A, L, st);
+    if (project) {
+        mean_kernel<<<nb, LB, 0, st>>>(N, b, lw.part);
+        mean_finish_kernel<<<1, LB, 0, st>>>(lw.part, nb, lw.mean, N);
+        sub_mean_kernel<<<G, 256, 0, st>>>(N, const_cast<double*>(b), lw.mean);
+    }
+    zero_kernel<<<G, 256, 0, st>>>(N, x);
+    Scal init;
+    std::memset(&init, 0, sizeof(init));
+    init.first = 1;
+    CB_CUDA(cudaMemcpyAsync(S, &init, sizeof(Scal), cudaMemcpyHostToDevice, st));
+    CB_CHECK_LAUNCH();
+    const Dims3 fd = dims_of(lw.lev[0]), cd = level1_dims(lw);
+    const float* w1 = level_w1(lw, mode);
+    const bool symmetric = lw.inner == LEARN_INNER_FCG || (lw.inner == LEARN_INNER_AUTO && A.gh.n == 0);
+    if (!symmetric) {
+        count_active_kernel<<<nb, LB, 0, st>>>(N, status, lw.part);
+        count_finish<<<1, LB, 0, st>>>(lw.part, nb, lw.mean + 1);
+    }
+    const int max_outer = 12;
+    const int chunk = 8;
+    for (int outer = 0; outer <= max_outer; ++outer) {
+        outer_residual_kernel<<<nb, LB, 0, st>>>(A, N, b, x, lw.r, lw.part, S);
+        outer_check_kernel<<<1, LB, 0, st>>>(lw.part, nb, S, max_outer);
+        CB_CUDA(cudaMemcpyAsync(lw.hostScal, S, sizeof(Scal), cudaMemcpyDeviceToHost, st));
+        CB_CUDA(cudaStreamSynchronize(st));
+        Scal* hs = static_cast<Scal*>(lw.hostScal);
+        if (outer == 0) {
+            // the tolerance needs ||b||^2: the first outer residual (x = 0) is b itself
+            double tol2 = rtol * rtol * hs->bb;
+            bool fin = hs->rr64 <= tol2 || !(hs->bb > 0.);
+            CB_CUDA(cudaMemcpyAsync(&S->tol2, &tol2, sizeof(double), cudaMemcpyHostToDevice, st));
+            if (fin) {
+                int one = 1;
+                CB_CUDA(cudaMemcpyAsync(&S->odone, &one, sizeof(int), cudaMemcpyHostToDevice, st));
+                break;
+            }
+        } else if (hs->odone) {
+            break;
+        }
+        // inner target: deep first, then only the factor still missing
+        double etaK = eta;
+        if (hs->bb > 0. && hs->rr64 > 0.) {
+            double need = 0.25 * rtol * sqrt(hs->bb / hs->rr64);
+            if (need > etaK) etaK = need;
+        }
+        if (etaK > 0.5) etaK = 0.5;
+        int cur = 0;
+        if (symmetric) {
+            inner_start_kernel<<<nb, LB, 0, st>>>(N, lw.r, lw.invD, status, lw.e, lw.p[0], lw.q[0], lw.part, S);
+            inner_start_finish_kernel<<<1, LB, 0, st>>>(lw.part, nb, S, etaK);
+        } else {
+            bs_start_kernel<<<nb, LB, 0, st>>>(N, lw.r, lw.rh, lw.e, lw.p[0], lw.q[0], lw.part, S);
+            bs_start_finish<<<1, LB, 0, st>>>(lw.part, nb, S, etaK, lw.mean + 1);
+        }
+        bool innerDone = false;
+        while (!innerDone) {
+            for (int it = 0; it < chunk; ++it) {
+                if (symmetric) {
+                    if (apply_levels(lw, lw.r, status, mode, S, st)) return 1;
+                    precond_z_kernel<<<nb, LB, 0, st>>>(N, fd, cd, lw.r, lw.invD, status, w1, lw.z, lw.q[cur], lw.part, S);
+                    beta_kernel<<<1, LB, 0, st>>>(lw.part, nb, S);
+                    direction_kernel<<<nb, LB, 0, st>>>(Af, N, lw.z, lw.p[cur], lw.p[cur ^ 1], lw.q[cur ^ 1], lw.r, lw.part, S);
+                    alpha_kernel<<<1, LB, 0, st>>>(lw.part, nb, S);
+                    step_kernel<<<nb, LB, 0, st>>>(N, lw.e, lw.r, lw.p[cur ^ 1], lw.q[cur ^ 1], lw.invD, status, lw.part, S);
+                    step_finish_kernel<<<1, LB, 0, st>>>(lw.part, nb, S, maxit);
+                    cur ^= 1;
+                } else {
+                    // p = p[0], v = q[0], ph = p[1], sh = q[1], s = z, t = t
+                    bs_dir_kernel<<<nb, LB, 0, st>>>(N, lw.r, lw.q[0], lw.invD, status, lw.p[0], lw.part, S);
+                    scale_finish<<<1, LB, 0, st>>>(lw.part, nb, S);
+                    if (apply_levels(lw, lw.p[0], status, mode, S, st)) return 1;
+                    bs_z_kernel<<<nb, LB, 0, st>>>(N, fd, cd, lw.p[0], lw.invD, status, w1, lw.p[1], S);
+                    bs_spmv_kernel<<<nb, LB, 0, st>>>(Af, N, lw.p[1], lw.q[0], lw.rh, nullptr, lw.part, S);
+                    bs_alpha_finish<<<1, LB, 0, st>>>(lw.part, nb, S);
+                    bs_s_kernel<<<nb, LB, 0, st>>>(N, lw.r, lw.q[0], lw.invD, status, lw.z, lw.part, S);
+                    scale_finish<<<1, LB, 0, st>>>(lw.part, nb, S);
+                    if (apply_levels(lw, lw.z, status, mode, S, st)) return 1;
+                    bs_z_kernel<<<nb, LB, 0, st>>>(N, fd, cd, lw.z, lw.invD, status, w1, lw.q[1], S);
+                    bs_spmv_kernel<<<nb, LB, 0, st>>>(Af, N, lw.q[1], lw.t, nullptr, lw.z, lw.part, S);
+                    bs_omega_finish<<<1, LB, 0, st>>>(lw.part, nb, S);
+                    bs_update_kernel<<<nb, LB, 0, st>>>(N, lw.e, lw.r, lw.p[1], lw.q[1], lw.z, lw.t, lw.rh, lw.part, S);
+                    bs_update_finish<<<1, LB, 0, st>>>(lw.part, nb, S, maxit);
+                }
+            }
+            CB_CHECK_LAUNCH();
+            CB_CUDA(cudaMemcpyAsync(lw.hostScal, S, sizeof(Scal), cudaMemcpyDeviceToHost, st));
+            CB_CUDA(cudaStreamSynchronize(st));
+            Scal* h2 = static_cast<Scal*>(lw.hostScal);
+            innerDone = h2->done != 0;
+            if (h2->iters >= maxit) break;
+        }
+        outer_update_kernel<<<G, 256, 0, st>>>(N, x, lw.e, S);
+        // the next outer pass re-opens the inner solve
+        int zero = 0;
+        CB_CUDA(cudaMemcpyAsync(&S->done, &zero, sizeof(int), cudaMemcpyHostToDevice, st));
+    }
+    publish_kernel<<<1, 32, 0, st>>>(S, out);
+    CB_CHECK_LAUNCH();
+    CB_CUDA(cudaMemcpyAsync(lw.hostScal, S, sizeof(Scal), cudaMemcpyDeviceToHost, st));
+    CB_CUDA(cudaStreamSynchronize(st));
+    lw.lastIters = static_cast<Scal*>(lw.hostScal)->iters;
+    lw.lastOuter = static_cast<Scal*>(lw.hostScal)->outer;
+    return 0;
+}
+
+// ---------------------------------------------------------------- training pairs
+namespace {
+
+// Pair of an intermediate iterate x_k of a plain solve: residual r_k = b - A x_k (FP64, then
+// rounded) and correction e_k = x* - x_k, so that A e_k = r_k.
+__global__ void __launch_bounds__(LB) snapshot_pair_kernel(OpSym A, long long N, const double* b, const double* xs, const double* xk, float* pb,
+                                                           float* px) {
+    for (long long c = blockIdx.x * (long long)LB + threadIdx.x; c < N; c += (long long)gridDim.x * LB) {
+        double y = __ldg(A.aP + c) * xk[c] + __ldg(A.aE + c) * xk[c + 1] + __ldg(A.aE + c - 1) * xk[c - 1]
+                   + __ldg(A.aN + c) * xk[c + A.nI] + __ldg(A.aN + c - A.nI) * xk[c - A.nI]
+                   + __ldg(A.aT + c) * xk[c + A.nIJ] + __ldg(A.aT + c - A.nIJ) * xk[c - A.nIJ];
+        if (A.gh.n > 0) {
+            uint32_t w = __ldg(A.gh.bits + (c >> 5));
+            if ((w >> (c & 31)) & 1u) {
+                int lo = 0, hi = A.gh.n;
+                while (lo < hi) { int mid = (lo + hi) >> 1; if (__ldg(A.gh.cell + mid) < c) lo = mid + 1; else hi = mid; }
+                double s = 0.;
+                for (int m = 0; m < 9; ++m) { int col = __ldg(A.gh.col + 9 * lo + m); if (col >= 0) s += __ldg(A.gh.val + 9 * lo + m) * xk[col]; }
+                y = s;
+            }
+        }
+        pb[c] = (float)(b[c] - y);
+        px[c] = (float)(xs[c] - xk[c]);
+    }
+}
+
+}  // namespace
+
+int learned_snapshot_pair(const OpSym& A, const Lat& L, const double* b, const double* xstar, const double* xk, float* pb, float* px,
+                          cudaStream_t st) {
+    snapshot_pair_kernel<<<nblocks(L.N), LB, 0, st>>>(A, L.N, b, xstar, xk, pb, px);
+    CB_CHECK_LAUNCH();
+    return 0;
+}
+
+// ---------------------------------------------------------------- training
+namespace {
+
+struct TrainScal {
+    double s, coef, loss, loss_sum;
+};
+
+__global__ void __launch_bounds__(LB) train_scale_kernel(long long N, const float* b, const float* invD, const uint8_t* st, double* part) {
+    double v[2] = {0., 0.};
+    for (long long c = blockIdx.x * (long long)LB + threadIdx.x; c < N; c += (long long)gridDim.x * LB) {
+        if (!is_active(st, c)) continue;
+        double u = (double)__ldg(invD + c) * b[c];
+        v[0] += u * u; v[1] += 1.;
+    }
+    block_sums(v, 2, part);
+}
+__global__ void train_scale_finish(const double* part, int nblk, TrainScal* T, Scal* S) {
+    double t[2];
+    totals(part, nblk, 2, t);
+    if (threadIdx.x == 0) {
+        double sc = t[1] > 0. ? sqrt(t[0] / t[1]) : 1.;
+        if (!(sc > 0.)) sc = 1.;
+        T->s = sc; S->s = sc; S->done = 0;
+    }
+}
+// err = M(b) - x*
+__global__ void __launch_bounds__(LB) train_err_kernel(long long N, Dims3 fd, Dims3 cd, const float* b, const float* invD, const uint8_t* st,
+                                                       const float* w1, const float* xs, float* err) {
+    for (long long c = blockIdx.x * (long long)LB + threadIdx.x; c < N; c += (long long)gridDim.x * LB) {
+        float zv;
+        if (is_inactive(st, c)) zv = 0.f;
+        else {
+            zv = __ldg(invD + c) * b[c];
+            if (w1 && is_active(st, c)) zv += prolong_at(fd, cd, w1, c);
+        }
+        err[c] = zv - xs[c];
+    }
+}
+// 7-point product restricted to the active cells (values elsewhere taken as zero): the
+// symmetric block of the p' matrix whose energy norm the training loss uses
+__device__ __forceinline__ float apply_active(const OpSymF32& A, const uint8_t* st, long long N, long long c, const float* x) {
+    auto xv = [&](long long e_) { return (e_ >= 0 && e_ < N && st[e_] == ST_ACTIVE) ? x[e_] : 0.f; };
+    return __ldg(A.aP + c) * xv(c) + __ldg(A.aE + c) * xv(c + 1) + __ldg(A.aE + c - 1) * xv(c - 1) + __ldg(A.aN + c) * xv(c + A.nI)
+           + __ldg(A.aN + c - A.nI) * xv(c - A.nI) + __ldg(A.aT + c) * xv(c + A.nIJ) + __ldg(A.aT + c - A.nIJ) * xv(c - A.nIJ);
+}
+// g = -(A err), h = -(A x*): partial err.g and x*.h (energy norms of the error and of x*);
+// with immersed-boundary cells, on the active block only
+__global__ void __launch_bounds__(LB) train_energy_kernel(OpSymF32 A, long long N, const uint8_t* st, const float* err, const float* xs, float* g,
+                                                          double* part) {
+    double v[2] = {0., 0.};
+    for (long long c = blockIdx.x * (long long)LB + threadIdx.x; c < N; c += (long long)gridDim.x * LB) {
+        float ge, hx;
+        if (st == nullptr) {
+            ge = -applyF(A, c, [&](long long e_) { return err[e_]; });
+            hx = -applyF(A, c, [&](long long e_) { return xs[e_]; });
+        } else if (st[c] == ST_ACTIVE) {
+            ge = -apply_active(A, st, N, c, err);
+            hx = -apply_active(A, st, N, c, xs);
+        } else {
+            ge = 0.f; hx = 0.f;
+        }
+        g[c] = ge;
+        v[0] += (double)err[c] * ge;
+        v[1] += (double)xs[c] * hx;
+    }
+    block_sums(v, 2, part);
+}
+__global__ void train_energy_finish(const double* part, int nblk, TrainScal* T, float* lossOut) {
+    double t[2];
+    totals(part, nblk, 2, t);
+    if (threadIdx.x == 0) {
+        double den = t[1] > 0. ? t[1] : 1.;
+        T->coef = 2. / den;
+        T->loss = t[0] / den;
+        T->loss_sum += t[0] / den;
+        if (lossOut) *lossOut = (float)(t[0] / den);
+    }
+}
+// dL/dz on the cells where z carries the prolonged term
+__global__ void train_dz_kernel(long long N, const float* g, const uint8_t* st, const TrainScal* T, float inv_batch, float* dz) {
+    long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (c >= N) return;
+    dz[c] = is_active(st, c) ? (float)T->coef * g[c] * inv_batch : 0.f;
+}
+__global__ void adam_kernel(int n, float* p, const float* g, float* m, float* v, float lr, float b1, float b2, float eps, int t) {
+    int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n) return;
+    float gq = g[q];
+    float mq = b1 * m[q] + (1.f - b1) * gq;
+    float vq = b2 * v[q] + (1.f - b2) * gq * gq;
+    m[q] = mq; v[q] = vq;
+    float mh = mq / (1.f - powf(b1, (float)t)), vh = vq / (1.f - powf(b2, (float)t));
+    p[q] = p[q] - lr * mh / (sqrtf(vh) + eps);
+}
+__global__ void loss_out_kernel(TrainScal* T, float* hist, int step, float inv_batch) {
+    if (threadIdx.x == 0) { hist[step] = (float)(T->loss_sum * inv_batch); T->loss_sum = 0.; }
+}
+
+// one application M(b) for pair (b, x*): error in lw.z, energy loss, g = -(A err) in lw.e
+int pair_forward(LearnedWork& lw, const OpSymF32& Af, const uint8_t* status, const Lat& L, const float* b, const float* xs, int mode,
+                 TrainScal* T, float* lossOut, cudaStream_t st) {
+    const long long N = L.N;
+    const int nb = nblocks(N);
+    Scal* S = static_cast<Scal*>(lw.scal);
+    train_scale_kernel<<<nb, LB, 0, st>>>(N, b, lw.invD, status, lw.part);
+    train_scale_finish<<<1, LB, 0, st>>>(lw.part, nb, T, S);
+    if (apply_levels(lw, b, status, mode, S, st)) return 1;
+    train_err_kernel<<<nb, LB, 0, st>>>(N, dims_of(lw.lev[0]), level1_dims(lw), b, lw.invD, status, level_w1(lw, mode), xs, lw.z);
+    train_energy_kernel<<<nb, LB, 0, st>>>(Af, N, status, lw.z, xs, lw.e, lw.part);
+    train_energy_finish<<<1, LB, 0, st>>>(lw.part, nb, T, lossOut);
+    CB_CHECK_LAUNCH();
+    return 0;
+}
+
+int check_net_error(LearnedWork& lw) {
+    if (!lw.weights) return 0;
+    int herr = 0;
+    CB_CUDA(cudaMemcpy(&herr, lw.weights->err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (herr) { set_error("tensor-core convolution: an MMA completion wait timed out"); return 1; }
+    return 0;
+}
+
+}  // namespace
+
+int learned_eval(LearnedWork& lw, const OpSym& A, const uint8_t* status, const Lat& L, const float* pairsB, const float* pairsX, int nPairs,
+                 int mode, float* lossHost, cudaStream_t st) {
+    if (mode == NET_MODE_NETWORK && (!lw.haveParams || lw.nLev < 2)) { set_error("no network parameters on this handle"); return 1; }
+    if (mode != NET_MODE_JACOBI && !lw.masksReady && level_masks(lw, status, st)) return 1;
+    OpSymF32 Af = cast_operator(lw, A, L, st);
+    TrainScal* T = nullptr;
+    float* dl = nullptr;
+    CB_CUDA(cudaMallocAsync(&T, sizeof(TrainScal), st));
+    CB_CUDA(cudaMallocAsync(&dl, sizeof(float) * (nPairs > 0 ? nPairs : 1), st));
+    CB_CUDA(cudaMemsetAsync(T, 0, sizeof(TrainScal), st));
+    int rc = 0;
+    for (int q = 0; q < nPairs && !rc; ++q)
+        rc = pair_forward(lw, Af, status, L, pairsB + (size_t)q * L.PS + L.H, pairsX + (size_t)q * L.PS + L.H, mode, T, dl + q, st);
+    if (!rc && nPairs > 0 && lossHost) rc = cudaMemcpyAsync(lossHost, dl, sizeof(float) * nPairs, cudaMemcpyDeviceToHost, st) != cudaSuccess;
+    cudaStreamSynchronize(st);
+    cudaFreeAsync(T, st); cudaFreeAsync(dl, st);
+    CB_CUDA(cudaStreamSynchronize(st));
+    if (rc) { set_error("evaluation failed"); return 1; }
+    return check_net_error(lw);
+}
+
+int learned_train(LearnedWork& lw, const OpSym& A, const uint8_t* status, const Lat& L, const float* pairsB, const float* pairsX,
+                  int nPairs, int steps, int batch, float lr, unsigned seed, float* lossHost, cudaStream_t st) {
+    if (lw.nLev < 2 || !lw.weights) { set_error("lattice too small for the level pyramid of the learned preconditioner"); return 1; }
+    const long long N = L.N;
+    const int G = grid_for(N, 256);
+    if (!lw.masksReady && level_masks(lw, status, st)) return 1;
+    OpSymF32 Af = cast_operator(lw, A, L, st);
+    NetBuffers& W = *lw.weights;
+    TrainScal* T = nullptr;
+    float *mom = nullptr, *vel = nullptr, *hist = nullptr;
+    CB_CUDA(cudaMallocAsync(&T, sizeof(TrainScal), st));
+    CB_CUDA(cudaMallocAsync(&mom, sizeof(float) * NET_PARAMS, st));
+    CB_CUDA(cudaMallocAsync(&vel, sizeof(float) * NET_PARAMS, st));
+    CB_CUDA(cudaMallocAsync(&hist, sizeof(float) * (steps > 0 ? steps : 1), st));
+    CB_CUDA(cudaMemsetAsync(T, 0, sizeof(TrainScal), st));
+    CB_CUDA(cudaMemsetAsync(mom, 0, sizeof(float) * NET_PARAMS, st));
+    CB_CUDA(cudaMemsetAsync(vel, 0, sizeof(float) * NET_PARAMS, st));
+    unsigned long long rs = seed * 6364136223846793005ull + 1442695040888963407ull;
+    auto next = [&]() { rs = rs * 6364136223846793005ull + 1442695040888963407ull; return (unsigned)(rs >> 33); };
+    const float inv_batch = 1.f / (float)batch;
+    const Scal* S = static_cast<const Scal*>(lw.scal);
+    for (int step = 0; step < steps; ++step) {
+        CB_CUDA(cudaMemsetAsync(W.grad, 0, sizeof(float) * NET_PARAMS, st));
+        if (net_pack_weights(W, st)) return 1;
+        for (int q = 0; q < batch; ++q) {
+            int idx = (int)(next() % (unsigned)nPairs);
+            const float* b = pairsB + (size_t)idx * L.PS + L.H;
+            const float* xs = pairsX + (size_t)idx * L.PS + L.H;
+            if (pair_forward(lw, Af, status, L, b, xs, NET_MODE_NETWORK, T, nullptr, st)) return 1;
+            train_dz_kernel<<<G, 256, 0, st>>>(N, lw.e, status, T, inv_batch, lw.r);
+            // adjoint chain: dL/dw_l = P_l^T dL/dw_(l-1) (into u_l), dL/dy_l = gain_l s dL/dw_l (into w_l)
+            for (int l = 1; l < lw.nLev; ++l) {
+                Level& c = lw.lev[l];
+                const Level& f = lw.lev[l - 1];
+                restrict_kernel<<<restrict_grid(dims_of(c)), 256, 0, st>>>(dims_of(f), dims_of(c), l == 1 ? lw.r : f.u, nullptr, nullptr, 1.f,
+                                                                           c.u, c.w, c.gain, nullptr, nullptr, 0.f, S);
+                if (l >= lw.netFrom && net_backward(c.net, c.w, st)) return 1;
+            }
+        }
+        loss_out_kernel<<<1, 32, 0, st>>>(T, hist, step, inv_batch);
+        adam_kernel<<<grid_for(NET_PARAMS, 256), 256, 0, st>>>(NET_PARAMS, W.params, W.grad, mom, vel, lr, 0.9f, 0.999f, 1e-8f, step + 1);
+        CB_CHECK_LAUNCH();
+    }
+    if (net_pack_weights(W, st)) return 1;
+    if (lossHost && steps > 0) CB_CUDA(cudaMemcpyAsync(lossHost, hist, sizeof(float) * steps, cudaMemcpyDeviceToHost, st));
+    CB_CUDA(cudaStreamSynchronize(st));
+    cudaFreeAsync(T, st); cudaFreeAsync(mom, st); cudaFreeAsync(vel, st); cudaFreeAsync(hist, st);
+    CB_CUDA(cudaStreamSynchronize(st));
+    if (check_net_error(lw)) return 1;
+    lw.haveParams = true;
+    return 0;
+}
+
+}  // namespace cb

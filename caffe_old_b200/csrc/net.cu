@@ -125,6 +125,18 @@ int net_alloc(NetBuffers& nb, const Lat& L, void* (*alloc)(size_t, void*), void*
     return 0;
 }
 
+int net_alloc_shared(NetBuffers& nb, const Lat& L, const NetBuffers& owner, void* (*alloc)(size_t, void*), void* ctx) {
+    nb.L = L;
+    size_t actBytes = (size_t)L.N * 16 * sizeof(__nv_bfloat16);
+    bool ok = true;
+    for (int q = 0; q < 4; ++q) ok = ok && (nb.act[q] = static_cast<__nv_bfloat16*>(alloc(actBytes, ctx)));
+    for (int q = 0; q < 2; ++q) ok = ok && (nb.gz[q] = static_cast<__nv_bfloat16*>(alloc(actBytes, ctx)));
+    ok = ok && (nb.y = static_cast<float*>(alloc(sizeof(float) * (size_t)L.N, ctx)));
+    if (!ok) { set_error("network buffer allocation failed"); return 1; }
+    nb.wfwd = owner.wfwd; nb.wbwd = owner.wbwd; nb.params = owner.params; nb.grad = owner.grad; nb.err = owner.err;
+    return 0;
+}
+
 int net_pack_weights(NetBuffers& nb, cudaStream_t st) {
     pack_weights_kernel<<<dim3(27, NET_LAYERS), 256, 0, st>>>(nb.params, nb.wfwd, nb.wbwd);
     CB_CHECK_LAUNCH();
@@ -141,11 +153,13 @@ static const float* bias_of(const NetBuffers& nb, int l) { return nb.params + (s
 static const __nv_bfloat16* wf_of(const NetBuffers& nb, int l) { return nb.wfwd + (size_t)l * 27 * 256; }
 static const __nv_bfloat16* wb_of(const NetBuffers& nb, int l) { return nb.wbwd + (size_t)l * 27 * 256; }
 
-int net_forward(NetBuffers& nb, cudaStream_t st) {
+int net_forward_if(NetBuffers& nb, const int* skip, cudaStream_t st) {
     for (int l = 0; l < 3; ++l)
-        if (launch_conv3d(nb.L, 0, nb.act[l], wf_of(nb, l), bias_of(nb, l), nb.act[l + 1], nullptr, nullptr, nb.err, st)) return 1;
-    return launch_conv3d(nb.L, 1, nb.act[3], wf_of(nb, 3), bias_of(nb, 3), nullptr, nb.y, nullptr, nb.err, st);
+        if (launch_conv3d(nb.L, 0, nb.act[l], wf_of(nb, l), bias_of(nb, l), nb.act[l + 1], nullptr, nullptr, nb.err, st, skip)) return 1;
+    return launch_conv3d(nb.L, 1, nb.act[3], wf_of(nb, 3), bias_of(nb, 3), nullptr, nb.y, nullptr, nb.err, st, skip);
 }
+
+int net_forward(NetBuffers& nb, cudaStream_t st) { return net_forward_if(nb, nullptr, st); }
 
 static int weight_grad(NetBuffers& nb, int l, const __nv_bfloat16* x, const __nv_bfloat16* dz, cudaStream_t st) {
     const Lat& L = nb.L;

@@ -142,6 +142,45 @@ int caffe_precond_net_apply(int nI, int nJ, int nK, const float* params, const f
 int caffe_precond_net_grad(int nI, int nJ, int nK, const float* params, const float* x2, const float* dy,
                            float* y, float* dparams);
 
+/* Learned preconditioner of the p' solve (p_form CAFFE_P_LEARNED or CAFFE_P_LEARNED_MIXED):
+ * an FP32 flexible Krylov solve inside FP64 refinement, preconditioned by
+ *     M(r) = D^-1 r + sum_l P_l (4^l s y_l),   y_l = net(R_l D^-1 r / s)
+ * on a pyramid of coarsened lattices (l >= 1), with one network (above) serving every level.
+ * No counterpart in the reference: the reference solves p' with its Krylov library only
+ * (src/Math/SparseMatrix.cpp:95-100).  Every solve still reaches p_rtol in the FP64 true
+ * residual; the plain FP64 solve re-runs on the device when the learned one does not.
+ * Parameters: caffe_precond_param_count() floats; NULL removes them (the solve then uses the
+ * Jacobi part alone). */
+int caffe_dev_set_precond(caffe_dev* h, const float* params);
+int caffe_dev_get_precond(caffe_dev* h, float* params);
+/* CAFFE_NET_JACOBI: M = D^-1 (the method without the network); CAFFE_NET_NETWORK (default);
+ * CAFFE_NET_LEVELS: the pyramid with an identity in place of the network. */
+enum { CAFFE_NET_JACOBI = 0, CAFFE_NET_NETWORK = 1, CAFFE_NET_LEVELS = 2 };
+int caffe_dev_set_precond_mode(caffe_dev* h, int mode);
+/* inner_method: 0 automatic (flexible CG for a symmetric p' matrix, flexible BiCGStab with
+ * immersed-boundary ghost rows), 1 flexible CG, 2 flexible BiCGStab.  net_from_level: first
+ * pyramid level (>= 1) that runs the network; finer levels use the identity. */
+int caffe_dev_set_precond_options(caffe_dev* h, int inner_method, int net_from_level);
+/* Training pairs (b, x) with A x = b, kept on the device in FP32.  record_pairs(capacity > 0)
+ * stores the right-hand side and solution of every following p' solve until `capacity` pairs
+ * are held, plus `snapshots` residual/correction pairs (b - A x_k, x - x_k) per solve from
+ * plain re-solves truncated after k = 8, 32, 128, ... iterations; capacity 0 stops recording.
+ * add_pairs uploads host pairs, arrays [n_pairs][nI*nJ*nK]; copy_pairs appends another
+ * handle's pairs (same lattice and device). */
+int caffe_dev_record_pairs(caffe_dev* h, int capacity, int snapshots);
+int caffe_dev_pair_count(caffe_dev* h);
+int caffe_dev_add_pairs(caffe_dev* h, const float* b_pairs, const float* x_pairs, int n_pairs);
+int caffe_dev_copy_pairs(caffe_dev* dst, caffe_dev* src);
+/* Train on the handle's pairs with its current p' operator, on the device: loss per pair
+ * ||M(b) - x||^2_E / ||x||^2_E in the energy norm of the (negated, positive) p' matrix, on its
+ * active-cell block with an immersed body; Adam with learning rate lr, `steps` updates of
+ * `batch` random pairs.  params_inout holds the starting parameters and receives the trained
+ * ones; loss_hist (optional) receives the mean loss of each step.  Afterwards the handle's
+ * solves use the trained parameters. */
+int caffe_dev_train_precond(caffe_dev* h, int steps, int batch, float lr, unsigned seed, float* params_inout, float* loss_hist);
+/* Loss of one application M(b) for every stored pair, in the given mode: loss[pair_count]. */
+int caffe_dev_eval_precond(caffe_dev* h, int mode, float* loss);
+
 /* caffe_ksp7_solve_device without any device allocation.  It has no counterpart in the
  * reference.  For callers that cannot call cudaMalloc/cudaFree from inside a solve -- a program
  * whose own allocator already owns nearly all of HBM, or a time loop that cannot take the

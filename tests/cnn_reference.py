@@ -61,12 +61,15 @@ def conv_T(g, W):
     return out
 
 
-def forward(params, x2, shape, bf=True):
+def forward(params, x2, shape, bf=True, extra_const=None):
+    """extra_const: value of a constant input channel 2 (the level channel), if any."""
     nI, nJ, nK = shape
     layers = unpack(params)
     rnd = bf16 if bf else (lambda a: np.asarray(a, dtype=np.float64))
     x = np.zeros((nK, nJ, nI, C))
     x[..., :2] = rnd(x2.reshape(nK, nJ, nI, 2))
+    if extra_const is not None:
+        x[..., 2] = rnd(np.full((nK, nJ, nI), extra_const))
     acts = [x]
     for l in range(3):
         W, b = layers[l]
