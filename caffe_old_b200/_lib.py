@@ -102,7 +102,7 @@ def lib():
     L.caffe_dev_set_precond.argtypes = [vp, vp]
     L.caffe_dev_get_precond.argtypes = [vp, vp]
     L.caffe_dev_set_precond_mode.argtypes = [vp, ci]
-    L.caffe_dev_set_precond_options.argtypes = [vp, ci, ci]
+    L.caffe_dev_set_precond_options.argtypes = [vp, ci, ci, ci]
     L.caffe_dev_record_pairs.argtypes = [vp, ci, ci]
     L.caffe_dev_pair_count.argtypes = [vp]
     L.caffe_dev_add_pairs.argtypes = [vp, vp, vp, ci]

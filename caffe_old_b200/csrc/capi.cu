@@ -2,6 +2,7 @@
 // the solver fields, both linear systems and the Krylov workspace in HBM, and one stream.
 // One time step of Simple / Piso / IbPiso is a fixed sequence of kernel launches on that
 // stream with no host synchronisation inside it.
+#include <algorithm>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -40,6 +41,36 @@ struct StepAcc {
 __global__ void pair_cast_kernel(long long N, const double* b, const double* x, float* pb, float* px) {
     long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (c < N) { pb[c] = (float)b[c]; px[c] = (float)x[c]; }
+}
+
+// zero-mean gauge of a singular p' solution: block partial sums, mean, subtraction
+__global__ void __launch_bounds__(256) gauge_partial_kernel(const double* x, long long N, double* part) {
+    __shared__ double sm[256];
+    double s = 0.;
+    for (long long c = blockIdx.x * 256ll + threadIdx.x; c < N; c += (long long)gridDim.x * 256) s += x[c];
+    sm[threadIdx.x] = s;
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w) sm[threadIdx.x] += sm[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[blockIdx.x] = sm[0];
+}
+__global__ void __launch_bounds__(256) gauge_mean_kernel(double* part, int nblk, long long N) {
+    __shared__ double sm[256];
+    double s = 0.;
+    for (int b = threadIdx.x; b < nblk; b += 256) s += part[b];
+    sm[threadIdx.x] = s;
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w) sm[threadIdx.x] += sm[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[nblk] = sm[0] / (double)N;
+}
+__global__ void gauge_apply_kernel(double* x, long long N, const double* mean) {
+    long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (c < N) x[c] = x[c] - *mean;
 }
 
 __global__ void acc_kernel(const KspOut* o, StepAcc* acc, int kind, int nr) {
@@ -130,6 +161,7 @@ struct caffe_dev {
     int pairCap = 0, pairCount = 0;
     int pairSnapshots = 0;       // intermediate-iterate pairs per recorded solve
     double* snapX = nullptr;     // iterate of a truncated re-solve (one FP64 cell plane)
+    double* gaugePart = nullptr; // partial sums of the zero-mean gauge (1024 + 1 doubles)
     bool recording = false;
     // reductions and statistics
     double* chunkMax = nullptr;
@@ -367,6 +399,16 @@ int ph_solve_pcorr(caffe_dev* h) {
         rc = ksp_bicgstab_sym(A, h->pb, h->pc, h->L, h->kw, h->cs.p_rtol, h->cs.maxit, h->st, project);
     }
     if (rc) return rc;
+    if (project) {
+        // singular system: the solution's constant is fixed to zero mean (the discrete gradient
+        // on meshes with non-planar faces is not blind to it), whichever Krylov method ran
+        if (!h->gaugePart && !(h->gaugePart = h->dalloc<double>(1025))) { set_error("allocation failed"); return 1; }
+        int nb = (int)std::min<long long>(1024, (h->L.N + 255) / 256);
+        gauge_partial_kernel<<<nb, 256, 0, h->st>>>(h->pc, h->L.N, h->gaugePart);
+        gauge_mean_kernel<<<1, 256, 0, h->st>>>(h->gaugePart, nb, h->L.N);
+        gauge_apply_kernel<<<grid_for(h->L.N, 256), 256, 0, h->st>>>(h->pc, h->L.N, h->gaugePart + nb);
+        CB_CHECK_LAUNCH();
+    }
     acc_kernel<<<1, 32, 0, h->st>>>(h->kw.out, h->acc, 1, 1);
     CB_CHECK_LAUNCH();
     if (h->recording && h->pairCount < h->pairCap) {
@@ -821,14 +863,20 @@ int caffe_dev_set_precond_mode(caffe_dev* h, int mode) {
     return 0;
 }
 
-int caffe_dev_set_precond_options(caffe_dev* h, int inner_method, int net_from_level) {
+int caffe_dev_set_precond_options(caffe_dev* h, int inner_method, int net_from_level, int restart) {
     g_err.clear();
     if (!h) { set_error("handle is NULL"); return 1; }
-    if (inner_method < LEARN_INNER_AUTO || inner_method > LEARN_INNER_BICGSTAB || net_from_level < 1) { set_error("invalid options"); return 1; }
+    if (inner_method < LEARN_INNER_AUTO || inner_method > LEARN_INNER_FGMRES || net_from_level < 1 || restart < 1 ||
+        restart > FGMRES_MAX_RESTART) {
+        set_error("invalid options");
+        return 1;
+    }
     CB_CUDA(cudaSetDevice(h->device));
     if (h->ensure_learned()) return 1;
+    if (h->lw.fgCap > 0 && restart > h->lw.fgCap) { set_error("the FGMRES restart length cannot grow after the first FGMRES solve"); return 1; }
     h->lw.inner = inner_method;
     h->lw.netFrom = net_from_level;
+    h->lw.restart = restart;
     return 0;
 }
 

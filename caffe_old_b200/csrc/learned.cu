@@ -700,6 +700,160 @@ __global__ void publish_kernel(const Scal* S, KspOut* out) {
     out->status[0] = S->status;
 }
 
+// ---------------------------------------------------------------- inner FGMRES (FP32)
+// Right-preconditioned flexible GMRES (Saad 1993): z_j = M(v_j), w = A z_j, classical
+// Gram-Schmidt against v_0..v_j with FP64 dot accumulation, Givens rotations on the
+// Hessenberg column, x = sum y_j z_j at the end of the cycle.  It tolerates any change of M
+// between applications, the case of the BF16 network with ReLU.
+constexpr int FGM = FGMRES_MAX_RESTART;
+constexpr int FG_DOT_BLOCKS = 592;    // 4 x 148 SMs: cell chunks of the multi-dot kernel
+
+struct FgScal {
+    double H[(FGM + 1) * FGM];   // column-major: H[j * (FGM + 1) + i]
+    double cs[FGM], sn[FGM], g[FGM + 1], y[FGM];
+    double beta;
+    int jEnd;
+};
+
+// v_0 = r / ||r|| (||r||^2 from the outer residual), e = 0
+__global__ void fg_init_kernel(long long N, const float* r, float* v0, float* e, const Scal* S, FgScal* F) {
+    if (S->done) return;
+    long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    double beta = sqrt(S->rr64);
+    if (c == 0) { F->beta = beta; F->g[0] = beta; F->jEnd = 0; }
+    if (c < N) { v0[c] = (float)((double)r[c] / beta); e[c] = 0.f; }
+}
+__global__ void fg_start_finish(Scal* S, double eta, const double* nact) {
+    if (S->done || threadIdx.x != 0) return;
+    S->rr0 = S->rr64; S->rr = S->rr64;
+    S->tin2 = eta * eta * S->rr64;
+    S->nact = *nact;
+    S->done = !(S->rr64 > 0.);
+}
+// partial sum of (D^-1 x)^2 over active cells (the network scale of M(x))
+__global__ void __launch_bounds__(LB) scale_partial_kernel(long long N, const float* x, const float* invD, const uint8_t* st, double* part,
+                                                           const Scal* S) {
+    if (S->done) return;
+    double a[1] = {0.};
+    for (long long c = blockIdx.x * (long long)LB + threadIdx.x; c < N; c += (long long)gridDim.x * LB)
+        if (is_active(st, c)) { double u = (double)__ldg(invD + c) * x[c]; a[0] += u * u; }
+    block_sums(a, 1, part);
+}
+// w = A z (FP32, with the ghost rows)
+__global__ void __launch_bounds__(LB) fg_spmv_kernel(OpSymF32 A, long long N, const float* z, float* w, const Scal* S) {
+    if (S->done) return;
+    for (long long c = blockIdx.x * (long long)LB + threadIdx.x; c < N; c += (long long)gridDim.x * LB)
+        w[c] = applyF(A, c, [&](long long e_) { return z[e_]; });
+}
+// part[i * FG_DOT_BLOCKS + chunk] = sum over the chunk of w . v_i, i = blockIdx.x
+__global__ void __launch_bounds__(LB) fg_dots_kernel(long long N, const float* w, const float* V, long long PS, double* part, const Scal* S) {
+    if (S->done) return;
+    const int i = blockIdx.x;
+    const long long chunk = (N + gridDim.y - 1) / gridDim.y;
+    const long long c0 = blockIdx.y * chunk, c1 = min(N, c0 + chunk);
+    const float* v = V + i * PS;
+    double a = 0.;
+    for (long long c = c0 + threadIdx.x; c < c1; c += LB) a += (double)w[c] * v[c];
+    __shared__ double sm[LB / 32];
+    for (int off = 16; off > 0; off >>= 1) a += __shfl_xor_sync(0xffffffffu, a, off);
+    if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = a;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.;
+        for (int u = 0; u < LB / 32; ++u) t += sm[u];
+        part[(size_t)i * gridDim.y + blockIdx.y] = t;
+    }
+}
+// H[0..j][j] from the partials (block q sums entry q)
+__global__ void fg_dots_finish(const double* part, int nchunk, int j, FgScal* F, const Scal* S) {
+    if (S->done) return;
+    const int i = blockIdx.x;
+    __shared__ double sm[LB];
+    double t = 0.;
+    for (int b = threadIdx.x; b < nchunk; b += blockDim.x) t += part[(size_t)i * nchunk + b];
+    sm[threadIdx.x] = t;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s) sm[threadIdx.x] += sm[threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) F->H[(size_t)j * (FGM + 1) + i] = sm[0];
+}
+// w -= sum_i H[i][j] v_i; partial ||w||^2
+__global__ void __launch_bounds__(LB) fg_orth_kernel(long long N, float* w, const float* V, long long PS, int j, const FgScal* F, double* part,
+                                                     const Scal* S) {
+    if (S->done) return;
+    __shared__ float h[FGM + 1];
+    for (int i = threadIdx.x; i <= j; i += blockDim.x) h[i] = (float)F->H[(size_t)j * (FGM + 1) + i];
+    __syncthreads();
+    double a[1] = {0.};
+    for (long long c = blockIdx.x * (long long)LB + threadIdx.x; c < N; c += (long long)gridDim.x * LB) {
+        float x = w[c];
+        for (int i = 0; i <= j; ++i) x -= h[i] * V[i * PS + c];
+        w[c] = x;
+        a[0] += (double)x * x;
+    }
+    block_sums(a, 1, part);
+}
+// h_{j+1,j}, rotations, residual estimate, stop test
+__global__ void fg_step_finish(const double* part, int nblk, int j, int m, int max_iters, FgScal* F, Scal* S) {
+    if (S->done) return;
+    double t[1];
+    totals(part, nblk, 1, t);
+    if (threadIdx.x != 0) return;
+    double* Hc = F->H + (size_t)j * (FGM + 1);
+    double hn = sqrt(t[0]);
+    Hc[j + 1] = hn;
+    for (int i = 0; i < j; ++i) {
+        double a = Hc[i], b = Hc[i + 1];
+        Hc[i] = F->cs[i] * a + F->sn[i] * b;
+        Hc[i + 1] = -F->sn[i] * a + F->cs[i] * b;
+    }
+    double a = Hc[j], b = Hc[j + 1];
+    double r = sqrt(a * a + b * b);
+    double c = r > 0. ? a / r : 1., sn = r > 0. ? b / r : 0.;
+    F->cs[j] = c; F->sn[j] = sn;
+    Hc[j] = r; Hc[j + 1] = 0.;
+    F->g[j + 1] = -sn * F->g[j];
+    F->g[j] = c * F->g[j];
+    double res2 = F->g[j + 1] * F->g[j + 1];
+    S->rr = res2;
+    S->iters += 1;
+    F->jEnd = j + 1;
+    bool stop = res2 <= S->tin2 || j + 1 >= m || S->iters >= max_iters || !(hn > 0.) || res2 != res2;
+    if (stop) S->done = 1;
+    S->alpha = hn > 0. ? 1. / hn : 0.;   // scale of the next basis vector
+}
+// v_{j+1} = w / h_{j+1,j}
+__global__ void fg_scale_kernel(long long N, const float* w, float* vn, const Scal* S) {
+    if (S->done) return;
+    long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (c < N) vn[c] = (float)((double)w[c] * S->alpha);
+}
+// y = R^-1 g (upper triangular, jEnd x jEnd)
+__global__ void fg_solve_kernel(FgScal* F) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const int n = F->jEnd;
+    for (int i = n - 1; i >= 0; --i) {
+        double s = F->g[i];
+        for (int k = i + 1; k < n; ++k) s -= F->H[(size_t)k * (FGM + 1) + i] * F->y[k];
+        double d = F->H[(size_t)i * (FGM + 1) + i];
+        F->y[i] = d != 0. ? s / d : 0.;
+    }
+}
+// e = sum_i y_i z_i
+__global__ void __launch_bounds__(LB) fg_combine_kernel(long long N, const float* Z, long long PS, const FgScal* F, float* e) {
+    __shared__ float y[FGM];
+    const int n = F->jEnd;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) y[i] = (float)F->y[i];
+    __syncthreads();
+    for (long long c = blockIdx.x * (long long)LB + threadIdx.x; c < N; c += (long long)gridDim.x * LB) {
+        float a = 0.f;
+        for (int i = 0; i < n; ++i) a += y[i] * Z[i * PS + c];
+        e[c] = a;
+    }
+}
+
 // ---------------------------------------------------------------- pyramid host side
 Dims3 dims_of(const Level& l) { return Dims3{l.n[0], l.n[1], l.n[2]}; }
 
@@ -757,6 +911,8 @@ OpSymF32 cast_operator(LearnedWork& lw, const OpSym& A, const Lat& L, cudaStream
 
 int learned_alloc(LearnedWork& lw, const Lat& L, void* (*alloc)(size_t, void*), void* ctx) {
     lw.L = L;
+    lw.alloc = alloc;
+    lw.allocCtx = ctx;
     auto fcell = [&]() -> float* {
         float* b = static_cast<float*>(alloc(sizeof(float) * (size_t)L.PS, ctx));
         return b ? b + L.H : nullptr;
@@ -809,6 +965,21 @@ void learned_free_host(LearnedWork& lw) {
     lw.hostScal = nullptr;
 }
 
+namespace {
+int fg_alloc(LearnedWork& lw, int m) {
+    if (lw.fgCap >= m) return 0;
+    if (lw.fgCap > 0) { set_error("FGMRES restart length cannot grow after the first FGMRES solve"); return 1; }
+    const Lat& L = lw.L;
+    lw.fgV = static_cast<float*>(lw.alloc(sizeof(float) * (size_t)L.PS * (m + 1), lw.allocCtx));
+    lw.fgZ = static_cast<float*>(lw.alloc(sizeof(float) * (size_t)L.PS * m, lw.allocCtx));
+    lw.fgScal = lw.alloc(sizeof(FgScal), lw.allocCtx);
+    lw.fgPart = static_cast<double*>(lw.alloc(sizeof(double) * (size_t)(FGM + 1) * FG_DOT_BLOCKS, lw.allocCtx));
+    if (!lw.fgV || !lw.fgZ || !lw.fgScal || !lw.fgPart) { set_error("FGMRES workspace allocation failed"); return 1; }
+    lw.fgCap = m;
+    return 0;
+}
+}  // namespace
+
 int learned_solve(LearnedWork& lw, const OpSym& A, const uint8_t* status, const double* b, double* x, const Lat& L, double rtol, int maxit,
                   double eta, int project, int mode, KspOut* out, cudaStream_t st) {
     const long long N = L.N;
@@ -831,7 +1002,16 @@ int learned_solve(LearnedWork& lw, const OpSym& A, const uint8_t* status, const 
     CB_CHECK_LAUNCH();
     const Dims3 fd = dims_of(lw.lev[0]), cd = level1_dims(lw);
     const float* w1 = level_w1(lw, mode);
-    const bool symmetric = lw.inner == LEARN_INNER_FCG || (lw.inner == LEARN_INNER_AUTO && A.gh.n == 0);
+    const bool nonsym = A.gh.n > 0;
+    int method = lw.inner;
+    if (method == LEARN_INNER_AUTO)
+        method = !nonsym ? LEARN_INNER_FCG : (mode == NET_MODE_NETWORK ? LEARN_INNER_FGMRES : LEARN_INNER_BICGSTAB);
+    const bool symmetric = method == LEARN_INNER_FCG;
+    const bool fgmres = method == LEARN_INNER_FGMRES;
+    const int m = lw.restart < 1 ? 1 : (lw.restart > FGM ? FGM : lw.restart);
+    if (fgmres && fg_alloc(lw, m)) return 1;
+    FgScal* F = static_cast<FgScal*>(lw.fgScal);
+    const long long PS = L.PS;
     if (!symmetric) {
         count_active_kernel<<<nb, LB, 0, st>>>(N, status, lw.part);
         count_finish<<<1, LB, 0, st>>>(lw.part, nb, lw.mean + 1);
@@ -865,6 +1045,38 @@ int learned_solve(LearnedWork& lw, const OpSym& A, const uint8_t* status, const 
         }
         if (etaK > 0.5) etaK = 0.5;
         int cur = 0;
+        if (fgmres) {
+            fg_init_kernel<<<G, 256, 0, st>>>(N, lw.r, lw.fgV + L.H, lw.e, S, F);
+            fg_start_finish<<<1, 32, 0, st>>>(S, etaK, lw.mean + 1);
+            CB_CHECK_LAUNCH();
+            for (int j = 0; j < m; ++j) {
+                float* vj = lw.fgV + j * PS + L.H;
+                float* zj = lw.fgZ + j * PS + L.H;
+                scale_partial_kernel<<<nb, LB, 0, st>>>(N, vj, lw.invD, status, lw.part, S);
+                scale_finish<<<1, LB, 0, st>>>(lw.part, nb, S);
+                if (apply_levels(lw, vj, status, mode, S, st)) return 1;
+                bs_z_kernel<<<nb, LB, 0, st>>>(N, fd, cd, vj, lw.invD, status, w1, zj, S);
+                fg_spmv_kernel<<<nb, LB, 0, st>>>(Af, N, zj, lw.t, S);
+                fg_dots_kernel<<<dim3(j + 1, FG_DOT_BLOCKS), LB, 0, st>>>(N, lw.t, lw.fgV + L.H, PS, lw.fgPart, S);
+                fg_dots_finish<<<j + 1, LB, 0, st>>>(lw.fgPart, FG_DOT_BLOCKS, j, F, S);
+                fg_orth_kernel<<<nb, LB, 0, st>>>(N, lw.t, lw.fgV + L.H, PS, j, F, lw.part, S);
+                fg_step_finish<<<1, LB, 0, st>>>(lw.part, nb, j, m, maxit, F, S);
+                fg_scale_kernel<<<G, 256, 0, st>>>(N, lw.t, lw.fgV + (j + 1) * PS + L.H, S);
+                if ((j & 7) == 7 || j == m - 1) {
+                    CB_CHECK_LAUNCH();
+                    CB_CUDA(cudaMemcpyAsync(lw.hostScal, S, sizeof(Scal), cudaMemcpyDeviceToHost, st));
+                    CB_CUDA(cudaStreamSynchronize(st));
+                    if (static_cast<Scal*>(lw.hostScal)->done) break;
+                }
+            }
+            fg_solve_kernel<<<1, 32, 0, st>>>(F);
+            fg_combine_kernel<<<nb, LB, 0, st>>>(N, lw.fgZ + L.H, PS, F, lw.e);
+            CB_CHECK_LAUNCH();
+            outer_update_kernel<<<G, 256, 0, st>>>(N, x, lw.e, S);
+            int zero = 0;
+            CB_CUDA(cudaMemcpyAsync(&S->done, &zero, sizeof(int), cudaMemcpyHostToDevice, st));
+            continue;
+        }
         if (symmetric) {
             inner_start_kernel<<<nb, LB, 0, st>>>(N, lw.r, lw.invD, status, lw.e, lw.p[0], lw.q[0], lw.part, S);
             inner_start_finish_kernel<<<1, LB, 0, st>>>(lw.part, nb, S, etaK);

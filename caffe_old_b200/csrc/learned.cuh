@@ -31,8 +31,11 @@ struct Level {
 };
 
 enum { NET_MODE_JACOBI = 0, NET_MODE_NETWORK = 1, NET_MODE_LEVELS = 2 };
-// inner Krylov method: flexible CG for a symmetric operator, flexible BiCGStab otherwise
-enum { LEARN_INNER_AUTO = 0, LEARN_INNER_FCG = 1, LEARN_INNER_BICGSTAB = 2 };
+// inner Krylov method: automatic = flexible CG for a symmetric operator; for a non-symmetric
+// one, FGMRES when the network runs (a preconditioner that varies between applications) and
+// BiCGStab otherwise (a fixed linear preconditioner)
+enum { LEARN_INNER_AUTO = 0, LEARN_INNER_FCG = 1, LEARN_INNER_BICGSTAB = 2, LEARN_INNER_FGMRES = 3 };
+constexpr int FGMRES_MAX_RESTART = 64;
 
 struct LearnedWork {
     Lat L;
@@ -56,13 +59,23 @@ struct LearnedWork {
     bool haveParams = false;
     int netFrom = 1;             // first level that runs the network (finer levels: identity)
     int inner = LEARN_INNER_AUTO;
+    int restart = 30;            // FGMRES cycle length (one cycle per FP64 refinement pass)
+    // FGMRES basis (restart + 1 planes) and preconditioned vectors (restart planes), one
+    // allocation each, planes PS apart; scalar record and dot partials
+    float* fgV = nullptr;
+    float* fgZ = nullptr;
+    int fgCap = 0;
+    void* fgScal = nullptr;
+    double* fgPart = nullptr;
+    void* (*alloc)(size_t, void*) = nullptr;
+    void* allocCtx = nullptr;
     int lastIters = 0, lastOuter = 0;
 };
 
 int learned_alloc(LearnedWork& lw, const Lat& L, void* (*alloc)(size_t, void*), void* ctx);
 void learned_free_host(LearnedWork& lw);
-// FP64 refinement around an FP32 flexible Krylov solve (flexible CG for the symmetric
-// operator, flexible BiCGStab when immersed-boundary ghost rows make it non-symmetric) with
+// FP64 refinement around an FP32 inner Krylov solve (flexible CG for the symmetric operator;
+// FGMRES or BiCGStab when immersed-boundary ghost rows make it non-symmetric) with
 //   M(r) = D^-1 r + sum_l P_l (gain_l s y_l),  y_l = net(R_l D^-1 r / s) (mode NETWORK),
 //   y_l = R_l D^-1 r / s (mode LEVELS), nothing (mode JACOBI).
 // Writes iterations / outer passes / relative residual / status to *out (device).

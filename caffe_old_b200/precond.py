@@ -25,7 +25,7 @@ LAYER_PARAMS = TAPS * CHANNELS * CHANNELS + CHANNELS
 PARAMS = LAYERS * LAYER_PARAMS
 
 MODES = {"jacobi": 0, "network": 1, "levels": 2}
-INNER = {"auto": 0, "fcg": 1, "bicgstab": 2}
+INNER = {"auto": 0, "fcg": 1, "bicgstab": 2, "fgmres": 3}
 
 DEFAULT_WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "precond_params.npy")
 
@@ -96,10 +96,11 @@ def set_mode(solver, mode: str) -> None:
     _check(lib().caffe_dev_set_precond_mode(solver._h, MODES[mode]), "set_precond_mode")
 
 
-def set_options(solver, inner: str = "auto", net_from_level: int = 1) -> None:
-    """Inner Krylov method of the learned solve and the first pyramid level that runs the
-    network (finer levels use the identity)."""
-    _check(lib().caffe_dev_set_precond_options(solver._h, INNER[inner], int(net_from_level)), "set_precond_options")
+def set_options(solver, inner: str = "auto", net_from_level: int = 1, restart: int = 30) -> None:
+    """Inner Krylov method of the learned solve, the first pyramid level that runs the
+    network (finer levels use the identity) and the FGMRES cycle length."""
+    _check(lib().caffe_dev_set_precond_options(solver._h, INNER[inner], int(net_from_level), int(restart)),
+           "set_precond_options")
 
 
 def record_pairs(solver, capacity: int, snapshots: int = 0) -> None:

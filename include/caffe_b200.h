@@ -157,10 +157,13 @@ int caffe_dev_get_precond(caffe_dev* h, float* params);
  * CAFFE_NET_LEVELS: the pyramid with an identity in place of the network. */
 enum { CAFFE_NET_JACOBI = 0, CAFFE_NET_NETWORK = 1, CAFFE_NET_LEVELS = 2 };
 int caffe_dev_set_precond_mode(caffe_dev* h, int mode);
-/* inner_method: 0 automatic (flexible CG for a symmetric p' matrix, flexible BiCGStab with
- * immersed-boundary ghost rows), 1 flexible CG, 2 flexible BiCGStab.  net_from_level: first
- * pyramid level (>= 1) that runs the network; finer levels use the identity. */
-int caffe_dev_set_precond_options(caffe_dev* h, int inner_method, int net_from_level);
+/* inner_method: 0 automatic (flexible CG for a symmetric p' matrix; with immersed-boundary
+ * ghost rows, FGMRES when the network runs and BiCGStab otherwise), 1 flexible CG,
+ * 2 BiCGStab (right-preconditioned; needs a fixed linear preconditioner), 3 FGMRES.
+ * net_from_level: first pyramid level (>= 1) that runs the network; finer levels use the
+ * identity.  restart: FGMRES cycle length, 1..64 (one cycle per FP64 refinement pass; it
+ * cannot grow after the handle's first FGMRES solve). */
+int caffe_dev_set_precond_options(caffe_dev* h, int inner_method, int net_from_level, int restart);
 /* Training pairs (b, x) with A x = b, kept on the device in FP32.  record_pairs(capacity > 0)
  * stores the right-hand side and solution of every following p' solve until `capacity` pairs
  * are held, plus `snapshots` residual/correction pairs (b - A x_k, x - x_k) per solve from

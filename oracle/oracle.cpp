@@ -1101,6 +1101,14 @@ struct Solver {
             for (double& v : bv[0]) v -= mean;
         }
         pStats = kspSolve(cs.p_method, A[1], bv[0], xv[0], cs.p_rtol, cs.maxit);
+        if (pSingular()) {
+            // the solution is defined up to a constant, and on meshes with non-planar faces the
+            // discrete gradient (sum of face values times area vectors) is not blind to that
+            // constant: it is fixed to zero mean so that every Krylov method gives the same p'
+            std::vector<double> ones(xv[0].size(), 1.);
+            double mean = dotv(xv[0], ones) / (double)xv[0].size();
+            for (double& v : xv[0]) v -= mean;
+        }
         pItersLast = pStats.iters; pItersTotal += pStats.iters; ++nPSolves;
         pResMax = std::max(pResMax, pStats.rel_res);
         for (int c = 0; c < N; ++c) if (!inactive(c)) pc.c[c] = xv[0][row[c]];
