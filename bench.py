@@ -1,17 +1,22 @@
 #!/usr/bin/env python
-"""Benchmark of the B200 path: time-steps/s (and p-solve ms) with every linear solve
-taken to a 1e-8 true relative residual, on one GPU per rank.
+"""Benchmark of the B200 path: time-steps/s and p-solve ms with every pressure-correction
+solve taken to a 1e-8 true relative residual (FP64), on one GPU per rank.
 
-Default workload: 3-D lid-driven cavity, 128^3 cells, Re = 400, PISO (1 inner iteration,
-2 pressure corrections), central convection, Jacobi-BiCGStab momentum, Jacobi-PCG
-pressure correction, dt = 1e-3, synthetic (no dataset involved), plain FP64.
+Default workload: flow over an immersed-boundary sphere, 384 x 256 x 256 = 25.2M cells,
+Re = 300, IB-PISO (2 inner iterations, 3 pressure corrections), dt = 2e-3, synthetic
+(seeded mesh and case, no dataset), pressure correction in the learned + mixed-precision
+form (FP32 inner Krylov solve with the level-pyramid preconditioner inside FP64 iterative
+refinement).  The same steps from rest are also run with the plain FP64 pressure solve
+(--compare-fp64 steps) and both are reported.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
-                  [--workload c2|c1|c3|c5] [--p-form fp64|mixed|...] [--size n]
+                  [--workload c5|c2|c1|c3] [--p-form learned_mixed|fp64|mixed|learned]
+                  [--precond levels|network|jacobi] [--inner auto|fcg|bicgstab|fgmres]
+                  [--params file.npy] [--size n] [--compare-fp64 K]
 
 One JSON line on rank 0.  --impl reference times the CPU restatement of the reference
 path (the reference itself cannot be built here: it needs MPI, PETSc and Boost) on the
-host cores, on the same workload.
+host cores, on a reduced lattice of the same workload, scaled to the full lattice.
 """
 from __future__ import annotations
 
@@ -68,6 +73,19 @@ def workload(name: str, size: int | None, p_form: str):
         raise SystemExit(f"unknown workload {name}")
     spec = spec.replace(p_form=p_form)
     return nodes, spec, label + f"_{p_form}"
+
+
+def sample_workload(name: str, size: int | None):
+    """Reduced lattice of the same workload for the CPU baseline (1/512 of the cells for the
+    25M-cell sphere, 1/64 for the cavities)."""
+    if name == "c5":
+        full = (384, 256, 256) if not size else (size * 3 // 2, size, size)
+        return workload(name, max(8, full[1] // 8), "fp64"), full
+    if name in ("c2", "c3"):
+        n = size or 128
+        return workload(name, max(8, n // 4), "fp64"), (n, n, n)
+    n = size or 64
+    return workload(name, n, "fp64"), (n, n, 1)
 
 
 class ClockSampler:
@@ -148,71 +166,122 @@ def barrier(pg):
         pg.barrier()
 
 
-def cpu_baseline(nodes, spec, steps: int = 1) -> dict:
-    """The CPU restatement of the reference path (oracle) on the host cores, same workload."""
+def _oracle_steps(nodes, spec, steps: int, budget_s: float):
     from oracle import oracle as O
     O.build()
     threads = os.cpu_count() or 1
     O.set_threads(threads)
     s = O.OracleSolver(nodes, spec)
-    t = time.perf_counter()
+    times, iters = [], []
+    t_all = time.perf_counter()
     for _ in range(steps):
+        t = time.perf_counter()
         s.solve()
-    dt = time.perf_counter() - t
-    st = s.stats()
+        times.append(time.perf_counter() - t)
+        iters.append(int(s.stats()["p_iters_total"]))
+        if time.perf_counter() - t_all > budget_s:
+            break
     s.close()
-    return {"value": steps / dt, "unit": "time-steps/s", "cores": threads, "kind": "port",
-            "sample": f"{steps} time step(s) from rest of the same workload, oracle restatement (C++ -O2, OpenMP), "
-                      f"{dt:.1f} s, p' iterations in the last step {int(st['p_iters_total'])}"}
+    return times, iters, threads
+
+
+def scaled_cpu(args, steps: int, budget_s: float) -> dict:
+    """The CPU restatement of the reference path (oracle, C++ -O2 with OpenMP on every host
+    core) timed on a reduced lattice of the same workload, scaled to the full lattice by
+    cells x Krylov iterations: time per step grows with the cell count and, for these
+    Jacobi-preconditioned Krylov solves, iterations grow with the lattice's linear size."""
+    (nodes, spec, label), full = sample_workload(args.workload, args.size)
+    sample_cells = int(np.prod([d - 1 for d in nodes.shape[:3]]))
+    full_cells = int(np.prod(full))
+    times, iters, threads = _oracle_steps(nodes, spec, steps, budget_s)
+    t_step = sum(times) / len(times)
+    linear = (full_cells / sample_cells) ** (1.0 / 3.0) if full[2] > 1 else (full_cells / sample_cells) ** 0.5
+    scale = (full_cells / sample_cells) * linear
+    value = 1.0 / (t_step * scale)
+    return {"value": value, "unit": "time-steps/s", "cores": threads, "kind": "port",
+            "sample": f"{len(times)} step(s) from rest of the same case on a {nodes.shape[2]-1}x{nodes.shape[1]-1}x{nodes.shape[0]-1} "
+                      f"lattice ({sample_cells} cells): {t_step:.2f} s/step, p' iterations/step {iters}; scaled to "
+                      f"{full_cells} cells by cells x linear size = x{scale:.0f} (oracle restatement, C++ -O2, OpenMP)",
+            "sample_s_per_step": t_step, "scale_factor": scale}
+
+
+def case_label(args) -> str:
+    if args.workload == "c5":
+        dims = (384, 256, 256) if not args.size else (args.size * 3 // 2, args.size, args.size)
+        return f"ibpiso_sphere_{dims[0]}x{dims[1]}x{dims[2]}_re300_{args.p_form}"
+    return workload(args.workload, args.size, args.p_form)[2]
 
 
 def run_reference(args, world, rank, pg):
     if rank != 0:
         return
-    nodes, spec, label = workload(args.workload, args.size, "fp64")
-    from oracle import oracle as O
-    O.build()
-    threads = os.cpu_count() or 1
-    O.set_threads(threads)
-    s = O.OracleSolver(nodes, spec)
-    budget = float(os.environ.get("CAFFE_REF_BUDGET_S", "150"))
-    for _ in range(min(args.warmup, 1)):
-        s.solve()
-    times = []
-    t_all = time.perf_counter()
-    for _ in range(args.steps):
-        t = time.perf_counter()
-        s.solve()
-        times.append(time.perf_counter() - t)
-        if time.perf_counter() - t_all > budget:
-            break
-    total = sum(times)
-    value = len(times) / total
+    budget = float(os.environ.get("CAFFE_REF_BUDGET_S", "120"))
+    cpu = scaled_cpu(args, max(1, args.steps), budget)
+    full_label = case_label(args)
+    value = cpu["value"]
     line = {
         "impl": "reference", "metric": "time-steps/s at 1e-8 true relative residual", "value": value,
-        "unit": "time-steps/s", "n_gpus": args.gpus, "steps": len(times), "warmup": min(args.warmup, 1),
-        "ms_per_step": 1e3 * total / len(times), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64", "data": "synthetic", "config": {"workload": label, "cells": int(np.prod([d - 1 for d in nodes.shape[:3]]))},
-        "cpu_baseline": {"value": value, "unit": "time-steps/s", "cores": threads, "kind": "port",
-                         "sample": f"{len(times)} of {args.steps} requested steps (time-bounded at {budget:.0f} s), "
-                                   "CPU restatement of the reference path; the reference binary needs MPI, PETSc and Boost, "
-                                   "absent on this image"},
+        "unit": "time-steps/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": 0,
+        "ms_per_step": 1e3 / value, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic", "config": {"workload": full_label, "reference_path": "plain FP64 (CPU restatement)"},
+        "cpu_baseline": {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")},
         "e2e": {"value": value, "unit": "time-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
 
 
+# algorithmic bytes per cell and inner iteration of the learned solve (FP32 vectors, the
+# level pyramid's restriction reads and the prolonged term's reads included; coarse levels
+# excluded): flexible BiCGStab 170 B (two preconditioner applications), flexible CG 110 B
+LEARNED_BYTES = {"bicgstab": 170.0, "fcg": 110.0}
+
+
+def configure_precond(dev, args):
+    from caffe_old_b200 import precond as P
+    if not args.p_form.startswith("learned"):
+        return None
+    params = None
+    if args.params:
+        params = np.load(args.params).astype(np.float32)
+    elif args.precond == "network":
+        params = P.load_default()
+        if params is None:
+            params = P.identity_params(0)
+    if params is not None:
+        P.set_params(dev, params)
+    P.set_mode(dev, args.precond)
+    P.set_options(dev, args.inner, args.net_from, args.restart)
+    return params
+
+
+def inner_method(spec, args):
+    if args.inner != "auto":
+        return args.inner
+    if spec.kind != "ibpiso":
+        return "fcg"
+    return "fgmres" if args.precond == "network" else "bicgstab"
+
+
 def run_b200(args, world, rank, local, pg):
     import torch
+    from caffe_old_b200 import _lib
     from caffe_old_b200.solver import make_solver
     torch.cuda.set_device(local)
     nodes, spec, label = workload(args.workload, args.size, args.p_form)
     dev = make_solver(nodes, spec, device=local)
+    configure_precond(dev, args)
     N = dev.ncells
     stream = torch.cuda.ExternalStream(dev.stream, device=local)
+    per_step = []
+
+    def record(tag):
+        st = dev.last_stats
+        per_step.append({"phase": tag, "p_ms": round(st["p_ms"], 2), "p_iters": st["p_iters_total"], "p_solves": st["p_solves"],
+                         "fallbacks": st["fallbacks"], "step_ms": round(st["step_ms"], 2), "p_res_max": st["p_res_max"]})
 
     for _ in range(args.warmup):
         dev.solve()
+        record("warmup")
     dev.synchronize()
     barrier(pg)
     sampler = ClockSampler(local)
@@ -220,34 +289,43 @@ def run_b200(args, world, rank, local, pg):
     time.sleep(0.3)
     t0 = torch.cuda.Event(enable_timing=True)
     t1 = torch.cuda.Event(enable_timing=True)
-    p_ms, p_iters, p_solves, mom_ms, mom_iters, status = 0.0, 0, 0, 0.0, 0, 0
+    p_ms, p_iters, p_solves, mom_ms, mom_iters, status, fallbacks, res_max = 0.0, 0, 0, 0.0, 0, 0, 0, 0.0
     conts = []
+    l0 = _lib.lib().caffe_launch_count()
     t0.record(stream)
     for _ in range(args.steps):
         conts.append(dev.solve())
         st = dev.last_stats
+        record("timed")
         p_ms += st["p_ms"]; p_iters += st["p_iters_total"]; p_solves += st["p_solves"]
         mom_ms += st["mom_ms"]; mom_iters += sum(st["mom_iters"]); status = max(status, st["status"])
+        fallbacks += st["fallbacks"]; res_max = max(res_max, st["p_res_max"])
     t1.record(stream)
     t1.synchronize()
+    launches = _lib.lib().caffe_launch_count() - l0
     clocks = sampler.stop()
     elapsed_ms = t0.elapsed_time(t1)
     elapsed_ms = max_over_ranks(pg, elapsed_ms)
     ms_per_step = elapsed_ms / args.steps
     value = world * args.steps / (elapsed_ms / 1e3)
 
-    # roofline of the dominant kernel: the pressure-correction Krylov solve
+    # roofline of the dominant kernel group: the pressure-correction Krylov iterations
     hbm, peak_kind = peaks()
-    per_row = PCG_BYTES_PER_ROW if spec.p_method == "cg_jacobi" else BICGSTAB_BYTES_PER_ROW
-    rows = N - (dev.last_stats.get("n_ghost", 0) * 0)
-    bytes_p = per_row * rows * p_iters
-    achieved = bytes_p / (p_ms / 1e3) / 1e9 if p_ms > 0 else None
-    roofline = {"bound": "hbm", "kernel": "cg_kernel (pressure-correction Jacobi-PCG, persistent)"
-                if spec.p_method == "cg_jacobi" else "bicgstab_kernel (pressure correction)",
-                "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": (achieved / hbm) if achieved else None,
+    learned = args.p_form.startswith("learned")
+    method = inner_method(spec, args) if learned else ("pcg" if spec.p_method == "cg_jacobi" else "bicgstab64")
+    if learned:
+        per_row = LEARNED_BYTES.get(method)
+        kname = {"bicgstab": "learned inner flexible BiCGStab iteration (FP32, level pyramid)",
+                 "fcg": "learned inner flexible CG iteration (FP32, level pyramid)"}.get(method, "learned inner FGMRES iteration")
+    else:
+        per_row = PCG_BYTES_PER_ROW if method == "pcg" else BICGSTAB_BYTES_PER_ROW
+        kname = "cg1_kernel (persistent Jacobi-PCG, FP64)" if method == "pcg" else "bicgstab_kernel (persistent Jacobi-BiCGStab, FP64)"
+    achieved = per_row * N * p_iters / (p_ms / 1e3) / 1e9 if (p_ms > 0 and per_row) else None
+    roofline = {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                "frac": (achieved / hbm) if achieved else None,
                 "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
                 "traffic": None, "bytes_per_row_iteration": per_row,
-                "launch_ms_avg": p_ms / max(p_solves, 1), "iterations_per_launch": p_iters / max(p_solves, 1)}
+                "p_solve_ms_per_step": p_ms / args.steps, "iterations_per_step": p_iters / args.steps}
 
     # end to end through the C ABI with host buffers: per step, upload the solver state
     # (u, p, face mass fluxes) from pinned memory, solve, read u and p back
@@ -262,7 +340,7 @@ def run_b200(args, world, rank, local, pg):
         dev.synchronize()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
-        ke = args.steps
+        ke = max(1, args.e2e_steps)
         e0.record(stream)
         for _ in range(ke):
             for nm in up:
@@ -273,44 +351,78 @@ def run_b200(args, world, rank, local, pg):
         e1.record(stream)
         e1.synchronize()
         e_ms = max_over_ranks(pg, e0.elapsed_time(e1))
-        e2e = {"value": world * ke / (e_ms / 1e3), "unit": "time-steps/s",
+        e2e = {"value": world * ke / (e_ms / 1e3), "unit": "time-steps/s", "steps": ke,
                "h2d_bytes_per_step": 8 * sum(sizes[nm] for nm in up),
                "d2h_bytes_per_step": 8 * sum(sizes[nm] for nm in down) + 128,
                "api": "caffe_dev_array (pinned host buffers) + caffe_dev_solve, per step"}
+    dev.close()
+
+    # the same steps from rest with the plain FP64 pressure-correction solve
+    compare = None
+    if args.compare_fp64 > 0 and learned and rank == 0:
+        ref = make_solver(nodes, spec.replace(p_form="fp64"), device=local)
+        rows = []
+        for k in range(args.compare_fp64):
+            ref.solve()
+            st = ref.last_stats
+            rows.append({"step": k + 1, "p_ms": round(st["p_ms"], 2), "p_iters": st["p_iters_total"], "step_ms": round(st["step_ms"], 2),
+                         "p_res_max": st["p_res_max"]})
+        ref.close()
+        same = per_step[:args.compare_fp64]
+        pf = sum(r["p_ms"] for r in rows) / len(rows)
+        pl = sum(r["p_ms"] for r in same) / len(same)
+        itf = sum(r["p_iters"] for r in rows) / len(rows)
+        itl = sum(r["p_iters"] for r in same) / len(same)
+        sf = sum(r["step_ms"] for r in rows) / len(rows)
+        sl = sum(r["step_ms"] for r in same) / len(same)
+        compare = {"plain_fp64_steps_from_rest": rows, "learned_same_steps": same,
+                   "p_solve_ms_ratio_fp64_over_learned": pf / pl if pl > 0 else None,
+                   "krylov_iterations_ratio_fp64_over_learned": itf / itl if itl > 0 else None,
+                   "time_steps_per_s_ratio_learned_over_fp64": sf / sl if sl > 0 else None}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(nodes, spec.replace(p_form="fp64"), steps=1)
+        cpu = scaled_cpu(args, 1, 60.0)
+        cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
 
-    launches_per_step = 3 + 2 + (6 * spec.n_pcorr if spec.kind != "simple" else 6) + 3
     if rank == 0:
         working_set = N * 8 * 60
         line = {
             "metric": "time-steps/s at 1e-8 true relative residual", "value": value, "unit": "time-steps/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64 fields and outer solve; f32 inner Krylov; bf16 network" if learned else "f64",
             "data": "synthetic (seeded mesh and case, no dataset)",
-            "config": {"workload": label, "cells": N, "p_form": args.p_form, "parallelism": f"replicas x{world}",
+            "config": {"workload": label, "cells": N, "p_form": args.p_form,
+                       "precond": args.precond if learned else None, "inner": method,
+                       "parallelism": f"replicas x{world}",
                        "l2": f"inputs larger than L2: working set ~{working_set / 2**30:.1f} GiB > 126 MB"},
             "p_solve_ms": p_ms / args.steps, "momentum_solve_ms": mom_ms / args.steps,
             "p_iters_per_step": p_iters / args.steps, "mom_iters_per_step": mom_iters / args.steps,
+            "p_res_max": res_max, "fallbacks": fallbacks,
             "continuity_last": conts[-1], "solver_status": status,
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
-            "gpu_launches": launches_per_step * args.steps,
+            "gpu_launches": launches, "compare": compare, "per_step": per_step,
         }
         print(json.dumps(line), flush=True)
-    dev.close()
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
-    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=("b200", "reference"))
-    ap.add_argument("--workload", default="c2", choices=("c1", "c2", "c3", "c5"))
-    ap.add_argument("--p-form", default="fp64", choices=tuple(C.P_FORMS))
+    ap.add_argument("--workload", default="c5", choices=("c1", "c2", "c3", "c5"))
+    ap.add_argument("--p-form", default="learned_mixed", choices=tuple(C.P_FORMS))
+    ap.add_argument("--precond", default="levels", choices=("levels", "network", "jacobi"))
+    ap.add_argument("--inner", default="auto", choices=("auto", "fcg", "bicgstab", "fgmres"))
+    ap.add_argument("--net-from", type=int, default=1)
+    ap.add_argument("--restart", type=int, default=30)
+    ap.add_argument("--params", default=None, help="network parameters (.npy); default: the shipped ones")
     ap.add_argument("--size", type=int, default=None)
+    ap.add_argument("--compare-fp64", type=int, default=1, help="plain FP64 steps from rest to compare with")
+    ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()

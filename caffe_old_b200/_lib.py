@@ -67,8 +67,8 @@ EXPORTS = (
     "caffe_ksp7_solve", "caffe_ksp7_solve_device", "caffe_ksp7_solve_device_noalloc",
     "caffe_precond_param_count", "caffe_precond_net_apply", "caffe_precond_net_grad",
     "caffe_dev_set_precond", "caffe_dev_get_precond", "caffe_dev_set_precond_mode", "caffe_dev_set_precond_options",
-    "caffe_dev_record_pairs", "caffe_dev_pair_count", "caffe_dev_add_pairs", "caffe_dev_copy_pairs", "caffe_dev_train_precond",
-    "caffe_dev_eval_precond",
+    "caffe_dev_record_pairs", "caffe_dev_pair_count", "caffe_dev_add_pairs", "caffe_dev_add_random_pairs", "caffe_dev_copy_pairs", "caffe_dev_train_precond",
+    "caffe_dev_eval_precond", "caffe_launch_count",
 )
 
 
@@ -107,8 +107,11 @@ def lib():
     L.caffe_dev_pair_count.argtypes = [vp]
     L.caffe_dev_add_pairs.argtypes = [vp, vp, vp, ci]
     L.caffe_dev_copy_pairs.argtypes = [vp, vp]
+    L.caffe_dev_add_random_pairs.argtypes = [vp, ci, ctypes.c_uint]
     L.caffe_dev_train_precond.argtypes = [vp, ci, ci, ctypes.c_float, ctypes.c_uint, vp, vp]
     L.caffe_dev_eval_precond.argtypes = [vp, ci, vp]
+    L.caffe_launch_count.restype = ctypes.c_longlong
+    L.caffe_launch_count.argtypes = []
     _lib = L
     return L
 

@@ -912,6 +912,19 @@ int caffe_dev_add_pairs(caffe_dev* h, const float* b_pairs, const float* x_pairs
     return 0;
 }
 
+int caffe_dev_add_random_pairs(caffe_dev* h, int n_pairs, unsigned seed) {
+    g_err.clear();
+    if (!h || n_pairs < 0) { set_error("invalid arguments"); return 1; }
+    CB_CUDA(cudaSetDevice(h->device));
+    if (h->ensure_learned() || h->ensure_pairs(h->pairCount + n_pairs)) return 1;
+    size_t off = (size_t)h->pairCount * h->L.PS;
+    if (learned_random_pairs(h->lw, h->pOp(), h->ib ? h->status : nullptr, h->L, n_pairs, seed, h->pairB + off, h->pairX + off, h->st))
+        return 1;
+    CB_CUDA(cudaStreamSynchronize(h->st));
+    h->pairCount += n_pairs;
+    return 0;
+}
+
 int caffe_dev_copy_pairs(caffe_dev* dst, caffe_dev* src) {
     g_err.clear();
     if (!dst || !src) { set_error("handle is NULL"); return 1; }

@@ -1170,6 +1170,63 @@ int learned_snapshot_pair(const OpSym& A, const Lat& L, const double* b, const d
     return 0;
 }
 
+// ---------------------------------------------------------------- random multi-scale pairs
+namespace {
+
+// uniform in [-1, 1) from a 64-bit integer hash (splitmix64 finaliser) of (seed, pair, cell)
+__device__ __forceinline__ float hash_uniform(unsigned seed, unsigned q, unsigned long long c) {
+    unsigned long long x = c + 0x9E3779B97F4A7C15ull * (((unsigned long long)seed << 32) ^ (unsigned long long)(q + 1));
+    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+    x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+    x = x ^ (x >> 31);
+    return (float)((double)(x >> 11) * (1.0 / 9007199254740992.0)) * 2.f - 1.f;
+}
+__global__ void rand_fill_kernel(long long n, unsigned seed, unsigned q, float* out) {
+    long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (c < n) out[c] = hash_uniform(seed, q, (unsigned long long)c);
+}
+// out = P wc on the finer level fd (mask: zero on non-active cells of the cell lattice)
+__global__ void prolong_only_kernel(Dims3 fd, Dims3 cd, const float* wc, const uint8_t* st, float* out) {
+    long long Nf = (long long)fd.n0 * fd.n1 * fd.n2;
+    long long f = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (f >= Nf) return;
+    out[f] = (st && st[f] != ST_ACTIVE) ? 0.f : prolong_at(fd, cd, wc, f);
+}
+__global__ void mask_active_kernel(long long N, const uint8_t* st, float* x) {
+    long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (c < N && st && st[c] != ST_ACTIVE) x[c] = 0.f;
+}
+__global__ void __launch_bounds__(LB) apply_f32_kernel(OpSymF32 A, long long N, const float* x, float* y) {
+    for (long long c = blockIdx.x * (long long)LB + threadIdx.x; c < N; c += (long long)gridDim.x * LB)
+        y[c] = applyF(A, c, [&](long long e_) { return x[e_]; });
+}
+
+}  // namespace
+
+int learned_random_pairs(LearnedWork& lw, const OpSym& A, const uint8_t* status, const Lat& L, int nPairs, unsigned seed, float* pairsB,
+                         float* pairsX, cudaStream_t st) {
+    OpSymF32 Af = cast_operator(lw, A, L, st);
+    const long long N = L.N;
+    for (int q = 0; q < nPairs; ++q) {
+        float* b = pairsB + (size_t)q * L.PS + L.H;
+        float* e = pairsX + (size_t)q * L.PS + L.H;
+        const int l = lw.nLev > 1 ? q % lw.nLev : 0;
+        if (l == 0) {
+            rand_fill_kernel<<<grid_for(N, 256), 256, 0, st>>>(N, seed, (unsigned)q, e);
+            mask_active_kernel<<<grid_for(N, 256), 256, 0, st>>>(N, status, e);
+        } else {
+            rand_fill_kernel<<<grid_for(lw.lev[l].N, 256), 256, 0, st>>>(lw.lev[l].N, seed, (unsigned)q, lw.lev[l].w);
+            for (int k = l - 1; k >= 1; --k)
+                prolong_only_kernel<<<grid_for(lw.lev[k].N, 256), 256, 0, st>>>(dims_of(lw.lev[k]), dims_of(lw.lev[k + 1]), lw.lev[k + 1].w,
+                                                                               nullptr, lw.lev[k].w);
+            prolong_only_kernel<<<grid_for(N, 256), 256, 0, st>>>(dims_of(lw.lev[0]), dims_of(lw.lev[1]), lw.lev[1].w, status, e);
+        }
+        apply_f32_kernel<<<nblocks(N), LB, 0, st>>>(Af, N, e, b);
+        CB_CHECK_LAUNCH();
+    }
+    return 0;
+}
+
 // ---------------------------------------------------------------- training
 namespace {
 

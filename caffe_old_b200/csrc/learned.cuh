@@ -87,6 +87,11 @@ int learned_train(LearnedWork& lw, const OpSym& A, const uint8_t* status, const 
 // Training pair of an intermediate iterate xk of a solve with solution xstar: (b - A xk, xstar - xk) in FP32.
 int learned_snapshot_pair(const OpSym& A, const Lat& L, const double* b, const double* xstar, const double* xk, float* pb, float* px,
                           cudaStream_t st);
+// n synthetic pairs (A e, e): e = seeded uniform noise on pyramid level q mod levels,
+// prolonged to the cell lattice (zero off the active cells): smooth at every scale the
+// pyramid spans.  Written to FP32 halo-padded planes [n][PS].
+int learned_random_pairs(LearnedWork& lw, const OpSym& A, const uint8_t* status, const Lat& L, int nPairs, unsigned seed, float* pairsB,
+                         float* pairsX, cudaStream_t st);
 // Energy-norm loss of one application M(b) against x* for each of n pairs (mode as above).
 int learned_eval(LearnedWork& lw, const OpSym& A, const uint8_t* status, const Lat& L, const float* pairsB, const float* pairsX,
                  int nPairs, int mode, float* lossHost, cudaStream_t st);

@@ -125,6 +125,11 @@ def add_pairs(solver, b: np.ndarray, x: np.ndarray) -> None:
            "add_pairs")
 
 
+def add_random_pairs(solver, n: int, seed: int = 0) -> None:
+    """Append n synthetic multi-scale pairs (A e, e) built with the solver's current p' matrix."""
+    _check(lib().caffe_dev_add_random_pairs(solver._h, int(n), int(seed) & 0xFFFFFFFF), "add_random_pairs")
+
+
 def copy_pairs(dst, src) -> None:
     _check(lib().caffe_dev_copy_pairs(dst._h, src._h), "copy_pairs")
 
@@ -148,4 +153,4 @@ def evaluate(solver, mode: str = "network") -> np.ndarray:
 
 
 __all__ = ["PARAMS", "MODES", "INNER", "identity_params", "load_default", "set_params", "get_params", "set_mode", "set_options",
-           "record_pairs", "pair_count", "add_pairs", "copy_pairs", "train", "evaluate", "weight_view"]
+           "record_pairs", "pair_count", "add_pairs", "add_random_pairs", "copy_pairs", "train", "evaluate", "weight_view"]

@@ -174,6 +174,11 @@ int caffe_dev_record_pairs(caffe_dev* h, int capacity, int snapshots);
 int caffe_dev_pair_count(caffe_dev* h);
 int caffe_dev_add_pairs(caffe_dev* h, const float* b_pairs, const float* x_pairs, int n_pairs);
 int caffe_dev_copy_pairs(caffe_dev* dst, caffe_dev* src);
+/* Append n_pairs synthetic pairs (A e, e) built with the handle's current p' operator: e is
+ * seeded noise on pyramid level (pair mod levels), prolonged to the cell lattice, so the
+ * pairs cover every scale the pyramid spans (inputs like the Krylov vectors the network
+ * meets inside a solve, not only right-hand sides). */
+int caffe_dev_add_random_pairs(caffe_dev* h, int n_pairs, unsigned seed);
 /* Train on the handle's pairs with its current p' operator, on the device: loss per pair
  * ||M(b) - x||^2_E / ||x||^2_E in the energy norm of the (negated, positive) p' matrix, on its
  * active-cell block with an immersed body; Adam with learning rate lr, `steps` updates of
@@ -183,6 +188,9 @@ int caffe_dev_copy_pairs(caffe_dev* dst, caffe_dev* src);
 int caffe_dev_train_precond(caffe_dev* h, int steps, int batch, float lr, unsigned seed, float* params_inout, float* loss_hist);
 /* Loss of one application M(b) for every stored pair, in the given mode: loss[pair_count]. */
 int caffe_dev_eval_precond(caffe_dev* h, int mode, float* loss);
+
+/* Number of kernel launches this library has issued in this process (all handles). */
+long long caffe_launch_count(void);
 
 /* caffe_ksp7_solve_device without any device allocation.  It has no counterpart in the
  * reference.  For callers that cannot call cudaMalloc/cudaFree from inside a solve -- a program
