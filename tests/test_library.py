@@ -20,7 +20,7 @@ def built():
 def header_functions():
     src = open(_lib.HEADER_PATH).read()
     src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
-    return sorted(set(re.findall(r"^\s*(?:const\s+)?\w+\s*\*?\s*(caffe_\w+)\s*\(", src, flags=re.M)))
+    return sorted(set(re.findall(r"^\s*(?:const\s+)?(?:long\s+)?\w+\s*\*?\s*(caffe_\w+)\s*\(", src, flags=re.M)))
 
 
 def test_header_lists_entry_points():
