@@ -418,7 +418,7 @@ def main():
     ap.add_argument("--precond", default="levels", choices=("levels", "network", "jacobi"))
     ap.add_argument("--inner", default="auto", choices=("auto", "fcg", "bicgstab", "fgmres"))
     ap.add_argument("--net-from", type=int, default=1)
-    ap.add_argument("--restart", type=int, default=30)
+    ap.add_argument("--restart", type=int, default=40)
     ap.add_argument("--params", default=None, help="network parameters (.npy); default: the shipped ones")
     ap.add_argument("--size", type=int, default=None)
     ap.add_argument("--compare-fp64", type=int, default=1, help="plain FP64 steps from rest to compare with")

@@ -710,6 +710,7 @@ constexpr int FG_DOT_BLOCKS = 592;    // 4 x 148 SMs: cell chunks of the multi-d
 
 struct FgScal {
     double H[(FGM + 1) * FGM];   // column-major: H[j * (FGM + 1) + i]
+    double h1[FGM + 1], h2[FGM + 1];   // the two Gram-Schmidt passes of the current column
     double cs[FGM], sn[FGM], g[FGM + 1], y[FGM];
     double beta;
     int jEnd;
@@ -764,8 +765,8 @@ __global__ void __launch_bounds__(LB) fg_dots_kernel(long long N, const float* w
         part[(size_t)i * gridDim.y + blockIdx.y] = t;
     }
 }
-// H[0..j][j] from the partials (block q sums entry q)
-__global__ void fg_dots_finish(const double* part, int nchunk, int j, FgScal* F, const Scal* S) {
+// h[0..j] from the partials (block q sums entry q)
+__global__ void fg_dots_finish(const double* part, int nchunk, double* h, const Scal* S) {
     if (S->done) return;
     const int i = blockIdx.x;
     __shared__ double sm[LB];
@@ -777,14 +778,14 @@ __global__ void fg_dots_finish(const double* part, int nchunk, int j, FgScal* F,
         if ((int)threadIdx.x < s) sm[threadIdx.x] += sm[threadIdx.x + s];
         __syncthreads();
     }
-    if (threadIdx.x == 0) F->H[(size_t)j * (FGM + 1) + i] = sm[0];
+    if (threadIdx.x == 0) h[i] = sm[0];
 }
-// w -= sum_i H[i][j] v_i; partial ||w||^2
-__global__ void __launch_bounds__(LB) fg_orth_kernel(long long N, float* w, const float* V, long long PS, int j, const FgScal* F, double* part,
+// w -= sum_i h[i] v_i; partial ||w||^2
+__global__ void __launch_bounds__(LB) fg_orth_kernel(long long N, float* w, const float* V, long long PS, int j, const double* hc, double* part,
                                                      const Scal* S) {
     if (S->done) return;
     __shared__ float h[FGM + 1];
-    for (int i = threadIdx.x; i <= j; i += blockDim.x) h[i] = (float)F->H[(size_t)j * (FGM + 1) + i];
+    for (int i = threadIdx.x; i <= j; i += blockDim.x) h[i] = (float)hc[i];
     __syncthreads();
     double a[1] = {0.};
     for (long long c = blockIdx.x * (long long)LB + threadIdx.x; c < N; c += (long long)gridDim.x * LB) {
@@ -802,6 +803,7 @@ __global__ void fg_step_finish(const double* part, int nblk, int j, int m, int m
     totals(part, nblk, 1, t);
     if (threadIdx.x != 0) return;
     double* Hc = F->H + (size_t)j * (FGM + 1);
+    for (int i = 0; i <= j; ++i) Hc[i] = F->h1[i] + F->h2[i];   // classical Gram-Schmidt, two passes
     double hn = sqrt(t[0]);
     Hc[j + 1] = hn;
     for (int i = 0; i < j; ++i) {
@@ -1057,9 +1059,14 @@ int learned_solve(LearnedWork& lw, const OpSym& A, const uint8_t* status, const 
                 if (apply_levels(lw, vj, status, mode, S, st)) return 1;
                 bs_z_kernel<<<nb, LB, 0, st>>>(N, fd, cd, vj, lw.invD, status, w1, zj, S);
                 fg_spmv_kernel<<<nb, LB, 0, st>>>(Af, N, zj, lw.t, S);
-                fg_dots_kernel<<<dim3(j + 1, FG_DOT_BLOCKS), LB, 0, st>>>(N, lw.t, lw.fgV + L.H, PS, lw.fgPart, S);
-                fg_dots_finish<<<j + 1, LB, 0, st>>>(lw.fgPart, FG_DOT_BLOCKS, j, F, S);
-                fg_orth_kernel<<<nb, LB, 0, st>>>(N, lw.t, lw.fgV + L.H, PS, j, F, lw.part, S);
+                // classical Gram-Schmidt with one re-orthogonalisation (CGS2): FP32 vectors lose
+                // orthogonality in a single pass once the preconditioner is strong
+                for (int pass = 0; pass < 2; ++pass) {
+                    double* hc = pass == 0 ? F->h1 : F->h2;
+                    fg_dots_kernel<<<dim3(j + 1, FG_DOT_BLOCKS), LB, 0, st>>>(N, lw.t, lw.fgV + L.H, PS, lw.fgPart, S);
+                    fg_dots_finish<<<j + 1, LB, 0, st>>>(lw.fgPart, FG_DOT_BLOCKS, hc, S);
+                    fg_orth_kernel<<<nb, LB, 0, st>>>(N, lw.t, lw.fgV + L.H, PS, j, hc, lw.part, S);
+                }
                 fg_step_finish<<<1, LB, 0, st>>>(lw.part, nb, j, m, maxit, F, S);
                 fg_scale_kernel<<<G, 256, 0, st>>>(N, lw.t, lw.fgV + (j + 1) * PS + L.H, S);
                 if ((j & 7) == 7 || j == m - 1) {

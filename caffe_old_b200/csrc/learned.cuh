@@ -59,7 +59,7 @@ struct LearnedWork {
     bool haveParams = false;
     int netFrom = 1;             // first level that runs the network (finer levels: identity)
     int inner = LEARN_INNER_AUTO;
-    int restart = 30;            // FGMRES cycle length (one cycle per FP64 refinement pass)
+    int restart = 40;            // FGMRES cycle length (one cycle per FP64 refinement pass)
     // FGMRES basis (restart + 1 planes) and preconditioned vectors (restart planes), one
     // allocation each, planes PS apart; scalar record and dot partials
     float* fgV = nullptr;

@@ -96,7 +96,7 @@ def set_mode(solver, mode: str) -> None:
     _check(lib().caffe_dev_set_precond_mode(solver._h, MODES[mode]), "set_precond_mode")
 
 
-def set_options(solver, inner: str = "auto", net_from_level: int = 1, restart: int = 30) -> None:
+def set_options(solver, inner: str = "auto", net_from_level: int = 1, restart: int = 40) -> None:
     """Inner Krylov method of the learned solve, the first pyramid level that runs the
     network (finer levels use the identity) and the FGMRES cycle length."""
     _check(lib().caffe_dev_set_precond_options(solver._h, INNER[inner], int(net_from_level), int(restart)),
