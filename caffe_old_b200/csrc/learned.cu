@@ -35,6 +35,7 @@
 // of its active-cell block), gradient dL/dz = 2 (-A)(z - x*) / ||x*||^2_E, carried through the
 // prolongations (adjoint: P^T) to every level's network output and back-propagated by the
 // tensor-core backward pass; Adam update.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -227,7 +228,7 @@ constexpr int RFI = 2 * RCI + 2, RFJ = 2 * RCJ + 2, RFK = 2 * RCK + 2;
 
 __global__ void __launch_bounds__(256) restrict_kernel(Dims3 fd, Dims3 cd, const float* fin, const float* invD, const uint8_t* st,
                                                        float scale, float* out, float* out2, float mul2, __nv_bfloat16* act0,
-                                                       const float* maskc, float chan, const Scal* S) {
+                                                       __nv_bfloat16* act0n, const float* maskc, float chan, const Scal* S) {
     if (S && S->done) return;
     __shared__ float s0[RFK][RFJ][RFI];
     __shared__ float t1[RFK][RFJ][RCI];
@@ -287,6 +288,12 @@ __global__ void __launch_bounds__(256) restrict_kernel(Dims3 fd, Dims3 cd, const
             uint4* dst = reinterpret_cast<uint4*>(act0 + (size_t)c * 16);
             dst[0] = reinterpret_cast<uint4*>(v)[0];
             dst[1] = reinterpret_cast<uint4*>(v)[1];
+            if (act0n) {
+                v[0] = __float2bfloat16_rn(-acc * (float)(1. / S->s));
+                uint4* dn = reinterpret_cast<uint4*>(act0n + (size_t)c * 16);
+                dn[0] = reinterpret_cast<uint4*>(v)[0];
+                dn[1] = reinterpret_cast<uint4*>(v)[1];
+            }
         }
     }
 }
@@ -316,15 +323,17 @@ __device__ __forceinline__ float prolong_at(const Dims3& fd, const Dims3& cd, co
     return 0.75f * k0 + 0.25f * k1;
 }
 
-// w_l = gain * (ydiv ? y : s y) + P w_{l+1}   (wc null on the coarsest level)
-__global__ void __launch_bounds__(256) prolong_kernel(Dims3 fd, Dims3 cd, const float* wc, const float* y, int ydiv, float gain,
-                                                      float* out, const Scal* S) {
+// w_l = gain * (ydiv ? y : s y) + P w_{l+1}   (wc null on the coarsest level); with yn, the
+// network term is odd: y <- (y - yn) / 2 (yn = the network applied to the negated input)
+__global__ void __launch_bounds__(256) prolong_kernel(Dims3 fd, Dims3 cd, const float* wc, const float* y, const float* yn, int ydiv,
+                                                      float gain, float* out, const Scal* S) {
     if (S->done) return;
     long long Nf = (long long)fd.n0 * fd.n1 * fd.n2;
     long long f = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (f >= Nf) return;
     float sy = ydiv ? 1.f : (float)S->s;
-    float v = gain * sy * y[f];
+    float yv = yn ? 0.5f * (y[f] - yn[f]) : y[f];
+    float v = gain * sy * yv;
     if (wc) v += prolong_at(fd, cd, wc, f);
     out[f] = v;
 }
@@ -869,17 +878,18 @@ int apply_levels(LearnedWork& lw, const float* rfine, const uint8_t* status, int
         const Level& f = lw.lev[l - 1];
         restrict_kernel<<<restrict_grid(dims_of(c)), 256, 0, st>>>(dims_of(f), dims_of(c), l == 1 ? rfine : f.u, l == 1 ? lw.invD : nullptr,
                                                                    l == 1 ? status : nullptr, c.rscale, c.u, nullptr, 0.f,
-                                                                   netAt(l) ? c.net.act[0] : nullptr, c.mask, c.chan, S);
+                                                                   netAt(l) ? c.net.act[0] : nullptr, netAt(l) ? c.netNeg.act[0] : nullptr,
+                                                                   c.mask, c.chan, S);
     }
     CB_CHECK_LAUNCH();
     for (int l = 1; l < lw.nLev; ++l)
-        if (netAt(l) && net_forward_if(lw.lev[l].net, &S->done, st)) return 1;
+        if (netAt(l) && (net_forward_if(lw.lev[l].net, &S->done, st) || net_forward_if(lw.lev[l].netNeg, &S->done, st))) return 1;
     for (int l = lw.nLev - 1; l >= 1; --l) {
         Level& f = lw.lev[l];
         const bool top = l + 1 >= lw.nLev;
         prolong_kernel<<<grid_for(f.N, 256), 256, 0, st>>>(dims_of(f), top ? dims_of(f) : dims_of(lw.lev[l + 1]),
-                                                           top ? nullptr : lw.lev[l + 1].w, netAt(l) ? f.net.y : f.u, netAt(l) ? 0 : 1,
-                                                           f.gain, f.w, S);
+                                                           top ? nullptr : lw.lev[l + 1].w, netAt(l) ? f.net.y : f.u,
+                                                           netAt(l) ? f.netNeg.y : nullptr, netAt(l) ? 0 : 1, f.gain, f.w, S);
     }
     CB_CHECK_LAUNCH();
     return 0;
@@ -895,7 +905,7 @@ int level_masks(LearnedWork& lw, const uint8_t* status, cudaStream_t st) {
         const Level& f = lw.lev[l - 1];
         restrict_kernel<<<restrict_grid(dims_of(c)), 256, 0, st>>>(dims_of(f), dims_of(c), l == 1 ? nullptr : f.mask, nullptr,
                                                                    l == 1 ? status : nullptr, c.rscale, c.mask, nullptr, 0.f, nullptr,
-                                                                   nullptr, 0.f, nullptr);
+                                                                   nullptr, nullptr, 0.f, nullptr);
     }
     CB_CHECK_LAUNCH();
     lw.masksReady = true;
@@ -954,7 +964,9 @@ int learned_alloc(LearnedWork& lw, const Lat& L, void* (*alloc)(size_t, void*), 
         if (!c.u || !c.w || !c.mask) { set_error("learned-solver allocation failed"); return 1; }
         Lat Lc = make_lat(c.n[0], c.n[1], c.n[2]);
         int rc = lw.nLev == 1 ? net_alloc(c.net, Lc, alloc, ctx) : net_alloc_shared(c.net, Lc, lw.lev[1].net, alloc, ctx);
-        if (rc) return 1;
+        if (rc || net_alloc_shared(c.netNeg, Lc, lw.lev[1].net, alloc, ctx)) return 1;
+        c.w2 = static_cast<float*>(alloc(sizeof(float) * (size_t)c.N, ctx));
+        if (!c.w2) { set_error("learned-solver allocation failed"); return 1; }
         ++lw.nLev;
     }
     lw.weights = lw.nLev >= 2 ? &lw.lev[1].net : nullptr;
@@ -1018,7 +1030,8 @@ int learned_solve(LearnedWork& lw, const OpSym& A, const uint8_t* status, const 
         count_active_kernel<<<nb, LB, 0, st>>>(N, status, lw.part);
         count_finish<<<1, LB, 0, st>>>(lw.part, nb, lw.mean + 1);
     }
-    const int max_outer = 12;
+    // FGMRES: one restart cycle per refinement pass, as many cycles as the iteration budget allows
+    const int max_outer = fgmres ? std::max(12, maxit / m + 1) : 12;
     const int chunk = 8;
     for (int outer = 0; outer <= max_outer; ++outer) {
         outer_residual_kernel<<<nb, LB, 0, st>>>(A, N, b, x, lw.r, lw.part, S);
@@ -1241,6 +1254,11 @@ struct TrainScal {
     double s, coef, loss, loss_sum;
 };
 
+__global__ void half_split_kernel(long long n, float* a, float* b) {
+    long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (c < n) { float v = 0.5f * a[c]; a[c] = v; b[c] = -v; }
+}
+
 __global__ void __launch_bounds__(LB) train_scale_kernel(long long N, const float* b, const float* invD, const uint8_t* st, double* part) {
     double v[2] = {0., 0.};
     for (long long c = blockIdx.x * (long long)LB + threadIdx.x; c < N; c += (long long)gridDim.x * LB) {
@@ -1414,8 +1432,12 @@ int learned_train(LearnedWork& lw, const OpSym& A, const uint8_t* status, const 
                 Level& c = lw.lev[l];
                 const Level& f = lw.lev[l - 1];
                 restrict_kernel<<<restrict_grid(dims_of(c)), 256, 0, st>>>(dims_of(f), dims_of(c), l == 1 ? lw.r : f.u, nullptr, nullptr, 1.f,
-                                                                           c.u, c.w, c.gain, nullptr, nullptr, 0.f, S);
-                if (l >= lw.netFrom && net_backward(c.net, c.w, st)) return 1;
+                                                                           c.u, c.w, c.gain, nullptr, nullptr, nullptr, 0.f, S);
+                if (l >= lw.netFrom) {
+                    // y = (net(x) - net(-x)) / 2: the two evaluations get dL/dy / 2 and -dL/dy / 2
+                    half_split_kernel<<<grid_for(c.N, 256), 256, 0, st>>>(c.N, c.w, c.w2);
+                    if (net_backward(c.net, c.w, st) || net_backward(c.netNeg, c.w2, st)) return 1;
+                }
             }
         }
         loss_out_kernel<<<1, 32, 0, st>>>(T, hist, step, inv_batch);

@@ -27,7 +27,9 @@ struct Level {
     float* u = nullptr;  // restricted Jacobi-scaled residual (training: adjoint of w)
     float* w = nullptr;  // prolongation accumulator (training: dL/dy)
     float* mask = nullptr;   // fraction of active cells
-    NetBuffers net;      // activations of this level; weights shared with level 1
+    NetBuffers net;      // activations of this level for the input x; weights shared with level 1
+    NetBuffers netNeg;   // activations for the input -x (the network term is odd: (net(x) - net(-x)) / 2)
+    float* w2 = nullptr; // training: dL/dy of the -x evaluation
 };
 
 enum { NET_MODE_JACOBI = 0, NET_MODE_NETWORK = 1, NET_MODE_LEVELS = 2 };

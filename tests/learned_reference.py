@@ -2,7 +2,8 @@
 the checker of the device kernels: cell-centred trilinear prolongation P, restriction
 R = P^T scaled to a cell average, and the preconditioner
     M(r) = D^-1 r + P_1 w_1,   w_l = gain_l s y_l + P_(l+1) w_(l+1)
-with y_l = u_l / s (the LEVELS form) or the network of cnn_reference (the NETWORK form).
+with y_l = u_l / s (the LEVELS form) or the odd network term (net(x) - net(-x)) / 2 of
+cnn_reference (the NETWORK form).
 Arrays are indexed [k, j, i]."""
 from __future__ import annotations
 
@@ -58,8 +59,9 @@ def rscale(fine) -> float:
     return 1.0 / 2 ** sum(1 for n in fine if n > 1)
 
 
-def apply_M(r: np.ndarray, invD: np.ndarray, active: np.ndarray, mode: str = "levels", params=None):
-    """M(r) on a [k, j, i] lattice; active: boolean mask (all True without an immersed body)."""
+def apply_M(r: np.ndarray, invD: np.ndarray, active: np.ndarray, mode: str = "levels", params=None, bf: bool = False):
+    """M(r) on a [k, j, i] lattice; active: boolean mask (all True without an immersed body);
+    bf: round the network's input, weights and activations to bfloat16 as the device does."""
     dims = r.shape
     levels = pyramid(dims)
     u0 = np.where(active, invD * r, 0.0)
@@ -82,10 +84,13 @@ def apply_M(r: np.ndarray, invD: np.ndarray, active: np.ndarray, mode: str = "le
         if mode == "levels":
             y = us[l] / s
         else:
-            x2 = np.stack([us[l].ravel() / s, masks[l].ravel()], axis=1)
-            y, _ = R.forward(params.astype(np.float64), x2, (levels[l][2], levels[l][1], levels[l][0]), bf=False,
-                             extra_const=l / 8.0)
-            y = y.reshape(us[l].shape)
+            # the network term is odd: (net(x) - net(-x)) / 2
+            shape = (levels[l][2], levels[l][1], levels[l][0])
+            xp = np.stack([us[l].ravel() / s, masks[l].ravel()], axis=1)
+            xn = np.stack([-us[l].ravel() / s, masks[l].ravel()], axis=1)
+            yp, _ = R.forward(params.astype(np.float64), xp, shape, bf=bf, extra_const=l / 8.0)
+            yn, _ = R.forward(params.astype(np.float64), xn, shape, bf=bf, extra_const=l / 8.0)
+            y = (0.5 * (yp - yn)).reshape(us[l].shape)
         v = gain * s * y
         if w is not None:
             v = v + prolong(w, levels[l])
