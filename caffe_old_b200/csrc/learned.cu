@@ -236,18 +236,35 @@ __global__ void __launch_bounds__(256) restrict_kernel(Dims3 fd, Dims3 cd, const
     const int I0 = blockIdx.x * RCI, J0 = blockIdx.y * RCJ, K0 = blockIdx.z * RCK;
     const int fi0 = 2 * I0 - 1, fj0 = 2 * J0 - 1, fk0 = 2 * K0 - 1;
     const unsigned fsJ = (unsigned)fd.n0, fsK = (unsigned)fd.n0 * (unsigned)fd.n1;
-    for (int u = threadIdx.x; u < RFI * RFJ * RFK; u += blockDim.x) {
-        int li = u % RFI, lj = (u / RFI) % RFJ, lk = u / (RFI * RFJ);
-        int fi = fi0 + li, fj = fj0 + lj, fk = fk0 + lk;
-        float v = 0.f;
-        if (fi >= 0 && fi < fd.n0 && fj >= 0 && fj < fd.n1 && fk >= 0 && fk < fd.n2) {
-            unsigned f = (unsigned)fk * fsK + (unsigned)fj * fsJ + (unsigned)fi;
-            if (!st || st[f] == ST_ACTIVE) {
-                v = fin ? fin[f] : 1.f;
-                if (invD) v *= __ldg(invD + f);
+    // stage the fine tile: four elements per thread and round, their loads issued together
+    constexpr int TOT = RFI * RFJ * RFK;
+    for (int u0 = threadIdx.x; u0 < TOT; u0 += 4 * blockDim.x) {
+        unsigned fidx[4];
+        bool in[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            int u = u0 + q * blockDim.x;
+            int li = u % RFI, lj = (u / RFI) % RFJ, lk = u / (RFI * RFJ);
+            int fi = fi0 + li, fj = fj0 + lj, fk = fk0 + lk;
+            in[q] = u < TOT && fi >= 0 && fi < fd.n0 && fj >= 0 && fj < fd.n1 && fk >= 0 && fk < fd.n2;
+            fidx[q] = in[q] ? (unsigned)fk * fsK + (unsigned)fj * fsJ + (unsigned)fi : 0u;
+        }
+        float fv[4], dv[4];
+        uint8_t sv[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            fv[q] = (in[q] && fin) ? __ldg(fin + fidx[q]) : 1.f;
+            dv[q] = (in[q] && invD) ? __ldg(invD + fidx[q]) : 1.f;
+            sv[q] = (in[q] && st) ? __ldg(st + fidx[q]) : (uint8_t)ST_ACTIVE;
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            int u = u0 + q * blockDim.x;
+            if (u < TOT) {
+                int li = u % RFI, lj = (u / RFI) % RFJ, lk = u / (RFI * RFJ);
+                s0[lk][lj][li] = (in[q] && sv[q] == ST_ACTIVE) ? fv[q] * dv[q] : 0.f;
             }
         }
-        s0[lk][lj][li] = v;
     }
     __syncthreads();
     for (int u = threadIdx.x; u < RFK * RFJ * RCI; u += blockDim.x) {
@@ -323,6 +340,38 @@ __device__ __forceinline__ float prolong_at(const Dims3& fd, const Dims3& cd, co
     return 0.75f * k0 + 0.25f * k1;
 }
 
+// (P wc) for the 4 consecutive cells 4q..4q+3 of the fine lattice fd: the (j, k) part of the
+// index and the four coarse rows are computed once when the 4 cells share a row
+__device__ __forceinline__ void prolong4(const Dims3& fd, const Dims3& cd, const float* wc, long long q, float (&out)[4]) {
+    const unsigned f0 = (unsigned)(4 * q), n0 = (unsigned)fd.n0, n1 = (unsigned)fd.n1;
+    const unsigned t = f0 / n0;
+    const int fi = (int)(f0 - t * n0);
+    if (fi + 3 >= fd.n0) {   // the 4 cells span a row end
+#pragma unroll
+        for (int m = 0; m < 4; ++m) out[m] = prolong_at(fd, cd, wc, (long long)f0 + m);
+        return;
+    }
+    const int fk = (int)(t / n1);
+    const int fj = (int)(t - (unsigned)fk * n1);
+    const int J0 = fj >> 1, J1 = pclamp((fj & 1) ? J0 + 1 : J0 - 1, cd.n1);
+    const int K0 = fk >> 1, K1 = pclamp((fk & 1) ? K0 + 1 : K0 - 1, cd.n2);
+    const unsigned sJ = (unsigned)cd.n0, sK = (unsigned)cd.n0 * (unsigned)cd.n1;
+    const float* r00 = wc + (unsigned)K0 * sK + (unsigned)J0 * sJ;
+    const float* r01 = wc + (unsigned)K0 * sK + (unsigned)J1 * sJ;
+    const float* r10 = wc + (unsigned)K1 * sK + (unsigned)J0 * sJ;
+    const float* r11 = wc + (unsigned)K1 * sK + (unsigned)J1 * sJ;
+    // the four fine cells draw on coarse columns I-1 .. I+2 around I = fi / 2
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+        const int i = fi + m;
+        const int I0 = i >> 1, I1 = pclamp((i & 1) ? I0 + 1 : I0 - 1, cd.n0);
+        auto row = [&](const float* w) { return 0.75f * __ldg(w + I0) + 0.25f * __ldg(w + I1); };
+        float k0 = 0.75f * row(r00) + 0.25f * row(r01);
+        float k1 = 0.75f * row(r10) + 0.25f * row(r11);
+        out[m] = 0.75f * k0 + 0.25f * k1;
+    }
+}
+
 // w_l = gain * (ydiv ? y : s y) + P w_{l+1}   (wc null on the coarsest level); with yn, the
 // network term is odd: y <- (y - yn) / 2 (yn = the network applied to the negated input)
 __global__ void __launch_bounds__(256) prolong_kernel(Dims3 fd, Dims3 cd, const float* wc, const float* y, const float* yn, int ydiv,
@@ -349,12 +398,14 @@ __global__ void __launch_bounds__(LB) precond_z_kernel(long long N, Dims3 fd, Di
         float R[4], D[4], Z[4], Q[4];
         uint8_t F[4];
         un4(ld4(r, q), R); un4(ld4(invD, q), D); un4(ld4(qprev, q), Q); st_flags4(st, q, F);
+        float PW[4] = {0.f, 0.f, 0.f, 0.f};
+        if (w1) prolong4(fd, cd, w1, q, PW);
 #pragma unroll
         for (int m = 0; m < 4; ++m) {
             if (F[m] == ST_INACTIVE) Z[m] = 0.f;
             else {
                 Z[m] = D[m] * R[m];
-                if (w1 && F[m] == ST_ACTIVE) Z[m] += prolong_at(fd, cd, w1, 4 * q + m);
+                if (F[m] == ST_ACTIVE) Z[m] += PW[m];
             }
             v[0] += (double)Z[m] * Q[m];
         }
@@ -542,12 +593,14 @@ __global__ void __launch_bounds__(LB) bs_z_kernel(long long N, Dims3 fd, Dims3 c
         float X[4], D[4], Y[4];
         uint8_t F[4];
         un4(ld4(x, q), X); un4(ld4(invD, q), D); st_flags4(st, q, F);
+        float PW[4] = {0.f, 0.f, 0.f, 0.f};
+        if (w1) prolong4(fd, cd, w1, q, PW);
 #pragma unroll
         for (int m = 0; m < 4; ++m) {
             if (F[m] == ST_INACTIVE) Y[m] = 0.f;
             else {
                 Y[m] = D[m] * X[m];
-                if (w1 && F[m] == ST_ACTIVE) Y[m] += prolong_at(fd, cd, w1, 4 * q + m);
+                if (F[m] == ST_ACTIVE) Y[m] += PW[m];
             }
         }
         st4(y, q, Y);
