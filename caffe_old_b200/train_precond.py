@@ -1,0 +1,86 @@
+"""Train the learned preconditioner on the GPU and write the parameters the package ships
+(caffe_old_b200/data/precond_params.npy).
+
+Training pairs come from the plain FP64 solver's first steps on several seeds of the IB
+channel case (Re ~ U[100, 300]):
+* the (b, x*) of every pressure-correction solve;
+* residual/correction pairs (b - A x_k, x* - x_k) from plain re-solves truncated after 8, 32
+  and 128 iterations;
+* multi-scale synthetic pairs (A e, e).
+
+All pairs live in HBM on one handle, and the network is trained there by the library's
+tensor-core forward and backward passes (Adam, energy-norm loss).
+
+  python -m caffe_old_b200.train_precond [--dims 256 128 128] [--seeds 1 2 3 4] [--steps-per-seed 4]
+                                         [--random 128] [--train-steps 1500] [--out path]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import time
+
+import numpy as np
+
+from . import cases as C
+from . import precond as P
+from .solver import make_solver
+
+
+def main(argv=None) -> dict:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--dims", type=int, nargs=3, default=(256, 128, 128))
+    ap.add_argument("--seeds", type=int, nargs="+", default=(11, 12, 13, 14))
+    ap.add_argument("--steps-per-seed", type=int, default=4)
+    ap.add_argument("--snapshots", type=int, default=3)
+    ap.add_argument("--random", type=int, default=128)
+    ap.add_argument("--train-steps", type=int, default=1500)
+    ap.add_argument("--batch", type=int, default=4)
+    ap.add_argument("--lr", type=float, default=5e-4)
+    ap.add_argument("--out", default=P.DEFAULT_WEIGHTS)
+    args = ap.parse_args(argv)
+    dims = tuple(args.dims)
+    t0 = time.time()
+    per_solve = 1 + args.snapshots
+    handles = []
+    store = None
+    for q, seed in enumerate(args.seeds):
+        nodes, spec, _ = C.config4_channel_sphere(dims, seed=seed)
+        s = make_solver(nodes, spec.replace(p_form="fp64"))
+        cap = args.steps_per_seed * spec.n_inner * spec.n_pcorr * per_solve
+        if store is None:
+            # the first seed's handle holds every pair and trains; the others hand theirs over
+            store = s
+            total = cap * len(args.seeds) + args.random
+            P.record_pairs(s, total, args.snapshots)
+        else:
+            P.record_pairs(s, cap, args.snapshots)
+        for _ in range(args.steps_per_seed):
+            s.solve()
+        if s is not store:
+            P.copy_pairs(store, s)
+            s.close()
+        else:
+            P.record_pairs(s, 0)
+        handles.append(seed)
+    P.add_random_pairs(store, args.random, seed=7)
+    n = P.pair_count(store)
+    t1 = time.time()
+    before = {m: float(P.evaluate(store, m).mean()) for m in ("jacobi", "levels")}
+    params, hist = P.train(store, P.identity_params(0), steps=args.train_steps, batch=args.batch, lr=args.lr, seed=1)
+    after = float(P.evaluate(store, "network").mean())
+    t2 = time.time()
+    store.close()
+    os.makedirs(os.path.dirname(os.path.abspath(args.out)), exist_ok=True)
+    np.save(args.out, params.astype(np.float32))
+    info = {"pairs": n, "seeds": list(args.seeds), "dims": list(dims), "pair_generation_s": round(t1 - t0, 1),
+            "training_s": round(t2 - t1, 1), "loss_jacobi": before["jacobi"], "loss_levels": before["levels"],
+            "loss_network": after, "loss_first_steps": [float(v) for v in hist[:5]],
+            "loss_last_steps": [float(v) for v in hist[-5:]], "out": args.out}
+    print(json.dumps(info), flush=True)
+    return info
+
+
+if __name__ == "__main__":
+    main()
