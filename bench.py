@@ -250,7 +250,9 @@ def configure_precond(dev, args):
     if params is not None:
         P.set_params(dev, params)
     P.set_mode(dev, args.precond)
-    P.set_options(dev, args.inner, args.net_from, args.restart)
+    net_from = args.net_from if args.net_from is not None else int(P.default_info().get("net_from", 1) if not args.params else 1)
+    args.net_from = net_from
+    P.set_options(dev, args.inner, net_from, args.restart)
     return params
 
 
@@ -417,7 +419,8 @@ def main():
     ap.add_argument("--p-form", default="learned_mixed", choices=tuple(C.P_FORMS))
     ap.add_argument("--precond", default="levels", choices=("levels", "network", "jacobi"))
     ap.add_argument("--inner", default="auto", choices=("auto", "fcg", "bicgstab", "fgmres"))
-    ap.add_argument("--net-from", type=int, default=1)
+    ap.add_argument("--net-from", type=int, default=None, help="first pyramid level that runs the network "
+                    "(default: the one the shipped parameters were trained for)")
     ap.add_argument("--restart", type=int, default=40)
     ap.add_argument("--params", default=None, help="network parameters (.npy); default: the shipped ones")
     ap.add_argument("--size", type=int, default=None)

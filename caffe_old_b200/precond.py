@@ -71,6 +71,16 @@ def load_default() -> np.ndarray | None:
     return None
 
 
+def default_info() -> dict:
+    """How the shipped parameters were trained (first network level, pairs, losses), or {}."""
+    path = os.path.splitext(DEFAULT_WEIGHTS)[0] + ".json"
+    if os.path.exists(path):
+        import json
+        with open(path) as f:
+            return json.load(f)
+    return {}
+
+
 def _check(rc: int, what: str) -> None:
     if rc != 0:
         raise CaffeError(f"{what}: " + last_error())
@@ -152,5 +162,5 @@ def evaluate(solver, mode: str = "network") -> np.ndarray:
     return out[:n]
 
 
-__all__ = ["PARAMS", "MODES", "INNER", "identity_params", "load_default", "set_params", "get_params", "set_mode", "set_options",
+__all__ = ["PARAMS", "MODES", "INNER", "identity_params", "load_default", "default_info", "set_params", "get_params", "set_mode", "set_options",
            "record_pairs", "pair_count", "add_pairs", "add_random_pairs", "copy_pairs", "train", "evaluate", "weight_view"]

@@ -37,7 +37,8 @@ def main(argv=None) -> dict:
     ap.add_argument("--random", type=int, default=128)
     ap.add_argument("--train-steps", type=int, default=1500)
     ap.add_argument("--batch", type=int, default=4)
-    ap.add_argument("--lr", type=float, default=5e-4)
+    ap.add_argument("--lr", type=float, default=2e-4)
+    ap.add_argument("--net-from", type=int, default=1, help="first pyramid level that runs the network")
     ap.add_argument("--out", default=P.DEFAULT_WEIGHTS)
     args = ap.parse_args(argv)
     dims = tuple(args.dims)
@@ -67,6 +68,7 @@ def main(argv=None) -> dict:
     P.add_random_pairs(store, args.random, seed=7)
     n = P.pair_count(store)
     t1 = time.time()
+    P.set_options(store, "auto", args.net_from)
     before = {m: float(P.evaluate(store, m).mean()) for m in ("jacobi", "levels")}
     params, hist = P.train(store, P.identity_params(0), steps=args.train_steps, batch=args.batch, lr=args.lr, seed=1)
     after = float(P.evaluate(store, "network").mean())
@@ -74,10 +76,13 @@ def main(argv=None) -> dict:
     store.close()
     os.makedirs(os.path.dirname(os.path.abspath(args.out)), exist_ok=True)
     np.save(args.out, params.astype(np.float32))
-    info = {"pairs": n, "seeds": list(args.seeds), "dims": list(dims), "pair_generation_s": round(t1 - t0, 1),
+    info = {"net_from": args.net_from, "pairs": n, "seeds": list(args.seeds), "dims": list(dims),
+            "train_steps": args.train_steps, "batch": args.batch, "lr": args.lr, "pair_generation_s": round(t1 - t0, 1),
             "training_s": round(t2 - t1, 1), "loss_jacobi": before["jacobi"], "loss_levels": before["levels"],
             "loss_network": after, "loss_first_steps": [float(v) for v in hist[:5]],
             "loss_last_steps": [float(v) for v in hist[-5:]], "out": args.out}
+    with open(os.path.splitext(args.out)[0] + ".json", "w") as f:
+        json.dump(info, f, indent=1)
     print(json.dumps(info), flush=True)
     return info
 
