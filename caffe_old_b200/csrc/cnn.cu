@@ -5,14 +5,16 @@
 // (k*nJ + j)*nI + i; zero padding outside the lattice.
 //
 // One CTA (128 threads, 4 warps) owns an 8 (i) x 16 (j) tile of output cells and marches
-// through KC consecutive k-planes.  For each output plane the tile is one UMMA problem
+// through KC consecutive k-planes, software-pipelined: four staged input planes rotate and two
+// TMEM accumulators alternate, so the MMAs of plane k+1 run while the CTA stores plane k and
+// stages plane k+2.  For each output plane the tile is one UMMA problem
 // M = 128 cells, N = 16 output channels, accumulated over the 27 taps with one
 // tcgen05.mma.kind::f16 of K = 16 input channels per tap into a 128 x 16 FP32 accumulator
 // in tensor memory.  Operands are in shared memory in the canonical no-swizzle K-major
 // layout (core matrices of 8 rows x 16 bytes): the A operand of tap (dk, dj, di) is input
 // plane k+dk shifted by di along i (three i-shifted copies of each plane are staged) and
 // by dj rows of the tile (a whole-core-matrix offset in the descriptor); B is the tap's
-// 16 x 16 weight block.  Three input planes rotate as the CTA moves along k, so each input
+// 16 x 16 weight block.  Input planes rotate through the staging slots as the CTA moves along k, so each input
 // plane is read from global memory once per tile.  The epilogue reads the accumulator with
 // tcgen05.ld (one TMEM lane per thread = one cell), applies bias / ReLU, or the ReLU mask
 // of the backward pass, and writes bf16 (or FP32 for the network output).
@@ -33,7 +35,8 @@ constexpr int TI = 8, TJ = 16;          // tile: 8 cells along i, 16 along j -> 
 constexpr int ROWS = TJ + 2;            // staged j-rows (one halo row each side)
 constexpr int GROUP_BYTES = 256;        // one j-row of 8 cells x 16 channels, canonical layout
 constexpr int BUF_BYTES = ROWS * GROUP_BYTES;          // 4608
-constexpr int NBUF = 9;                 // 3 planes x 3 i-shifts
+constexpr int NPL = 4;                  // rotating staged planes (3 in use by the MMAs, 1 being filled)
+constexpr int NBUF = 3 * NPL;           // planes x 3 i-shifts
 constexpr int W_BYTES = 27 * 512;       // 27 taps x 16 x 16 bf16
 constexpr uint32_t TMEM_COLS = 32;
 constexpr long long WAIT_LIMIT = 1ll << 20;   // try_wait rounds (each may block briefly): about a second at most
@@ -135,7 +138,7 @@ __global__ void __launch_bounds__(128) conv3d_tc_kernel(Lat L, const __nv_bfloat
     unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     unsigned char* wsm = smem;                                // W_BYTES
     unsigned char* bufs = smem + W_BYTES;                     // NBUF x BUF_BYTES
-    __shared__ __align__(8) uint64_t mbar;
+    __shared__ __align__(8) uint64_t mbar[2];
     __shared__ uint32_t tmem_base_sh;
     __shared__ float bias_sh[16];
 
@@ -149,56 +152,77 @@ __global__ void __launch_bounds__(128) conv3d_tc_kernel(Lat L, const __nv_bfloat
         reinterpret_cast<uint4*>(wsm)[u] = reinterpret_cast<const uint4*>(wpack)[u];
     if (threadIdx.x < 16) bias_sh[threadIdx.x] = bias ? bias[threadIdx.x] : 0.f;
     if (threadIdx.x == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar)));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[0])));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[1])));
     }
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base_sh)),
                      "r"(TMEM_COLS));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
-    // planes k0-1 and k0 into rotation slots 0 and 1
-    stage_plane(bufs, 0, in, L, i0, j0, k0 - 1);
-    stage_plane(bufs, 1, in, L, i0, j0, k0);
+    // plane p lives in rotation slot (p - k0 + 1) mod 4; planes k0-1, k0, k0+1 first
+    auto slot_of = [&](int plane) { return (plane - k0 + 1) & (NPL - 1); };
+    stage_plane(bufs, slot_of(k0 - 1), in, L, i0, j0, k0 - 1);
+    stage_plane(bufs, slot_of(k0), in, L, i0, j0, k0);
+    stage_plane(bufs, slot_of(k0 + 1), in, L, i0, j0, k0 + 1);
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;");
     const uint32_t tmem = tmem_base_sh;
-    const uint32_t bar = smem_u32(&mbar);
-    uint32_t phase = 0;
+    const uint32_t bar[2] = {smem_u32(&mbar[0]), smem_u32(&mbar[1])};
+    uint32_t phase[2] = {0u, 0u};
     bool failed = false;
-    int slotM = 0, slotC = 1, slotP = 2;   // planes k-1, k, k+1
+    int accFail = 0;
+    bool otherPending = false;
+
+    // the 27 MMAs of output plane k into accumulator acc (TMEM columns 16 acc .. 16 acc + 15),
+    // issued by one thread, completion signalled on bar[acc]
+    auto issue = [&](int k, int acc) {
+        if (threadIdx.x != 0) return;
+        const uint32_t wbase = smem_u32(wsm);
+        const uint32_t bbase = smem_u32(bufs);
+        const int slots[3] = {slot_of(k - 1), slot_of(k), slot_of(k + 1)};
+        int t = 0;
+#pragma unroll 1
+        for (int dk = 0; dk < 3; ++dk)
+#pragma unroll 1
+            for (int dj = 0; dj < 3; ++dj)
+#pragma unroll 1
+                for (int di = 0; di < 3; ++di, ++t) {
+                    uint32_t a_addr = bbase + (uint32_t)((slots[dk] * 3 + di) * BUF_BYTES + dj * GROUP_BYTES);
+                    uint64_t ad = sdesc(a_addr, 128, 256);
+                    uint64_t bd = sdesc(wbase + (uint32_t)(t * 512), 128, 256);
+                    mma_bf16(tmem + (uint32_t)(16 * acc), ad, bd, t > 0 ? 1u : 0u);
+                }
+        mma_commit(bar[acc]);
+    };
+
+    // Pipeline: while the MMAs of plane k+1 run, the CTA finishes plane k (wait, epilogue) and
+    // has already staged plane k+2; plane k+2 overwrites the slot of plane k-2, whose last
+    // reader (the MMAs of plane k-1) completed in the previous iteration.
+    if (k0 < k1) issue(k0, 0);
     for (int k = k0; k < k1; ++k) {
-        stage_plane(bufs, slotP, in, L, i0, j0, k + 1);
+        const int acc = (k - k0) & 1;
+        if (k + 2 <= k1) stage_plane(bufs, slot_of(k + 2), in, L, i0, j0, k + 2);
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         asm volatile("tcgen05.fence::before_thread_sync;");
         __syncthreads();
         asm volatile("tcgen05.fence::after_thread_sync;");
-        if (threadIdx.x == 0) {
-            const uint32_t wbase = smem_u32(wsm);
-            const uint32_t bbase = smem_u32(bufs);
-            int slots[3] = {slotM, slotC, slotP};
-            int t = 0;
-#pragma unroll 1
-            for (int dk = 0; dk < 3; ++dk)
-#pragma unroll 1
-                for (int dj = 0; dj < 3; ++dj)
-#pragma unroll 1
-                    for (int di = 0; di < 3; ++di, ++t) {
-                        uint32_t a_addr = bbase + (uint32_t)((slots[dk] * 3 + di) * BUF_BYTES + dj * GROUP_BYTES);
-                        uint64_t ad = sdesc(a_addr, 128, 256);
-                        uint64_t bd = sdesc(wbase + (uint32_t)(t * 512), 128, 256);
-                        mma_bf16(tmem, ad, bd, t > 0 ? 1u : 0u);
-                    }
-            mma_commit(bar);
-        }
-        bool ok = mbar_wait_bounded(bar, phase);
-        phase ^= 1u;
+        if (k + 1 < k1) issue(k + 1, acc ^ 1);
+        bool ok = mbar_wait_bounded(bar[acc], phase[acc]);
+        phase[acc] ^= 1u;
         // the decision to stop must be the same in every thread (barriers follow)
-        if (__syncthreads_or(ok ? 0 : 1)) { failed = true; break; }
+        if (__syncthreads_or(ok ? 0 : 1)) {
+            failed = true;
+            accFail = acc;
+            otherPending = k + 1 < k1;
+            break;
+        }
         asm volatile("tcgen05.fence::after_thread_sync;");
         // epilogue: thread = TMEM lane = output cell
         float v[16];
-        tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16), v);
+        tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(16 * acc), v);
         int m = threadIdx.x;
         int i = i0 + (m & 7), j = j0 + (m >> 3);
         if (i < L.nI && j < L.nJ) {
@@ -223,14 +247,16 @@ __global__ void __launch_bounds__(128) conv3d_tc_kernel(Lat L, const __nv_bfloat
                 dst[1] = reinterpret_cast<uint4*>(ob)[1];
             }
         }
-        // rotate planes; the accumulator is re-written by the next plane's first MMA only
-        // after every thread has finished reading it (barrier at the top of the loop)
-        int tmp = slotM; slotM = slotC; slotC = slotP; slotP = tmp;
+        // the accumulator just read is rewritten by the MMAs of plane k+2, issued in the next
+        // iteration after its barrier, i.e. after every thread has finished this epilogue
         asm volatile("tcgen05.fence::before_thread_sync;");
     }
     if (failed) {
         if (threadIdx.x == 0) atomicExch(err, 1);
-        mbar_wait_bounded(bar, phase ^ 1u);   // let any MMA in flight finish before freeing TMEM
+        // let the MMAs still in flight (at most the other accumulator's plane) finish before
+        // the tensor memory is freed
+        mbar_wait_bounded(bar[accFail], phase[accFail] ^ 1u);        // the plane whose wait ran out
+        if (otherPending) mbar_wait_bounded(bar[accFail ^ 1], phase[accFail ^ 1]);
     }
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
