@@ -233,65 +233,59 @@ __global__ void __launch_bounds__(256) restrict_kernel(Dims3 fd, Dims3 cd, const
     __shared__ float s0[RFK][RFJ][RFI];
     __shared__ float t1[RFK][RFJ][RCI];
     __shared__ float t2[RFK][RCJ][RCI];
+    __shared__ float wI[RCI][4], wJ[RCJ][4], wK[RCK][4];   // clamped trilinear weights of this tile
     const int I0 = blockIdx.x * RCI, J0 = blockIdx.y * RCJ, K0 = blockIdx.z * RCK;
     const int fi0 = 2 * I0 - 1, fj0 = 2 * J0 - 1, fk0 = 2 * K0 - 1;
     const unsigned fsJ = (unsigned)fd.n0, fsK = (unsigned)fd.n0 * (unsigned)fd.n1;
-    // stage the fine tile: four elements per thread and round, their loads issued together
-    constexpr int TOT = RFI * RFJ * RFK;
-    for (int u0 = threadIdx.x; u0 < TOT; u0 += 4 * blockDim.x) {
-        unsigned fidx[4];
-        bool in[4];
+    if (threadIdx.x < 4 * RCI) {
+        int ci = threadIdx.x >> 2, m = threadIdx.x & 3, I = I0 + ci;
+        wI[ci][m] = rweight_in(2 * I - 1 + m, fd.n0, I, cd.n0);
+    } else if (threadIdx.x < 4 * RCI + 4 * RCJ) {
+        int u = threadIdx.x - 4 * RCI, cj = u >> 2, m = u & 3, J = J0 + cj;
+        wJ[cj][m] = rweight_in(2 * J - 1 + m, fd.n1, J, cd.n1);
+    } else if (threadIdx.x < 4 * RCI + 4 * RCJ + 4 * RCK) {
+        int u = threadIdx.x - 4 * RCI - 4 * RCJ, ck = u >> 2, m = u & 3, K = K0 + ck;
+        wK[ck][m] = rweight_in(2 * K - 1 + m, fd.n2, K, cd.n2);
+    }
+    // stage the fine tile: one warp per (j, k) row of RFI cells, lanes along i; the three loads
+    // of an element are independent
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarp = blockDim.x >> 5;
+    for (int row = warp; row < RFJ * RFK; row += nwarp) {
+        const int lj = row % RFJ, lk = row / RFJ;
+        const int fj = fj0 + lj, fk = fk0 + lk;
+        const bool rowIn = fj >= 0 && fj < fd.n1 && fk >= 0 && fk < fd.n2;
+        const unsigned rowBase = rowIn ? (unsigned)fk * fsK + (unsigned)fj * fsJ : 0u;
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            int u = u0 + q * blockDim.x;
-            int li = u % RFI, lj = (u / RFI) % RFJ, lk = u / (RFI * RFJ);
-            int fi = fi0 + li, fj = fj0 + lj, fk = fk0 + lk;
-            in[q] = u < TOT && fi >= 0 && fi < fd.n0 && fj >= 0 && fj < fd.n1 && fk >= 0 && fk < fd.n2;
-            fidx[q] = in[q] ? (unsigned)fk * fsK + (unsigned)fj * fsJ + (unsigned)fi : 0u;
-        }
-        float fv[4], dv[4];
-        uint8_t sv[4];
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            fv[q] = (in[q] && fin) ? __ldg(fin + fidx[q]) : 1.f;
-            dv[q] = (in[q] && invD) ? __ldg(invD + fidx[q]) : 1.f;
-            sv[q] = (in[q] && st) ? __ldg(st + fidx[q]) : (uint8_t)ST_ACTIVE;
-        }
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            int u = u0 + q * blockDim.x;
-            if (u < TOT) {
-                int li = u % RFI, lj = (u / RFI) % RFJ, lk = u / (RFI * RFJ);
-                s0[lk][lj][li] = (in[q] && sv[q] == ST_ACTIVE) ? fv[q] * dv[q] : 0.f;
-            }
+        for (int li = lane; li < RFI + 31; li += 32) {
+            if (li >= RFI) break;
+            const int fi = fi0 + li;
+            const bool in = rowIn && fi >= 0 && fi < fd.n0;
+            const unsigned f = in ? rowBase + (unsigned)fi : 0u;
+            const float fv = (in && fin) ? __ldg(fin + f) : 1.f;
+            const float dv = (in && invD) ? __ldg(invD + f) : 1.f;
+            const uint8_t sv = (in && st) ? __ldg(st + f) : (uint8_t)ST_ACTIVE;
+            s0[lk][lj][li] = (in && sv == ST_ACTIVE) ? fv * dv : 0.f;
         }
     }
     __syncthreads();
     for (int u = threadIdx.x; u < RFK * RFJ * RCI; u += blockDim.x) {
-        int ci = u % RCI, lj = (u / RCI) % RFJ, lk = u / (RCI * RFJ);
-        int I = I0 + ci;
-        float a = 0.f;
-#pragma unroll
-        for (int m = 0; m < 4; ++m) a += rweight_in(2 * I - 1 + m, fd.n0, I, cd.n0) * s0[lk][lj][2 * ci + m];
-        t1[lk][lj][ci] = a;
+        const int ci = u & (RCI - 1), rest = u / RCI, lj = rest % RFJ, lk = rest / RFJ;
+        const float* src = &s0[lk][lj][2 * ci];
+        t1[lk][lj][ci] = wI[ci][0] * src[0] + wI[ci][1] * src[1] + wI[ci][2] * src[2] + wI[ci][3] * src[3];
     }
     __syncthreads();
     for (int u = threadIdx.x; u < RFK * RCJ * RCI; u += blockDim.x) {
-        int ci = u % RCI, cj = (u / RCI) % RCJ, lk = u / (RCI * RCJ);
-        int J = J0 + cj;
-        float a = 0.f;
-#pragma unroll
-        for (int m = 0; m < 4; ++m) a += rweight_in(2 * J - 1 + m, fd.n1, J, cd.n1) * t1[lk][2 * cj + m][ci];
-        t2[lk][cj][ci] = a;
+        const int ci = u & (RCI - 1), cj = (u / RCI) & (RCJ - 1), lk = u / (RCI * RCJ);
+        t2[lk][cj][ci] = wJ[cj][0] * t1[lk][2 * cj][ci] + wJ[cj][1] * t1[lk][2 * cj + 1][ci] + wJ[cj][2] * t1[lk][2 * cj + 2][ci] +
+                         wJ[cj][3] * t1[lk][2 * cj + 3][ci];
     }
     __syncthreads();
     for (int u = threadIdx.x; u < RCK * RCJ * RCI; u += blockDim.x) {
-        int ci = u % RCI, cj = (u / RCI) % RCJ, ck = u / (RCI * RCJ);
-        int I = I0 + ci, J = J0 + cj, K = K0 + ck;
+        const int ci = u & (RCI - 1), cj = (u / RCI) & (RCJ - 1), ck = u / (RCI * RCJ);
+        const int I = I0 + ci, J = J0 + cj, K = K0 + ck;
         if (I >= cd.n0 || J >= cd.n1 || K >= cd.n2) continue;
-        float acc = 0.f;
-#pragma unroll
-        for (int m = 0; m < 4; ++m) acc += rweight_in(2 * K - 1 + m, fd.n2, K, cd.n2) * t2[2 * ck + m][cj][ci];
+        float acc = wK[ck][0] * t2[2 * ck][cj][ci] + wK[ck][1] * t2[2 * ck + 1][cj][ci] + wK[ck][2] * t2[2 * ck + 2][cj][ci] +
+                    wK[ck][3] * t2[2 * ck + 3][cj][ci];
         acc *= scale;
         unsigned c = ((unsigned)K * (unsigned)cd.n1 + (unsigned)J) * (unsigned)cd.n0 + (unsigned)I;
         out[c] = acc;
