@@ -234,6 +234,10 @@ def run_reference(args, world, rank, pg):
 # level pyramid's restriction reads and the prolonged term's reads included; coarse levels
 # excluded): flexible BiCGStab 170 B (two preconditioner applications), flexible CG 110 B
 LEARNED_BYTES = {"bicgstab": 170.0, "fcg": 110.0}
+# DRAM bytes per cell and inner BiCGStab iteration of the fine-lattice kernels, from one ncu
+# capture (dram__bytes_read.sum + dram__bytes_write.sum, 240x160x160 case, per cell;
+# profiles/c5_ibsphere_learned_traffic.md); traffic grows with the cell count
+LEARNED_TRAFFIC_PER_CELL = {"bicgstab": 154.0}
 
 
 def configure_precond(dev, args):
@@ -326,7 +330,9 @@ def run_b200(args, world, rank, local, pg):
     roofline = {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": hbm, "unit": "GB/s",
                 "frac": (achieved / hbm) if achieved else None,
                 "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
-                "traffic": None, "bytes_per_row_iteration": per_row,
+                "traffic": (LEARNED_TRAFFIC_PER_CELL[method] * N if learned and method in LEARNED_TRAFFIC_PER_CELL else None),
+                "traffic_unit": "bytes per inner iteration (ncu capture, scaled by cells)",
+                "bytes_per_row_iteration": per_row,
                 "p_solve_ms_per_step": p_ms / args.steps, "iterations_per_step": p_iters / args.steps}
 
     # end to end through the C ABI with host buffers: per step, upload the solver state

@@ -60,12 +60,14 @@ struct Scal {
     double zq, pq, pr;          // (z, q_prev), (p, q), (p, r)
     double alpha, beta;
     double bb, tol2, rr64;      // outer: ||b||^2, tolerance, current true ||r||^2
+    double prev64;              // true ||r||^2 of the previous refinement pass
     double nact;
     double loss;
     double rho, omega, rv, ts, tt;   // flexible BiCGStab: (rhat, r), omega, (rhat, v), (t, s), (t, t)
     int done;                   // inner solve finished
     int odone;                  // outer solve finished
     int iters, outer, status, first;
+    int stall;                  // consecutive refinement passes that cut ||r|| by less than 10%
 };
 
 __device__ __forceinline__ void block_sums(double* v, int K, double* part) {
@@ -161,6 +163,13 @@ __global__ void outer_check_kernel(const double* part, int nblk, Scal* S, int ma
         bool conv = t[0] <= S->tol2 || !(S->bb > 0.);
         if (t[0] != t[0]) { S->status = 3; conv = true; }
         if (!conv && S->outer >= max_outer) { S->status = 1; conv = true; }
+        // stagnation: three refinement passes in a row that leave more than 90% of ||r|| end the
+        // solve with status 2, so the plain FP64 solve takes over at once
+        if (!conv && S->outer > 0) {
+            S->stall = t[0] > 0.81 * S->prev64 ? S->stall + 1 : 0;
+            if (S->stall >= 3) { S->status = 2; conv = true; }
+        }
+        S->prev64 = t[0];
         if (conv) S->odone = 1;
         S->done = S->odone;   // no inner solve when the outer one is finished
         S->outer += conv ? 0 : 1;
@@ -1077,8 +1086,9 @@ int learned_solve(LearnedWork& lw, const OpSym& A, const uint8_t* status, const 
         count_active_kernel<<<nb, LB, 0, st>>>(N, status, lw.part);
         count_finish<<<1, LB, 0, st>>>(lw.part, nb, lw.mean + 1);
     }
-    // FGMRES: one restart cycle per refinement pass, as many cycles as the iteration budget allows
-    const int max_outer = fgmres ? std::max(12, maxit / m + 1) : 12;
+    // FGMRES: one restart cycle per refinement pass, as many cycles as the iteration budget
+    // allows, at most 100
+    const int max_outer = fgmres ? std::min(100, std::max(12, maxit / m + 1)) : 12;
     const int chunk = 8;
     for (int outer = 0; outer <= max_outer; ++outer) {
         outer_residual_kernel<<<nb, LB, 0, st>>>(A, N, b, x, lw.r, lw.part, S);
