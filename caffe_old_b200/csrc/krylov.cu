@@ -404,111 +404,6 @@ __global__ void __launch_bounds__(KB) bicgstab_kernel(Op A, KArgs a) {
     }
 }
 
-// ------------------------------------------------------------------ CG
-template <class Op>
-__global__ void __launch_bounds__(KB) cg_kernel(Op A, KArgs a) {
-    cg::grid_group grid = cg::this_grid();
-    const long long N = a.N;
-    const long long T = (long long)gridDim.x * blockDim.x;
-    const long long t0 = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    const double* invD = a.invD;
-    double* z = a.rp;     // preconditioned residual
-    double* q = a.t;      // A p
-    int par = 0;
-    if (a.project) project_mean(grid, const_cast<double*>(a.b), N, t0, T, a.partials, par);
-    double acc[2];
-    acc[0] = acc[1] = 0.;
-    for (long long c = t0; c < N; c += T) {
-        double bv = a.b[c];
-        a.x[c] = 0.;
-        a.r[c] = bv;
-        double zv = __ldg(invD + c) * bv;
-        z[c] = zv;
-        acc[0] += bv * zv;
-        acc[1] += bv * bv;
-    }
-    double tot[2];
-    grid_reduce<2>(grid, acc, a.partials, par, tot);
-    double rz = tot[0], bb = tot[1];
-    double tol2 = a.rtol * a.rtol * bb;
-    int it = 0, status = 0;
-    double relres = 0.;
-    bool done = !(bb > 0.), fresh = true;
-    if (bb != bb) status = 3;
-    double beta = 0.;
-    int cur = 0;
-    while (!done) {
-        const double* po = a.p[cur];
-        double* pn = a.p[cur ^ 1];
-        // ---- phase 1: p = z + beta p_old;  q = A p;  (p, q)
-        double pq = 0.;
-        for (long long c = t0; c < N; c += T) {
-            auto pnew = [&](long long e) -> double {
-                double zv = ldcg(z + e);
-                return fresh ? zv : zv + beta * ldcg(po + e);
-            };
-            double y[1];
-            apply<1>(A, c, [&](int, long long e) { return pnew(e); }, y);
-            double pc = pnew(c);
-            pn[c] = pc;
-            q[c] = y[0];
-            pq += pc * y[0];
-        }
-        double t1[1];
-        {
-            double tmp[1] = {pq};
-            grid_reduce<1>(grid, tmp, a.partials, par, t1);
-        }
-        bool needT = false;
-        if (t1[0] == 0. || t1[0] != t1[0]) {
-            needT = true;
-        } else {
-            double alpha = rz / t1[0];
-            // ---- phase 2: x += alpha p;  r -= alpha q;  z = D^-1 r;  (r, z), (r, r)
-            acc[0] = acc[1] = 0.;
-            for (long long c = t0; c < N; c += T) {
-                double pc = ldcg(pn + c);
-                a.x[c] = a.x[c] + alpha * pc;
-                double rn = a.r[c] - alpha * ldcg(q + c);
-                a.r[c] = rn;
-                double zv = __ldg(invD + c) * rn;
-                z[c] = zv;
-                acc[0] += rn * zv;
-                acc[1] += rn * rn;
-            }
-            grid_reduce<2>(grid, acc, a.partials, par, tot);
-            it += 1;
-            fresh = false;
-            double rr = tot[1];
-            if (rr <= tol2 || it >= a.maxit || rr != rr) needT = true;
-            beta = tot[0] / rz;
-            rz = tot[0];
-            cur ^= 1;
-        }
-        if (needT) {
-            // ---- true residual r = b - A x, z = D^-1 r
-            acc[0] = acc[1] = 0.;
-            for (long long c = t0; c < N; c += T) {
-                double y[1];
-                apply<1>(A, c, [&](int, long long e) { return ldcg(a.x + e); }, y);
-                double rt = a.b[c] - y[0];
-                a.r[c] = rt;
-                double zv = __ldg(invD + c) * rt;
-                z[c] = zv;
-                acc[0] += rt * zv;
-                acc[1] += rt * rt;
-            }
-            grid_reduce<2>(grid, acc, a.partials, par, tot);
-            relres = sqrt(tot[1] / bb);
-            if (tot[1] <= tol2) { done = true; status = 0; }
-            else if (tot[1] != tot[1]) { done = true; status = 3; }
-            else if (it >= a.maxit) { done = true; status = 1; }
-            else { fresh = true; rz = tot[0]; beta = 0.; }
-        }
-    }
-    if (blockIdx.x == 0 && threadIdx.x == 0) { a.out->iters[0] = it; a.out->relres[0] = relres; a.out->status[0] = status; }
-}
-
 // ------------------------------------------------------------------ CG, one reduction per iteration
 // Chronopoulos & Gear (1989) form of preconditioned CG: with u = M^-1 r and w = A u the two
 // inner products (r, u) and (w, u) are taken together, so an iteration is one sweep and one
