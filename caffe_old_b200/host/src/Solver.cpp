@@ -11,6 +11,9 @@
 //   LinearSolvers.pressureCorrectionForm   fp64 | mixed | learned | learned_mixed
 //   LearnedPreconditioner.mode         levels | network | jacobi
 //   LearnedPreconditioner.parameters   file of caffe_precond_param_count() floats (raw or .npy)
+//   LearnedPreconditioner.firstNetworkLevel   first pyramid level that runs the network (1)
+//   LearnedPreconditioner.innerMethod  auto | fcg | bicgstab | fgmres
+//   LearnedPreconditioner.restart      FGMRES cycle length (40)
 #include "Solver.h"
 
 #include <cstring>
@@ -148,6 +151,13 @@ Solver::Solver(const Input& input, const HexaFvmMesh& mesh, int kind) : mesh_(me
         }
         if (caffe_dev_set_precond_mode(h_, m) != 0)
             Output::raiseException("Solver", "Solver", std::string("cannot set the preconditioner mode: ") + caffe_last_error());
+        std::string inner = c.get<std::string>("LearnedPreconditioner.innerMethod", std::string("auto"));
+        int im = inner == "fcg" ? 1 : (inner == "bicgstab" ? 2 : (inner == "fgmres" ? 3 : 0));
+        if (inner != "auto" && im == 0) Output::raiseException("Solver", "Solver", "unknown inner method \"" + inner + "\"");
+        int netFrom = c.get<int>("LearnedPreconditioner.firstNetworkLevel", 1);
+        int restart = c.get<int>("LearnedPreconditioner.restart", 40);
+        if (caffe_dev_set_precond_options(h_, im, netFrom, restart) != 0)
+            Output::raiseException("Solver", "Solver", std::string("cannot set the preconditioner options: ") + caffe_last_error());
     }
     mesh.attachSolver(this);
 }
