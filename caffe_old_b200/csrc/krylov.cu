@@ -3,11 +3,12 @@
 // The reference calls PETSc (KSPBCGS + PCSOR, src/Math/SparseMatrix.cpp:86-106) once
 // per system, from a zero initial guess, and returns the iteration count.  PETSc's
 // lexicographic SOR sweep is sequential, so the device solvers use Jacobi
-// preconditioning (BASELINE's plain FP64 GPU path) with the published algorithms:
+// preconditioning (the plain FP64 device path) with the published algorithms:
 //   * BiCGStab (van der Vorst 1992), right-preconditioned, for the momentum system
 //     (three right-hand sides sharing one operator sweep) and for non-symmetric
 //     pressure-correction systems (immersed-boundary ghost rows);
-//   * CG (Hestenes-Stiefel), for the symmetric pressure-correction system.
+//   * CG (Hestenes-Stiefel; Chronopoulos-Gear single-reduction form), for the symmetric
+//     pressure-correction system.
 // Every solve is one kernel launch: all blocks stay resident (cooperative launch) and
 // meet at grid barriers between the phases of an iteration; the dot products are summed
 // per block and then, in every block, over the block partials in a fixed order, so all

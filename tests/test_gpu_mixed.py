@@ -1,7 +1,7 @@
 """Precision form: FP32 inner solves inside FP64 iterative refinement for the pressure
 correction.  Every p' solve must still reach the FP64 true-residual tolerance, and the fields
-stay within 1e-6 relative L2 of the FP64 oracle (the bound BASELINE sets for the combined
-form); the per-field error is printed."""
+stay within 1e-6 relative L2 of the FP64 oracle (the bound for the combined learned +
+mixed-precision form); the per-field error is printed."""
 import numpy as np
 import pytest
 
