@@ -148,3 +148,35 @@ def fcg(A, b, M, rtol=1e-8, maxit=5000):
             return x, it
         p_old, q_old, pq_old = p, q, pq
     return x, maxit
+
+
+def fgmres(A, b, M, m=40, rtol=1e-5, maxit=2000):
+    """Restarted right-preconditioned FGMRES (Saad 1993), FP64, modified Gram-Schmidt."""
+    x = np.zeros_like(b)
+    bn = np.linalg.norm(b)
+    tot = 0
+    while tot < maxit:
+        r = b - A(x)
+        beta = np.linalg.norm(r)
+        if beta <= rtol * bn:
+            return x, tot
+        V, Z = [r / beta], []
+        H = np.zeros((m + 1, m))
+        y = np.zeros(0)
+        for j in range(m):
+            z = M(V[j])
+            w = A(z)
+            Z.append(z)
+            for i in range(j + 1):
+                H[i, j] = np.vdot(w, V[i])
+                w = w - H[i, j] * V[i]
+            H[j + 1, j] = np.linalg.norm(w)
+            tot += 1
+            e1 = np.zeros(j + 2)
+            e1[0] = beta
+            y, *_ = np.linalg.lstsq(H[:j + 2, :j + 1], e1, rcond=None)
+            if np.linalg.norm(H[:j + 2, :j + 1] @ y - e1) <= rtol * bn or H[j + 1, j] == 0.0 or tot >= maxit:
+                break
+            V.append(w / H[j + 1, j])
+        x = x + sum(yi * zi for yi, zi in zip(y, Z))
+    return x, tot

@@ -60,3 +60,28 @@ def test_level_pyramid_cuts_flexible_cg_iterations():
     params = P.identity_params(0)
     _, it_net = LR.fcg(A, b, lambda r: LR.apply_M(r, invD, act, "network", params), 1e-8, 3000)
     assert abs(it_net - its["levels"]) <= 1, (it_net, its)
+
+
+def test_odd_network_form_keeps_fgmres_convergent():
+    """A network with biases and constant input channels has an input-independent part; the
+    odd form (net(x) - net(-x)) / 2 the device applies removes it exactly (the output of a
+    zero residual is zero, and M(-r) = -M(r)), and FGMRES with it converges like the pyramid."""
+    rng = np.random.default_rng(4)
+    dims = (12, 16, 16)
+    A, diag = LR.poisson7(dims)
+    b = rng.standard_normal(dims)
+    invD = 1.0 / diag
+    act = np.ones(dims, bool)
+    params = P.identity_params(1, noise=0.3)
+    for l in range(P.LAYERS):
+        _, bias = P.weight_view(params, l)
+        bias[:] = 0.05 * rng.standard_normal(bias.shape)
+    r = rng.standard_normal(dims)
+    zp = LR.apply_M(r, invD, act, "network", params)
+    zn = LR.apply_M(-r, invD, act, "network", params)
+    assert np.allclose(zp, -zn, atol=1e-12 * np.abs(zp).max())
+    assert np.abs(LR.apply_M(np.zeros(dims), invD, act, "network", params)).max() == 0.0
+    _, it_lev = LR.fgmres(A, b, lambda v: LR.apply_M(v, invD, act, "levels"), 40, 1e-6, 400)
+    x, it_net = LR.fgmres(A, b, lambda v: LR.apply_M(v, invD, act, "network", params), 40, 1e-6, 400)
+    assert np.linalg.norm(b - A(x)) <= 1.01e-6 * np.linalg.norm(b)
+    assert it_net < 3 * it_lev, (it_net, it_lev)
