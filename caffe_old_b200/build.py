@@ -27,10 +27,23 @@ def build_oracle() -> str:
     return os.path.join(_ROOT, "oracle", "_build", "liboracle.so")
 
 
+REFERENCE = "/root/reference"
+
+
+def build_oracle_ref(reference: str = REFERENCE) -> bool:
+    """The reference's own geometry sources, compiled where they lie into oracle/_ref/ (a pin for
+    the oracle's geometry).  Returns False when the reference sources are not present."""
+    if not os.path.exists(os.path.join(reference, "src", "Math", "Geometry.cpp")):
+        return False
+    subprocess.run(["make", "-C", os.path.join(_ROOT, "oracle"), "-s", "ref", f"REF={reference}"], check=True)
+    return True
+
+
 def build_all() -> None:
     build_device()
     build_host()
     build_oracle()
+    build_oracle_ref()
 
 
 if __name__ == "__main__":

@@ -1,0 +1,51 @@
+// C entry points over the reference's own geometry code (src/Math/Geometry.cpp, Sphere.cpp,
+// Vector3D.cpp, Tensor3D.cpp), compiled where it lies by `make -C oracle ref` into
+// oracle/_ref/libref_geometry.so.  Test infrastructure only: it pins the oracle's mesh-metric
+// and immersed-boundary geometry against the reference's functions.
+#include "Geometry.h"
+#include "Sphere.h"
+
+namespace {
+void load(const double* p, int n, Point3D* out) {
+    for (int q = 0; q < n; ++q) out[q] = Point3D(p[3 * q], p[3 * q + 1], p[3 * q + 2]);
+}
+}  // namespace
+
+extern "C" {
+double ref_hex_volume(const double* p24) {
+    Point3D p[8];
+    load(p24, 8, p);
+    return Geometry::computeHexahedronVolume(p);
+}
+void ref_hex_centroid(const double* p24, double* out) {
+    Point3D p[8];
+    load(p24, 8, p);
+    Point3D c = Geometry::computeHexahedronCentroid(p);
+    out[0] = c.x; out[1] = c.y; out[2] = c.z;
+}
+double ref_quad_area(const double* p12) {
+    Point3D p[4];
+    load(p12, 4, p);
+    return Geometry::computeQuadrilateralArea(p);
+}
+void ref_quad_centroid(const double* p12, double* out) {
+    Point3D p[4];
+    load(p12, 4, p);
+    Point3D c = Geometry::computeQuadrilateralCentroid(p);
+    out[0] = c.x; out[1] = c.y; out[2] = c.z;
+}
+int ref_inside_hex(const double* pt, const double* p24) {
+    Point3D p[8];
+    load(p24, 8, p);
+    return Geometry::isInsideHexahedron(Point3D(pt[0], pt[1], pt[2]), p) ? 1 : 0;
+}
+void ref_nearest_intersect(double radius, const double* center, const double* pt, double* out) {
+    Sphere s(radius, Point3D(center[0], center[1], center[2]));
+    Point3D r = s.nearestIntersect(Point3D(pt[0], pt[1], pt[2]));
+    out[0] = r.x; out[1] = r.y; out[2] = r.z;
+}
+int ref_sphere_is_inside(double radius, const double* center, const double* pt) {
+    Sphere s(radius, Point3D(center[0], center[1], center[2]));
+    return s.isInside(Point3D(pt[0], pt[1], pt[2])) ? 1 : 0;
+}
+}

@@ -1,0 +1,89 @@
+"""Pins the oracle's geometry against the reference's own code: src/Math/Geometry.cpp,
+Sphere.cpp, Vector3D.cpp and Tensor3D.cpp compiled where they lie (`make -C oracle ref`,
+oracle/_ref/libref_geometry.so).  On seeded jittered and sheared hexahedra, the oracle's
+volume, centroid, face area and centroid, point-in-cell test and sphere intersection must be
+bit-identical to the reference's: both are FP64 with every product and sum rounded separately
+in the same order.  Skipped where the reference sources are absent (the library is not part of
+the repository)."""
+import ctypes
+import os
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_LIB = os.path.join(os.path.dirname(HERE), "oracle", "_ref", "libref_geometry.so")
+
+
+@pytest.fixture(scope="module")
+def libs():
+    from caffe_old_b200 import build as B
+    if not B.build_oracle_ref():
+        pytest.skip("reference geometry sources not present")
+    ref = ctypes.CDLL(REF_LIB)
+    O.lib()                                    # builds the oracle if needed
+    ora = ctypes.CDLL(O._LIB_PATH)             # own handle: the argument types below stay local
+    dp = ctypes.POINTER(ctypes.c_double)
+    for L, pre in ((ref, "ref_"), (ora, "oracle_")):
+        getattr(L, pre + "hex_volume").restype = ctypes.c_double
+        getattr(L, pre + "hex_volume").argtypes = [dp]
+        getattr(L, pre + "hex_centroid").argtypes = [dp, dp]
+        getattr(L, pre + "quad_area").restype = ctypes.c_double
+        getattr(L, pre + "quad_area").argtypes = [dp]
+        getattr(L, pre + "inside_hex").argtypes = [dp, dp]
+        getattr(L, pre + "nearest_intersect").argtypes = [ctypes.c_double, dp, dp, dp]
+    ref.ref_quad_centroid.argtypes = [dp, dp]
+    return ref, ora
+
+
+def _p(a):
+    return np.ascontiguousarray(a, dtype=np.float64).ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _hexes(n, seed):
+    """Unit-ish hexahedra in HexaFvmMesh vertex order, sheared and jittered."""
+    rng = np.random.default_rng(seed)
+    base = np.array([[0, 0, 0], [1, 0, 0], [1, 1, 0], [0, 1, 0], [0, 0, 1], [1, 0, 1], [1, 1, 1], [0, 1, 1]], float)
+    out = []
+    for _ in range(n):
+        h = base * rng.uniform(0.5, 2.0, 3) + rng.uniform(-3, 3, 3)
+        h[:, 0] += np.tan(np.radians(30.0)) * h[:, 2]
+        h += rng.uniform(-0.1, 0.1, h.shape)
+        out.append(h)
+    return out
+
+
+def test_hexahedron_volume_and_centroid_are_the_references(libs):
+    ref, ora = libs
+    for h in _hexes(200, 1):
+        assert ref.ref_hex_volume(_p(h)) == ora.oracle_hex_volume(_p(h))
+        cr, co = np.zeros(3), np.zeros(3)
+        ref.ref_hex_centroid(_p(h), _p(cr))
+        ora.oracle_hex_centroid(_p(h), _p(co))
+        assert np.array_equal(cr, co), (cr, co)
+
+
+def test_face_area_and_centroid_are_the_references(libs):
+    ref, ora = libs
+    for h in _hexes(100, 2):
+        for face in ([1, 2, 6, 5], [0, 4, 7, 3], [3, 7, 6, 2], [0, 1, 5, 4]):
+            q = h[face]
+            assert ref.ref_quad_area(_p(q)) == ora.oracle_quad_area(_p(q))
+
+
+def test_point_in_cell_and_sphere_intersection_are_the_references(libs):
+    ref, ora = libs
+    rng = np.random.default_rng(3)
+    for h in _hexes(60, 4):
+        lo, hi = h.min(0), h.max(0)
+        for _ in range(20):
+            pt = rng.uniform(lo - 0.2, hi + 0.2)
+            assert ref.ref_inside_hex(_p(pt), _p(h)) == ora.oracle_inside_hex(_p(pt), _p(h))
+    for _ in range(200):
+        c, pt, r = rng.uniform(-2, 2, 3), rng.uniform(-3, 3, 3), float(rng.uniform(0.05, 1.0))
+        a, b = np.zeros(3), np.zeros(3)
+        ref.ref_nearest_intersect(r, _p(c), _p(pt), _p(a))
+        ora.oracle_nearest_intersect(r, _p(c), _p(pt), _p(b))
+        assert np.array_equal(a, b), (a, b)
