@@ -87,3 +87,29 @@ def test_point_in_cell_and_sphere_intersection_are_the_references(libs):
         ref.ref_nearest_intersect(r, _p(c), _p(pt), _p(a))
         ora.oracle_nearest_intersect(r, _p(c), _p(pt), _p(b))
         assert np.array_equal(a, b), (a, b)
+
+
+def test_oracle_matches_the_reference_golden_geometry():
+    """The committed outputs of the reference's geometry code (tests/golden/, written by
+    tests/golden/make_geometry_golden.py) against the oracle, bit for bit; needs no reference
+    sources."""
+    g = np.load(os.path.join(HERE, "golden", "reference_geometry.npz"))
+    ora = ctypes.CDLL(O.lib()._name)
+    dp = ctypes.POINTER(ctypes.c_double)
+    ora.oracle_hex_volume.restype = ctypes.c_double
+    ora.oracle_hex_volume.argtypes = [dp]
+    ora.oracle_hex_centroid.argtypes = [dp, dp]
+    ora.oracle_quad_area.restype = ctypes.c_double
+    ora.oracle_quad_area.argtypes = [dp]
+    ora.oracle_nearest_intersect.argtypes = [ctypes.c_double, dp, dp, dp]
+    for q, h in enumerate(g["hexes"]):
+        assert ora.oracle_hex_volume(_p(h)) == g["volume"][q]
+        c = np.zeros(3)
+        ora.oracle_hex_centroid(_p(h), _p(c))
+        assert np.array_equal(c, g["centroid"][q])
+        for f, face in enumerate(g["faces"]):
+            assert ora.oracle_quad_area(_p(h[face])) == g["face_area"][q, f]
+    for q, row in enumerate(g["sphere"]):
+        o = np.zeros(3)
+        ora.oracle_nearest_intersect(float(row[0]), _p(row[1:4]), _p(row[4:7]), _p(o))
+        assert np.array_equal(o, g["nearest"][q])
