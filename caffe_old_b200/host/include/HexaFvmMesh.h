@@ -33,6 +33,7 @@ public:
     void writeTec360(double time, const std::string& directory);
     // the solver whose fields writeTec360 writes (set by the solver's constructor)
     void attachSolver(const Solver* s) const { solver_ = s; }
+    void detachSolver(const Solver* s) const { if (solver_ == s) solver_ = nullptr; }
 
 protected:
     int nI_ = 0, nJ_ = 0, nK_ = 0;

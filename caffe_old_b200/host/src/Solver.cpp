@@ -163,7 +163,7 @@ Solver::Solver(const Input& input, const HexaFvmMesh& mesh, int kind) : mesh_(me
 }
 
 Solver::~Solver() {
-    if (mesh_.nCells() > 0) mesh_.attachSolver(nullptr);
+    mesh_.detachSolver(this);
     if (h_) caffe_dev_destroy(h_);
 }
 
