@@ -1,9 +1,11 @@
-// caffeIbPiso: transient immersed-boundary PISO run of the case in the working directory (case/case.info,
-// case/initialConditions.info, mesh/structuredMesh.dat), written to solution/ every
-// RunControl.fileWriteInterval steps.  Same flow as the reference's Modules/caffeIbPiso.cpp.
+// caffeIbPiso: transient immersed-boundary PISO run of the case in the working directory
+// (case/case.info, case/initialConditions.info, mesh/structuredMesh.dat), written to solution/
+// every RunControl.fileWriteInterval steps; RunControl.writeRestart ON (optional) also writes
+// restart files of u and p at the end.  Same flow as the reference's Modules/caffeIbPiso.cpp.
 #include <iostream>
 #include <memory>
 
+#include "InitialConditions.h"
 #include "Input.h"
 #include "Parallel.h"
 #include "ParallelHexaFvmMesh.h"
@@ -31,6 +33,12 @@ int main(int argc, const char* argv[]) {
         }
         runControl.displayEndMessage();
         mesh->writeTec360(runControl.simTime(), "solution/");
+        // optional: uRestart.rst and pRestart.rst for a later run's restart initial conditions
+        if (input.caseParameters.get<std::string>("RunControl.writeRestart", std::string("OFF")) == "ON") {
+            InitialConditions ics(input);
+            ics.writeRestart(piso, "u");
+            ics.writeRestart(piso, "p");
+        }
     } catch (const char* errorMessage) {
         std::cerr << "Error: " << errorMessage << std::endl;
         rc = 1;
