@@ -4,6 +4,7 @@ import ctypes
 import os
 import re
 
+import numpy as np
 import pytest
 
 from caffe_old_b200 import _lib
@@ -78,3 +79,32 @@ def test_create_without_gpu_fails_loudly(built):
     nodes, spec, _ = C.config2_cavity3d(n=4, steps=1)
     with pytest.raises(_lib.CaffeError):
         Piso(nodes, spec)
+
+
+def test_c_abi_rejects_invalid_arguments_before_any_device_call(built):
+    """caffe_dev_create checks its arguments and the case record before it looks for a GPU,
+    and reports each problem through caffe_last_error (runs the same with or without a GPU)."""
+    L = _lib.lib()
+    nodes, spec, _ = C.config2_cavity3d(n=4, steps=1)
+    nodes = np.ascontiguousarray(nodes, dtype=np.float64)
+    ptr = nodes.ctypes.data_as(ctypes.c_void_p)
+    h = ctypes.c_void_p()
+
+    def create(case, n=(5, 5, 5), p=ptr, out=ctypes.byref(h)):
+        rc = L.caffe_dev_create(p, n[0], n[1], n[2], ctypes.byref(case) if case is not None else None, 0, out)
+        return rc, _lib.last_error()
+
+    good = _lib.make_case(spec)
+    assert create(good, p=None) == (1, "nodes is NULL")
+    assert create(good, out=None) == (1, "out is NULL")
+    assert create(good, n=(1, 5, 5)) == (1, "a mesh needs at least 2 nodes per direction")
+    assert create(None) == (1, "case is NULL")
+    bad = [("kind", 7, "invalid solver kind"), ("omega_p", 0.0, "relaxation factors must be positive"),
+           ("n_pcorr", 0, "numberOfPressureCorrections must be >= 1"), ("maxit", 0, "maxit must be >= 1"),
+           ("mom_method", C.KSP_METHODS["cg_jacobi"], "the momentum matrix is not symmetric: CG cannot solve it"),
+           ("p_form", 9, "invalid pressure-solve form")]
+    for field, value, msg in bad:
+        c = _lib.make_case(spec)
+        setattr(c, field, value)
+        assert create(c) == (1, msg), field
+    assert not h.value
