@@ -126,6 +126,20 @@ class DeviceSolver:
         if n < 0:
             raise CaffeError(f"get {name}: " + last_error())
 
+    # -- restart files (the reference's writeRestart layout; see restart.py)
+    def write_restart(self, name: str, path: str | None = None) -> str:
+        """Writes cell field ``name`` ("u" or "p") to ``path`` (default <name>Restart.rst)."""
+        from .restart import write_restart
+        path = path or f"{name}Restart.rst"
+        write_restart(path, self.field(name).reshape(self.ncells, -1), self.shape)
+        return path
+
+    def read_restart(self, name: str, path: str | None = None) -> None:
+        """Sets cell field ``name`` from a restart file (default <name>Restart.rst)."""
+        from .restart import read_restart
+        comps = self.size_of(name) // self.ncells
+        self.set_field(name, read_restart(path or f"{name}Restart.rst", self.shape, comps))
+
 
 class Simple(DeviceSolver):
     """SIMPLE (src/Solvers/Simple.h:33)."""

@@ -148,3 +148,24 @@ def test_restart_file_with_wrong_size_is_refused(restart_tool, tmp_path):
     assert r.returncode == 1 and "not a number" in r.stderr
     r, _ = _read(restart_tool, tmp_path, "p", 1, "missing.rst")
     assert r.returncode == 1 and "cannot open" in r.stderr
+
+
+def test_python_and_cpp_restart_files_are_interchangeable(restart_tool, tmp_path):
+    """caffe_old_b200.restart writes what the C++ host layer reads and reads what it writes,
+    bit for bit, for a scalar and a vector field."""
+    from caffe_old_b200.restart import read_restart, write_restart
+    for components, field in [(1, "p"), (3, "u")]:
+        planes = _planes(components, seed=20 + components)
+        cells = planes.T if components == 3 else planes[0]
+        write_restart(str(tmp_path / f"py_{field}.rst"), cells, DIMS)
+        r, back = _read(restart_tool, tmp_path, field, components, f"py_{field}.rst")
+        assert r.returncode == 0, r.stderr
+        assert np.array_equal(back.view(np.uint64), planes.view(np.uint64))
+        planes.tofile(tmp_path / "in.raw")
+        r = subprocess.run([restart_tool, "write", "in.raw", f"cpp_{field}.rst", str(components), *map(str, DIMS)], cwd=tmp_path,
+                           capture_output=True, text=True)
+        assert r.returncode == 0, r.stderr
+        got = read_restart(str(tmp_path / f"cpp_{field}.rst"), DIMS, components)
+        assert np.array_equal(np.asarray(got).view(np.uint64), np.ascontiguousarray(cells).view(np.uint64))
+    with pytest.raises(ValueError, match="were expected"):
+        read_restart(str(tmp_path / "py_p.rst"), DIMS, 3)
