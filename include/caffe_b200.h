@@ -98,12 +98,18 @@ int caffe_dev_solve(caffe_dev* h, double dt, caffe_step_stats* stats);
  * "courant", "ib_field", "ib_coeffs".  Names follow Simple.h:44-51 and IbPiso.h:46-47. */
 int caffe_dev_phase(caffe_dev* h, const char* name, double dt);
 
-/* Copy a named array between host and device (dir 0: device -> host, 1: host -> device),
- * synchronously.  Returns the element count of the array in doubles (so a call with
- * host == NULL queries the size), or -1 for an unknown name.  Names: "u", "p", "pCorr",
- * "d", "h", "gradP", "gradPCorr", "massFlow", "massFlowI/J/K", "pPatch0".."pPatch5",
- * metrics "vol", "cc", "SI/SJ/SK", "fcI/fcJ/fcK", "DI/DJ/DK", "momA" (7 x N), "momB" (N x 3),
- * "pcA" (7 x N), "pcB", "status", ...  Vectors are N x 3 interleaved on the host.
+/* Copy a named array between host and device, synchronously.  dir bit 0 gives the
+ * direction (0: device -> host, 1: host -> device); bit 1 selects the host layout of
+ * multi-component arrays (0: N x components interleaved, 2: one plane of N per component).
+ * So dir 0 / 1 read / write interleaved vectors, dir 2 / 3 read / write planes.  Returns the
+ * element count of the array in doubles (so a call with host == NULL queries the size), or
+ * -1 for an unknown name, a host buffer smaller than that count, or a write to a read-only
+ * array.  Names: fields "u", "u0", "p", "pCorr", "d", "gradP", "gradPCorr", "gradU" (9
+ * components; non-orthogonal correction only), "massFlow" (cell mass imbalance),
+ * "massFlowI/J/K" (face fluxes), "pPatch0".."pPatch5"; systems "momA" (N x 7, read-only),
+ * "momB" (N x 3), "pcA" (N x 7, read-only), "pcB"; read-only metrics "vol", "cc",
+ * "SI/SJ/SK", "fcI/fcJ/fcK", "DI/DJ/DK", "cvI/cvJ/cvK"; immersed boundary (read-only)
+ * "status", "ibCell", "ibCol", "ibValMom", "ibValP".
  * Field access of the reference: Field.h:53-61, HexaFvmMesh.h:66-142. */
 long caffe_dev_array(caffe_dev* h, const char* name, double* host, long count, int dir);
 
