@@ -1,7 +1,8 @@
 // Learned preconditioner in a flexible Krylov solve, and its training on the device.
 //
 // Preconditioner (additive multilevel with a learned level operator):
-//   M(r) = D^-1 r + P_1 w_1,   w_l = gain_l s y_l + P_(l+1) w_(l+1),   y_l = net(u_l / s, mask_l, l),
+//   M(r) = D^-1 r + P_1 w_1,   w_l = gain_l s y_l + P_(l+1) w_(l+1),
+//   y_l = (net(u_l / s, mask_l, l) - net(-u_l / s, mask_l, l)) / 2,
 //   u_1 = R_1 (D^-1 r),  u_(l+1) = R_(l+1) u_l,
 // on active cells (D^-1 r on ghost rows, 0 on inactive cells).  Level l halves every
 // direction of level l-1 that is longer than one cell; P is cell-centred trilinear
@@ -12,9 +13,14 @@
 // residual, the fraction of active cells and a constant level channel.  The network never
 // runs on the cell lattice itself: on the 25M-cell lattice level 1 holds 1/8 of the cells, so
 // the network costs a fraction of one fine-lattice sweep while the pyramid reaches the
-// smooth error that a 9^3 receptive field cannot.  Two reference forms use the same code:
-// JACOBI (no levels: M = D^-1, the method without the network) and LEVELS (y_l = u_l / s,
-// the pyramid with an identity in place of the network).
+// smooth error that a 9^3 receptive field cannot.  The network term is odd in the residual
+// (the second evaluation negates only the residual channel): a network with biases and
+// constant input channels has a part that does not depend on the residual, which would add
+// the same vector to every preconditioned direction; the odd form gives M(0) = 0 and
+// M(-r) = -M(r) exactly.  Levels finer than the first network level (netFrom) use the
+// identity.  Two reference forms use the same code: JACOBI (no levels: M = D^-1, the method
+// without the network) and LEVELS (y_l = u_l / s, the pyramid with an identity in place of
+// the network).
 //
 // Solve (learned + mixed precision): FP64 iterative refinement (true residual, update and
 // convergence test in FP64) around an FP32 flexible Krylov solve that tolerates a
@@ -23,7 +29,12 @@
 //      p_k = z_k - beta_k p_{k-1},  beta_k = (z_k, q_{k-1}) / (p_{k-1}, q_{k-1}),
 //      q_k = A p_k,  alpha_k = (p_k, r_k) / (p_k, q_k),  x += alpha p,  r -= alpha q;
 //  * right-preconditioned BiCGStab when immersed-boundary ghost rows make the matrix
-//    non-symmetric (x and r stay consistent for any M).
+//    non-symmetric and M is the fixed linear pyramid (BiCGStab needs a fixed linear
+//    preconditioner);
+//  * FGMRES(m) with re-orthogonalised classical Gram-Schmidt (CGS2) when the matrix is
+//    non-symmetric and the network runs: one restart cycle per FP64 refinement pass.
+// The refinement stops with status 2 (the plain FP64 solve then takes over) after three
+// passes in a row that each leave more than 90% of the true residual.
 // Each iteration is a short fixed sequence of kernels; their dot products go through block
 // partials and a one-block finaliser into a device-side scalar record, so the host never
 // waits inside an iteration.  Once the record's `done` flag is set every later kernel returns

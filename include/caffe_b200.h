@@ -138,8 +138,9 @@ int caffe_ksp7_solve_device(int nI, int nJ, int nK, const double* d_coef7, const
 /* Learned preconditioner network (an extension; the reference has no learned component):
  * a 4-layer 3-D convolutional network with 3x3x3 kernels and 16 channels, BF16 weights and
  * activations, FP32 accumulation on the tensor cores.  Parameters are FP32, layer by layer:
- * W[27 taps][16 out][16 in] then b[16]; tap = 9*(dk+1) + 3*(dj+1) + (di+1).  Layer 1 reads
- * input channels 0 and 1, layer 4 writes output channel 0. */
+ * W[27 taps][16 out][16 in] then b[16]; tap = 9*(dk+1) + 3*(dj+1) + (di+1).  Layer 4 writes
+ * output channel 0.  The host-data entry points below feed input channels 0 and 1; inside the
+ * p' solve a third channel carries the pyramid level. */
 int caffe_precond_param_count(void);
 /* Apply the network to a 2-channel input x2 (host, nI*nJ*nK x 2 floats); y receives the
  * output channel (host, nI*nJ*nK floats). */
@@ -150,8 +151,10 @@ int caffe_precond_net_grad(int nI, int nJ, int nK, const float* params, const fl
 
 /* Learned preconditioner of the p' solve (p_form CAFFE_P_LEARNED or CAFFE_P_LEARNED_MIXED):
  * an FP32 flexible Krylov solve inside FP64 refinement, preconditioned by
- *     M(r) = D^-1 r + sum_l P_l (4^l s y_l),   y_l = net(R_l D^-1 r / s)
- * on a pyramid of coarsened lattices (l >= 1), with one network (above) serving every level.
+ *     M(r) = D^-1 r + sum_l P_l (4^l s y_l),   y_l = (net(x_l) - net(-x_l)) / 2,
+ *     x_l = (R_l D^-1 r / s, active fraction, level / 8)  (the sign flips the first channel only)
+ * on a pyramid of coarsened lattices (l >= 1), with one network (above) serving every level;
+ * s is the RMS of D^-1 r over the active cells.
  * No counterpart in the reference: the reference solves p' with its Krylov library only
  * (src/Math/SparseMatrix.cpp:95-100).  Every solve still reaches p_rtol in the FP64 true
  * residual; the plain FP64 solve re-runs on the device when the learned one does not.
