@@ -112,3 +112,29 @@ def test_cavity_mass_conservation_and_symmetry():
     assert np.all(u[:, :, 2] == 0.0)           # 2-D: no z velocity
     assert u[-1, :, 0].mean() > 0.2            # lid drags the top row
     assert u[4, :, 0].mean() < 0.0             # return flow below
+
+
+def test_sphere_crossing_the_boundary():
+    """Edge case of IbPiso::computeIbField (IbPiso.cpp:65-117): a neighbour outside the domain
+    is read from the ib field's boundary patch, which stays 0 = FLUID, so every solid cell on
+    the boundary is a ghost cell even when all its in-domain neighbours are solid.  Image
+    points that fall between the boundary and the first cell centres have no enclosing cells:
+    the reference raises there (HexaFvmMesh::locateEnclosingCells, HexaFvmMesh.cpp:378-418),
+    and so does the oracle (the device library refuses such a case at creation)."""
+    from helpers import small_channel_sphere
+    nodes, spec = small_channel_sphere()
+    o = O.OracleSolver(nodes, spec.replace(ib_center=(0.0, 0.5, 0.5), ib_radius=0.4))
+    o.phase("ib_field")
+    st = o.get("status").reshape(12, 12, 32)
+    solid = st != 0
+    assert solid[:, :, 0].any()
+    assert np.all(st[:, :, 0][solid[:, :, 0]] == 1)
+    # some of them have only solid neighbours inside the domain
+    inner = solid[1:-1, 1:-1, 0] & solid[1:-1, 1:-1, 1] & solid[2:, 1:-1, 0] & solid[:-2, 1:-1, 0] \
+        & solid[1:-1, 2:, 0] & solid[1:-1, :-2, 0]
+    assert inner.any()
+    # away from the boundary the ordinary rule holds: solid cells with only solid neighbours are inactive
+    assert (st[:, :, 1:] == 2).any()
+    with pytest.raises(RuntimeError, match="outside the cell-centre lattice"):
+        o.phase("ib_coeffs")
+    o.close()
