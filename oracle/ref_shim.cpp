@@ -1,7 +1,9 @@
 // C entry points over the reference's own geometry code (src/Math/Geometry.cpp, Sphere.cpp,
-// Vector3D.cpp, Tensor3D.cpp), compiled where it lies by `make -C oracle ref` into
-// oracle/_ref/libref_geometry.so.  Test infrastructure only: it pins the oracle's mesh-metric
-// and immersed-boundary geometry against the reference's functions.
+// Vector3D.cpp, Tensor3D.cpp) and its Array3D container (src/DataStructures/Array3D.h/.tpp),
+// compiled where they lie by `make -C oracle ref` into oracle/_ref/libref_geometry.so.  Test
+// infrastructure only: it pins the oracle's mesh-metric and immersed-boundary geometry, and
+// its cell storage order, against the reference's code.
+#include "Array3D.h"
 #include "Geometry.h"
 #include "Sphere.h"
 
@@ -43,6 +45,16 @@ void ref_nearest_intersect(double radius, const double* center, const double* pt
     Sphere s(radius, Point3D(center[0], center[1], center[2]));
     Point3D r = s.nearestIntersect(Point3D(pt[0], pt[1], pt[2]));
     out[0] = r.x; out[1] = r.y; out[2] = r.z;
+}
+// offset of element (i, j, k) in an Array3D of sizeI x sizeJ x sizeK, or -1 where the
+// reference's bounds-checked operator() throws
+long ref_array3d_offset(int sizeI, int sizeJ, int sizeK, int i, int j, int k) {
+    Array3D<double> a(sizeI, sizeJ, sizeK);
+    try {
+        return (long)(&a(i, j, k) - a.data());
+    } catch (const char*) {
+        return -1;
+    }
 }
 int ref_sphere_is_inside(double radius, const double* center, const double* pt) {
     Sphere s(radius, Point3D(center[0], center[1], center[2]));

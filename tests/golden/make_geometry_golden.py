@@ -1,7 +1,8 @@
 """Writes tests/golden/reference_geometry.npz: outputs of the reference's own geometry code
 (src/Math/Geometry.cpp and Sphere.cpp, compiled where they lie into
 oracle/_ref/libref_geometry.so by `make -C oracle ref`) on seeded sheared and jittered
-hexahedra, so that the oracle stays pinned to them where the reference sources are absent.
+hexahedra, and its Array3D container's element offsets, so that the oracle stays pinned to
+them where the reference sources are absent.
 
   python tests/golden/make_geometry_golden.py
 """
@@ -58,8 +59,13 @@ def main():
         o = np.zeros(3)
         ref.ref_nearest_intersect(float(row[0]), p(row[1:4]), p(row[4:7]), p(o))
         near[q] = o
+    ref.ref_array3d_offset.restype = ctypes.c_long
+    ref.ref_array3d_offset.argtypes = [ctypes.c_int] * 6
+    dims = (7, 5, 3)
+    cells = np.array([(i, j, k) for k in range(dims[2]) for j in range(dims[1]) for i in range(dims[0])])
+    offs = np.array([ref.ref_array3d_offset(*dims, *map(int, c)) for c in cells])
     np.savez(os.path.join(HERE, "reference_geometry.npz"), hexes=H, volume=vol, centroid=cen, faces=faces, face_area=area,
-             sphere=sph, nearest=near)
+             sphere=sph, nearest=near, array3d_dims=np.array(dims), array3d_cells=cells, array3d_offsets=offs)
     print("wrote", os.path.join(HERE, "reference_geometry.npz"))
 
 

@@ -3,8 +3,9 @@ Sphere.cpp, Vector3D.cpp and Tensor3D.cpp compiled where they lie (`make -C orac
 oracle/_ref/libref_geometry.so).  On seeded jittered and sheared hexahedra, the oracle's
 volume, centroid, face area and centroid, point-in-cell test and sphere intersection must be
 bit-identical to the reference's: both are FP64 with every product and sum rounded separately
-in the same order.  Skipped where the reference sources are absent (the library is not part of
-the repository)."""
+in the same order.  The same library holds the reference's Array3D container, which pins the
+oracle's cell storage order.  Skipped where the reference sources are absent (the library is
+not part of the repository); the committed golden fixture covers that case."""
 import ctypes
 import os
 
@@ -89,6 +90,38 @@ def test_point_in_cell_and_sphere_intersection_are_the_references(libs):
         assert np.array_equal(a, b), (a, b)
 
 
+def _ref_offsets(ref, dims, cells):
+    ref.ref_array3d_offset.restype = ctypes.c_long
+    ref.ref_array3d_offset.argtypes = [ctypes.c_int] * 6
+    return np.array([ref.ref_array3d_offset(*dims, *c) for c in cells])
+
+
+def _oracle_cell_index(dims):
+    """Where the oracle stores each cell (i, j, k) of a Cartesian mesh: the index of the
+    centroid it reports for that cell."""
+    from caffe_old_b200 import cases as C
+    nI, nJ, nK = dims
+    s = O.OracleSolver(C.cartesian_nodes(dims, (nI, nJ, nK)), C.CaseSpec(kind="simple"))
+    cc = s.get("cc").reshape(-1, 3)
+    s.close()
+    ijk = np.floor(cc).astype(int)                     # unit cells: centroid (i+.5, j+.5, k+.5)
+    index = np.empty((nI, nJ, nK), dtype=int)
+    index[ijk[:, 0], ijk[:, 1], ijk[:, 2]] = np.arange(len(cc))
+    return index
+
+
+def test_cell_storage_order_is_the_references_array3d(libs):
+    """The oracle stores cell (i, j, k) at the element the reference's Array3D gives it
+    (Array3D.tpp:41-59, i fastest), and the reference's bounds-checked access refuses indices
+    outside the array."""
+    ref, _ = libs
+    dims = (7, 5, 3)
+    index = _oracle_cell_index(dims)
+    cells = [(i, j, k) for k in range(dims[2]) for j in range(dims[1]) for i in range(dims[0])]
+    assert np.array_equal(_ref_offsets(ref, dims, cells), [index[c] for c in cells])
+    assert list(_ref_offsets(ref, dims, [(-1, 0, 0), (0, 5, 0), (0, 0, 3), (7, 4, 2)])) == [-1, -1, -1, -1]
+
+
 def test_oracle_matches_the_reference_golden_geometry():
     """The committed outputs of the reference's geometry code (tests/golden/, written by
     tests/golden/make_geometry_golden.py) against the oracle, bit for bit; needs no reference
@@ -113,3 +146,7 @@ def test_oracle_matches_the_reference_golden_geometry():
         o = np.zeros(3)
         ora.oracle_nearest_intersect(float(row[0]), _p(row[1:4]), _p(row[4:7]), _p(o))
         assert np.array_equal(o, g["nearest"][q])
+    # cell storage order: the reference Array3D's offsets of every cell of a 7 x 5 x 3 array
+    dims = tuple(int(v) for v in g["array3d_dims"])
+    index = _oracle_cell_index(dims)
+    assert np.array_equal(g["array3d_offsets"], [index[tuple(c)] for c in g["array3d_cells"]])
