@@ -46,6 +46,23 @@ void ref_nearest_intersect(double radius, const double* center, const double* pt
     Point3D r = s.nearestIntersect(Point3D(pt[0], pt[1], pt[2]));
     out[0] = r.x; out[1] = r.y; out[2] = r.z;
 }
+// face vector (unit normal times area) of a quadrilateral, as the mesh set-up composes it
+// from the reference's Vector3D and Geometry routines (HexaFvmMesh.cpp:722-727)
+void ref_face_vector(const double* p12, double* out) {
+    Point3D p[4];
+    load(p12, 4, p);
+    Vector3D n = cross(p[1] - p[0], p[2] - p[0]).unitVector() * Geometry::computeQuadrilateralArea(p);
+    out[0] = n.x; out[1] = n.y; out[2] = n.z;
+}
+// diffusion metric D_f = |S|^2 / (S . r) and non-orthogonal vector c_f = S - r |S|^2 / (S . r)
+// of one cell face, in the reference's Vector3D arithmetic (HexaFvmMesh.cpp:872-884): out =
+// (D, c.x, c.y, c.z)
+void ref_d_and_c(const double* s3, const double* r3, double* out) {
+    Vector3D s(s3[0], s3[1], s3[2]), r(r3[0], r3[1], r3[2]);
+    double d = dot(s, s) / dot(s, r);
+    Vector3D c = s - r * dot(s, s) / dot(s, r);
+    out[0] = d; out[1] = c.x; out[2] = c.y; out[3] = c.z;
+}
 // offset of element (i, j, k) in an Array3D of sizeI x sizeJ x sizeK, or -1 where the
 // reference's bounds-checked operator() throws
 long ref_array3d_offset(int sizeI, int sizeJ, int sizeK, int i, int j, int k) {

@@ -150,3 +150,101 @@ def test_oracle_matches_the_reference_golden_geometry():
     dims = tuple(int(v) for v in g["array3d_dims"])
     index = _oracle_cell_index(dims)
     assert np.array_equal(g["array3d_offsets"], [index[tuple(c)] for c in g["array3d_cells"]])
+    # metric arrays of the sheared, jittered mesh
+    from caffe_old_b200 import cases as C
+    s = O.OracleSolver(g["mesh_nodes"], C.CaseSpec(kind="piso"))
+    assert np.array_equal(s.get("vol"), g["mesh_vol"])
+    assert np.array_equal(s.get("cc").reshape(-1, 3), g["mesh_cc"])
+    for d in "IJK":
+        assert np.array_equal(s.get("fc" + d).reshape(-1, 3), g["mesh_fc" + d]), d
+        assert np.array_equal(s.get("S" + d).reshape(-1, 3), g["mesh_S" + d]), d
+    dc = g["mesh_d_and_c"].reshape(6, -1, 4)
+    for f in range(6):
+        assert np.array_equal(s.get(f"dmet{f}"), dc[f, :, 0]), f
+        assert np.array_equal(s.get(f"cvec{f}").reshape(-1, 3), dc[f, :, 1:]), f
+    s.close()
+
+
+def test_mesh_metric_arrays_are_the_references(libs):
+    """The oracle's metric arrays of a sheared, jittered mesh -- cell volumes and centroids
+    (HexaFvmMesh::initializeCells, HexaFvmMesh.cpp:626-655) and face centroids and face vectors
+    (initializeFaces, :699-789) -- equal, bit for bit, the reference's Geometry and Vector3D
+    routines applied to the same nodes in the mesh set-up's vertex orders."""
+    from caffe_old_b200 import cases as C
+    ref, _ = libs
+    dp = ctypes.POINTER(ctypes.c_double)
+    ref.ref_face_vector.argtypes = [dp, dp]
+    nI, nJ, nK = 6, 5, 4
+    nodes = C.skewed_nodes((nI, nJ, nK), (1.0, 1.0, 1.0), 30.0, 0.1, 5)     # (k, j, i, xyz)
+    s = O.OracleSolver(nodes, C.CaseSpec(kind="piso"))
+    vol, cc = s.get("vol"), s.get("cc").reshape(-1, 3)
+    fc = {d: s.get("fc" + d).reshape(-1, 3) for d in "IJK"}
+    sv = {d: s.get("S" + d).reshape(-1, 3) for d in "IJK"}
+    s.close()
+    X = lambda i, j, k: nodes[k, j, i]
+    for k in range(nK):
+        for j in range(nJ):
+            for i in range(nI):
+                h = np.array([X(i, j, k), X(i + 1, j, k), X(i + 1, j + 1, k), X(i, j + 1, k),
+                              X(i, j, k + 1), X(i + 1, j, k + 1), X(i + 1, j + 1, k + 1), X(i, j + 1, k + 1)])
+                c = (k * nJ + j) * nI + i
+                assert ref.ref_hex_volume(_p(h)) == vol[c]
+                o = np.zeros(3)
+                ref.ref_hex_centroid(_p(h), _p(o))
+                assert np.array_equal(o, cc[c])
+    quads = {   # face arrays: I (nI+1) x nJ x nK, J nI x (nJ+1) x nK, K nI x nJ x (nK+1), i fastest
+        "I": (nI + 1, nJ, nK, lambda i, j, k: [X(i, j, k), X(i, j + 1, k), X(i, j + 1, k + 1), X(i, j, k + 1)]),
+        "J": (nI, nJ + 1, nK, lambda i, j, k: [X(i, j, k), X(i, j, k + 1), X(i + 1, j, k + 1), X(i + 1, j, k)]),
+        "K": (nI, nJ, nK + 1, lambda i, j, k: [X(i, j, k), X(i + 1, j, k), X(i + 1, j + 1, k), X(i, j + 1, k)]),
+    }
+    for d, (fI, fJ, fK, quad) in quads.items():
+        for k in range(fK):
+            for j in range(fJ):
+                for i in range(fI):
+                    q = np.array(quad(i, j, k))
+                    f = (k * fJ + j) * fI + i
+                    o = np.zeros(3)
+                    ref.ref_quad_centroid(_p(q), _p(o))
+                    assert np.array_equal(o, fc[d][f]), (d, i, j, k)
+                    ref.ref_face_vector(_p(q), _p(o))
+                    assert np.array_equal(o, sv[d][f]), (d, i, j, k)
+
+
+def test_diffusion_metrics_are_the_references(libs):
+    """D_f = |S|^2 / (S . r) and c_f = S - r |S|^2 / (S . r) of every face of every cell
+    (HexaFvmMesh::computeMeshMetrics, HexaFvmMesh.cpp:872-884): the oracle's values equal the
+    reference's Vector3D arithmetic on the same face vector S (outward: fAreaNorm*,
+    HexaFvmMesh.h:79-84) and cell-to-cell vector r (cell-to-face on the boundary: rCell*,
+    HexaFvmMesh.cpp:218-294), bit for bit, on a sheared, jittered mesh."""
+    from caffe_old_b200 import cases as C
+    ref, _ = libs
+    dp = ctypes.POINTER(ctypes.c_double)
+    ref.ref_d_and_c.argtypes = [dp, dp, dp]
+    nI, nJ, nK = 6, 5, 4
+    nodes = C.skewed_nodes((nI, nJ, nK), (1.0, 1.0, 1.0), 30.0, 0.1, 5)
+    s = O.OracleSolver(nodes, C.CaseSpec(kind="piso"))
+    cc = s.get("cc").reshape(nK, nJ, nI, 3)
+    fcI, fcJ, fcK = (s.get("fc" + d).reshape(*shp, 3) for d, shp in
+                     (("I", (nK, nJ, nI + 1)), ("J", (nK, nJ + 1, nI)), ("K", (nK + 1, nJ, nI))))
+    SI, SJ, SK = (s.get("S" + d).reshape(*shp, 3) for d, shp in
+                  (("I", (nK, nJ, nI + 1)), ("J", (nK, nJ + 1, nI)), ("K", (nK + 1, nJ, nI))))
+    dmet = [s.get(f"dmet{f}").reshape(nK, nJ, nI) for f in range(6)]
+    cvec = [s.get(f"cvec{f}").reshape(nK, nJ, nI, 3) for f in range(6)]
+    s.close()
+    for k in range(nK):
+        for j in range(nJ):
+            for i in range(nI):
+                c = cc[k, j, i]
+                faces = [  # (S outward, r) for east, west, north, south, top, bottom
+                    (SI[k, j, i + 1], cc[k, j, i + 1] - c if i < nI - 1 else fcI[k, j, i + 1] - c),
+                    (-SI[k, j, i], cc[k, j, i - 1] - c if i > 0 else fcI[k, j, i] - c),
+                    (SJ[k, j + 1, i], cc[k, j + 1, i] - c if j < nJ - 1 else fcJ[k, j + 1, i] - c),
+                    (-SJ[k, j, i], cc[k, j - 1, i] - c if j > 0 else fcJ[k, j, i] - c),
+                    (SK[k + 1, j, i], cc[k + 1, j, i] - c if k < nK - 1 else fcK[k + 1, j, i] - c),
+                    (-SK[k, j, i], cc[k - 1, j, i] - c if k > 0 else fcK[k, j, i] - c),
+                ]
+                for f, (sv, r) in enumerate(faces):
+                    out = np.zeros(4)
+                    ref.ref_d_and_c(_p(sv), _p(r), _p(out))
+                    assert out[0] == dmet[f][k, j, i], (f, i, j, k)
+                    assert np.array_equal(out[1:], cvec[f][k, j, i]), (f, i, j, k)
