@@ -73,6 +73,15 @@ long ref_array3d_offset(int sizeI, int sizeJ, int sizeK, int i, int j, int k) {
         return -1;
     }
 }
+// image point of a ghost-cell centre x: 2 BP - x with BP the sphere's nearest intersection,
+// in the reference's Vector3D arithmetic (IbPiso.cpp:137-138)
+void ref_image_point(double radius, const double* center, const double* x, double* out) {
+    Sphere s(radius, Point3D(center[0], center[1], center[2]));
+    Point3D xg(x[0], x[1], x[2]);
+    Point3D bp = s.nearestIntersect(xg);
+    Point3D ip = 2. * bp - xg;
+    out[0] = ip.x; out[1] = ip.y; out[2] = ip.z;
+}
 int ref_sphere_is_inside(double radius, const double* center, const double* pt) {
     Sphere s(radius, Point3D(center[0], center[1], center[2]));
     return s.isInside(Point3D(pt[0], pt[1], pt[2])) ? 1 : 0;

@@ -3,8 +3,9 @@
 oracle/_ref/libref_geometry.so by `make -C oracle ref`) on seeded sheared and jittered
 hexahedra, its Array3D container's element offsets, and the metric arrays (cell volumes and
 centroids, face centroids and face vectors, D_f and c_f) of a sheared, jittered mesh built
-from those routines, so that the oracle stays pinned to them where the reference sources are
-absent.
+from those routines, and the immersed-boundary geometry of the channel with a sphere (solid
+cells, ghost cells and their 8-cell stencils), so that the oracle stays pinned to them where
+the reference sources are absent.
 
   python tests/golden/make_geometry_golden.py
 """
@@ -29,6 +30,76 @@ def hexes(n, seed):
         h += rng.uniform(-0.1, 0.1, h.shape)
         out.append(h)
     return np.array(out)
+
+
+def ib_reference(ref, nodes, radius, center):
+    """Solid cells and ghost-cell stencils of one sphere on these nodes, from the reference's
+    own routines: cell centroids (Geometry::computeHexahedronCentroid), Sphere::isInside, the
+    image point 2 BP - x_G (Sphere::nearestIntersect, Vector3D arithmetic) and the search of
+    HexaFvmMesh::locateCell / locateEnclosingCells (HexaFvmMesh.cpp:345-418: the first node
+    hexahedron in k-j-i order that contains the point, then the first cell-centre hexahedron of
+    the 2 x 2 x 2 window below it, both by Geometry::isInsideHexahedron).  Ghost cells are solid
+    cells with a fluid 6-neighbour, a neighbour outside the domain counting as fluid
+    (IbPiso.cpp:65-117).  Returns (solid[k, j, i], ghost cell ids, stencils[ghost][8])."""
+    dp = ctypes.POINTER(ctypes.c_double)
+    p = lambda a: np.ascontiguousarray(a, dtype=np.float64).ctypes.data_as(dp)
+    ref.ref_hex_centroid.argtypes = [dp, dp]
+    ref.ref_sphere_is_inside.argtypes = [ctypes.c_double, dp, dp]
+    ref.ref_image_point.argtypes = [ctypes.c_double, dp, dp, dp]
+    ref.ref_inside_hex.argtypes = [dp, dp]
+    nK, nJ, nI = (d - 1 for d in nodes.shape[:3])
+    X = lambda i, j, k: nodes[k, j, i]
+
+    def hex_of(pt_of, i, j, k):
+        return np.array([pt_of(i, j, k), pt_of(i + 1, j, k), pt_of(i + 1, j + 1, k), pt_of(i, j + 1, k),
+                         pt_of(i, j, k + 1), pt_of(i + 1, j, k + 1), pt_of(i + 1, j + 1, k + 1), pt_of(i, j + 1, k + 1)])
+
+    cc = np.zeros((nK, nJ, nI, 3))
+    for k in range(nK):
+        for j in range(nJ):
+            for i in range(nI):
+                ref.ref_hex_centroid(p(hex_of(X, i, j, k)), p(cc[k, j, i]))
+    ctr = np.asarray(center, dtype=np.float64)
+    solid = np.array([[[bool(ref.ref_sphere_is_inside(radius, p(ctr), p(cc[k, j, i]))) for i in range(nI)] for j in range(nJ)]
+                      for k in range(nK)])
+    S = lambda i, j, k: 0 <= i < nI and 0 <= j < nJ and 0 <= k < nK and solid[k, j, i]
+    C = lambda i, j, k: cc[k, j, i]
+    ghosts, stencils = [], []
+    for k in range(nK):
+        for j in range(nJ):
+            for i in range(nI):
+                if not solid[k, j, i] or all(S(*n) for n in ((i + 1, j, k), (i - 1, j, k), (i, j + 1, k), (i, j - 1, k),
+                                                             (i, j, k + 1), (i, j, k - 1))):
+                    continue
+                ip = np.zeros(3)
+                ref.ref_image_point(radius, p(ctr), p(cc[k, j, i]), p(ip))
+                cell = next((a, b, c) for c in range(nK) for b in range(nJ) for a in range(nI)
+                            if ref.ref_inside_hex(p(ip), p(hex_of(X, a, b, c))))
+                found = None
+                for c in (cell[2] - 1, cell[2]):
+                    for b in (cell[1] - 1, cell[1]):
+                        for a in (cell[0] - 1, cell[0]):
+                            if found is not None:
+                                continue
+                            # the reference's bounds-checked Array3D throws beyond the cell-centre lattice
+                            if not (0 <= a < nI - 1 and 0 <= b < nJ - 1 and 0 <= c < nK - 1):
+                                raise ValueError("image point outside the cell-centre lattice")
+                            if ref.ref_inside_hex(p(ip), p(hex_of(C, a, b, c))):
+                                found = (a, b, c)
+                a, b, c = found
+                ghosts.append((k * nJ + j) * nI + i)
+                stencils.append([((c + dk) * nJ + (b + dj)) * nI + (a + di) for di, dj, dk in
+                                 ((0, 0, 0), (1, 0, 0), (1, 1, 0), (0, 1, 0), (0, 0, 1), (1, 0, 1), (1, 1, 1), (0, 1, 1))])
+    return solid, np.array(ghosts, dtype=np.int64), np.array(stencils, dtype=np.int64)
+
+
+def ib_case():
+    """Nodes and sphere of the immersed-boundary fixture: the 32 x 12 x 12 channel of the
+    parity tests."""
+    sys.path.insert(0, os.path.dirname(HERE))
+    from helpers import small_channel_sphere
+    nodes, spec = small_channel_sphere()
+    return nodes, float(spec.ib_radius), np.array(spec.ib_center, dtype=float)
 
 
 def main():
@@ -122,8 +193,11 @@ def main():
                     ref.ref_d_and_c(p(np.ascontiguousarray(sv)), p(np.ascontiguousarray(r)), p(out))
                     dc[f, k, j, i] = out
     mesh["mesh_d_and_c"] = dc
+    ib_nodes, ib_r, ib_c = ib_case()
+    solid, ghosts, stencils = ib_reference(ref, ib_nodes, ib_r, ib_c)
+    ib = {"ib_solid": solid, "ib_ghosts": ghosts, "ib_stencils": stencils}
     np.savez(os.path.join(HERE, "reference_geometry.npz"), hexes=H, volume=vol, centroid=cen, faces=faces, face_area=area,
-             sphere=sph, nearest=near, array3d_dims=np.array(dims), array3d_cells=cells, array3d_offsets=offs, **mesh)
+             sphere=sph, nearest=near, array3d_dims=np.array(dims), array3d_cells=cells, array3d_offsets=offs, **mesh, **ib)
     print("wrote", os.path.join(HERE, "reference_geometry.npz"))
 
 

@@ -163,6 +163,12 @@ def test_oracle_matches_the_reference_golden_geometry():
         assert np.array_equal(s.get(f"dmet{f}"), dc[f, :, 0]), f
         assert np.array_equal(s.get(f"cvec{f}").reshape(-1, 3), dc[f, :, 1:]), f
     s.close()
+    # immersed-boundary geometry of the channel with a sphere
+    nodes, radius, center = _geometry_generator().ib_case()
+    status, stencil = _oracle_ib(nodes, radius, center)
+    assert np.array_equal(g["ib_solid"].ravel(), status != 0)
+    assert np.array_equal(g["ib_ghosts"], np.flatnonzero(status == 1))
+    assert np.array_equal(g["ib_stencils"], stencil)
 
 
 def test_mesh_metric_arrays_are_the_references(libs):
@@ -248,3 +254,40 @@ def test_diffusion_metrics_are_the_references(libs):
                     ref.ref_d_and_c(_p(sv), _p(r), _p(out))
                     assert out[0] == dmet[f][k, j, i], (f, i, j, k)
                     assert np.array_equal(out[1:], cvec[f][k, j, i]), (f, i, j, k)
+
+
+def _geometry_generator():
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("make_geometry_golden", os.path.join(HERE, "golden", "make_geometry_golden.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def _oracle_ib(nodes, radius, center):
+    from caffe_old_b200 import cases as C
+    bc, refv = C.channel_bcs(1.0)
+    spec = C.CaseSpec(kind="ibpiso", bc=bc, ref_vec=refv, ib_radius=radius, ib_center=tuple(center))
+    o = O.OracleSolver(nodes, spec)
+    o.phase("ib_field")
+    o.phase("ib_coeffs")
+    status = o.get("status")
+    stencil = o.get("ibStencil").reshape(-1, 8).astype(np.int64)
+    o.close()
+    return status, stencil
+
+
+def test_immersed_boundary_geometry_is_the_references(libs):
+    """Ghost-cell geometry of IbPiso (IbPiso.cpp:65-140) on the channel with a sphere: the
+    oracle's solid cells are the cells whose centroid the reference's Sphere::isInside accepts,
+    and each ghost cell's 8-cell interpolation stencil is the one the reference's cell search
+    finds for the image point 2 BP - x_G computed by its own Vector3D arithmetic
+    (tests/golden/make_geometry_golden.py: ib_reference)."""
+    ref, _ = libs
+    gen = _geometry_generator()
+    nodes, radius, center = gen.ib_case()
+    solid, ghosts, stencils = gen.ib_reference(ref, nodes, radius, center)
+    status, stencil = _oracle_ib(nodes, radius, center)
+    assert np.array_equal(solid.ravel(), status != 0)
+    assert np.array_equal(np.flatnonzero(status == 1), ghosts) and len(ghosts) > 0
+    assert np.array_equal(stencil, stencils)
