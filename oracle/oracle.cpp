@@ -23,6 +23,17 @@
 //   * CG, Hestenes-Stiefel, Jacobi-preconditioned, tested on the true residual.
 // Reductions are summed in fixed 2048-row chunks and then in chunk order, so the
 // result does not depend on the OpenMP thread count.
+//
+// Pinning.  The geometry (hexahedron volume and centroid, face area, centroid and
+// vector, point-in-cell test, sphere intersection), the mesh metric arrays (D_f,
+// c_f), the cell storage order and the immersed-boundary geometry (solid cells,
+// ghost cells, image-point stencils) are pinned bit for bit against the reference's
+// own Geometry / Sphere / Vector3D / Tensor3D / Array3D code, compiled where it lies
+// (tests/test_oracle_pinned_reference.py; tests/golden/reference_geometry.npz keeps
+// the reference's outputs).  The rest -- the flow phases, the trilinear weights and
+// the Krylov solves -- is parity unpinned: the reference needs MPI, PETSc, Boost and
+// LAPACKE to build, none of which is present, so it follows the reference's source
+// line by line and is checked by the known-answer tests only.
 
 #include <cmath>
 #include <cstdint>
