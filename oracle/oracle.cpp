@@ -766,6 +766,119 @@ static KspStats kspSolve(int method, const Rows& A, const std::vector<double>& b
 }
 
 // ----------------------------------------------------------------------------
+// Diffusion (src/Solvers/Diffusion.cpp): scalar diffusion with unit diffusivity on one
+// block, one linear solve per call.  The reference's coefficients are kept as written
+// (Diffusion.cpp:73-85): a_nb = +D_f, a_P = -sum D_f + V/dt, b = (V/dt) phi0.  For a steady
+// case (a0P = 0) this is the Laplace equation; for an unsteady one it reads
+// (V/dt)(phi_P - phi0) = sum D_f (phi_P - phi_nb), the sign of the diffusion term opposite
+// to the heat equation's.
+// ----------------------------------------------------------------------------
+struct Diffusion {
+    Mesh m;
+    int N = 0;
+    int unsteady = 0, method = K_BICGSTAB_SGS, maxit = 10000;
+    double rtol = 1e-8;
+    Field<double> phi;
+    Field<V3> gradPhi;
+    BC<double> bc;
+    Rows A;
+    std::vector<double> b, x, res;
+    int iters = 0;
+    double relRes = 0., resInf = 0.;
+
+    // Diffusion::Diffusion (Diffusion.cpp:35-53): boundary types and reference values
+    // (PrimitiveBoundaryCondition(input, field), PrimitiveBoundaryCondition.tpp:4-30, which
+    // fixes the patches), then the uniform initial value of phi.
+    void init(const double* xyz, int nNI, int nNJ, int nNK, const int* types, const double* refs, int timeAccurate, double phi0,
+              int kspMethod, double tol, int maxIters) {
+        m.build(xyz, nNI, nNJ, nNK);
+        N = (int)m.N();
+        unsteady = timeAccurate; method = kspMethod; rtol = tol; maxit = maxIters;
+        phi.allocate(m.nI, m.nJ, m.nK);
+        gradPhi.allocate(m.nI, m.nJ, m.nK);
+        bc.init(&phi);
+        for (int f = 0; f < 6; ++f) {
+            if (types[f] < 0 || types[f] > 2) throw std::runtime_error("invalid boundary type");
+            bc.type[f] = (PType)types[f];
+            bc.ref[f] = refs[f];
+        }
+        bc.setFixedBoundaries();
+        std::fill(phi.c.begin(), phi.c.end(), phi0);
+        A.allocate(N, 7);
+        b.assign(N, 0.); x.assign(N, 0.); res.assign(N, 0.);
+    }
+
+    // Diffusion::solve (Diffusion.cpp:58-131); returns ||A x - b||_inf
+    double solve(double dt) {
+        for (int k = 0; k < m.nK; ++k)
+            for (int j = 0; j < m.nJ; ++j)
+                for (int i = 0; i < m.nI; ++i) {
+                    int c = m.cid(i, j, k);
+                    double a0P = unsteady ? m.vol[c] / dt : 0.;
+                    double a[7];
+                    for (int f = 0; f < 6; ++f) a[f + 1] = m.d[f][c];
+                    a[0] = -(a[1] + a[2] + a[3] + a[4] + a[5] + a[6]) + a0P;
+                    double bb = a0P * phi.c[c];
+                    bc.setImplicit(i, j, k, a, bb);
+                    int cols[7] = {c, i < m.uI() ? c + 1 : -1, i > 0 ? c - 1 : -1, j < m.uJ() ? c + m.nI : -1,
+                                   j > 0 ? c - m.nI : -1, k < m.uK() ? c + m.nI * m.nJ : -1, k > 0 ? c - m.nI * m.nJ : -1};
+                    A.setRow(c, 7, cols, a);
+                    b[c] = bb;
+                }
+        KspStats st = kspSolve(method, A, b, x, rtol, maxit);
+        iters = st.iters;
+        relRes = trueRelRes(A, b, x, res);
+        phi.c = x;
+        bc.setBoundaries();
+        extrapolateInteriorFaces();
+        cellGradients(m, phi, gradPhi);
+        A.mult(x, res);                       // res = A x - b (Diffusion.cpp:127-130)
+        resInf = 0.;
+        for (int q = 0; q < N; ++q) { res[q] -= b[q]; resInf = std::max(resInf, std::fabs(res[q])); }
+        return resInf;
+    }
+
+    // FvScalarScheme::extrapolateInteriorFaces (FvScalarScheme.cpp:70-156) on one block:
+    // volume-weighted faces, divergence-theorem gradients, then every interior face from the
+    // two cells' gradients, clamped to the range of the lower cell and its 6 neighbours.
+    // Each interior face is written by its lower cell only, so the order does not matter.
+    void extrapolateInteriorFaces() {
+        interpolateInteriorFaces(m, phi);
+        cellGradients(m, phi, gradPhi);
+#pragma omp parallel for schedule(static)
+        for (int k = 0; k < m.nK; ++k)
+            for (int j = 0; j < m.nJ; ++j)
+                for (int i = 0; i < m.nI; ++i) {
+                    int c = m.cid(i, j, k);
+                    double p = phi.c[c];
+                    bool lE = false, lN = false, lT = false;
+                    if (i < m.uI()) {
+                        phi.faceE(i, j, k) = 0.5 * (p + dot(gradPhi.c[c], m.c2f[0][c]) + phi.c[c + 1] + dot(gradPhi.c[c + 1], m.c2f[1][c + 1]));
+                        lE = true;
+                    }
+                    if (j < m.uJ()) {
+                        int n = c + m.nI;
+                        phi.faceN(i, j, k) = 0.5 * (p + dot(gradPhi.c[c], m.c2f[2][c]) + phi.c[n] + dot(gradPhi.c[n], m.c2f[3][n]));
+                        lN = true;
+                    }
+                    if (k < m.uK()) {
+                        int t = c + m.nI * m.nJ;
+                        phi.faceT(i, j, k) = 0.5 * (p + dot(gradPhi.c[c], m.c2f[4][c]) + phi.c[t] + dot(gradPhi.c[t], m.c2f[5][t]));
+                        lT = true;
+                    }
+                    // Field::maxNeighbour / minNeighbour (Field.tpp:407-438), boundary patches included
+                    double hi = p, lo = p;
+                    const double nb[6] = {phi.at(i + 1, j, k), phi.at(i - 1, j, k), phi.at(i, j + 1, k),
+                                          phi.at(i, j - 1, k), phi.at(i, j, k + 1), phi.at(i, j, k - 1)};
+                    for (double v : nb) { hi = std::max(hi, v); lo = std::min(lo, v); }
+                    if (lE) phi.faceE(i, j, k) = std::max(std::min(hi, phi.faceE(i, j, k)), lo);
+                    if (lN) phi.faceN(i, j, k) = std::max(std::min(hi, phi.faceN(i, j, k)), lo);
+                    if (lT) phi.faceT(i, j, k) = std::max(std::min(hi, phi.faceT(i, j, k)), lo);
+                }
+    }
+};
+
+// ----------------------------------------------------------------------------
 // Case description shared with the Python side (ctypes Structure of the same layout)
 // ----------------------------------------------------------------------------
 enum SolverKind { S_SIMPLE = 0, S_PISO = 1, S_IBPISO = 2 };
@@ -1423,6 +1536,72 @@ void oracle_nearest_intersect(double radius, const double* center, const double*
     orc::V3 l = orc::unitv(orc::v3(pt[0], pt[1], pt[2]) - c);
     orc::V3 r = c + radius * l;
     out[0] = r.x; out[1] = r.y; out[2] = r.z;
+}
+
+// Diffusion solver.  types: per face E W N S T B, 0 fixed, 1 zeroGradient, 2 empty; refs:
+// Boundaries.<face>.refValue; phi0: uniform initial phi.
+void* oracle_diffusion_create(const double* xyz, int nNI, int nNJ, int nNK, const int* types, const double* refs, int time_accurate,
+                              double phi0, int method, double rtol, int maxit) {
+    try {
+        auto* s = new orc::Diffusion();
+        s->init(xyz, nNI, nNJ, nNK, types, refs, time_accurate, phi0, method, rtol, maxit);
+        return s;
+    } catch (const std::exception& e) { g_err = e.what(); return nullptr; }
+}
+void oracle_diffusion_destroy(void* h) { delete static_cast<orc::Diffusion*>(h); }
+int oracle_diffusion_solve(void* h, double dt, double* residual_inf) {
+    try { *residual_inf = static_cast<orc::Diffusion*>(h)->solve(dt); return 0; }
+    catch (const std::exception& e) { g_err = e.what(); return 1; }
+}
+// Krylov iterations and true relative residual of the last solve
+void oracle_diffusion_stats(void* h, double* out) {
+    auto* s = static_cast<orc::Diffusion*>(h);
+    out[0] = s->iters; out[1] = s->relRes;
+}
+// "phi", "gradPhi" (N x 3), "phiFaceI/J/K", "phiPatch0".."phiPatch5", "A" (N x 7: aP aE aW aN
+// aS aT aB as assembled), "b"; dir 0 out, 1 in.  Returns the count in doubles, -1 if unknown.
+long oracle_diffusion_array(void* hh, const char* name, double* buf, long count, int dir) {
+    auto* s = static_cast<orc::Diffusion*>(hh);
+    std::string n(name);
+    auto vecd = [&](std::vector<double>& v) -> long {
+        long need = (long)v.size();
+        if (buf && count >= need) {
+            if (dir == 0) std::memcpy(buf, v.data(), sizeof(double) * need);
+            else std::memcpy(v.data(), buf, sizeof(double) * need);
+        }
+        return need;
+    };
+    if (n == "phi") return vecd(s->phi.c);
+    if (n == "phiFaceI") return vecd(s->phi.fI);
+    if (n == "phiFaceJ") return vecd(s->phi.fJ);
+    if (n == "phiFaceK") return vecd(s->phi.fK);
+    if (n.rfind("phiPatch", 0) == 0 && n.size() == 9 && n[8] >= '0' && n[8] <= '5') return vecd(s->phi.patch[n[8] - '0']);
+    if (n == "b") return vecd(s->b);
+    if (n == "gradPhi") {
+        long need = 3L * s->N;
+        if (buf && count >= need && dir == 0)
+            for (int q = 0; q < s->N; ++q) { buf[3 * q] = s->gradPhi.c[q].x; buf[3 * q + 1] = s->gradPhi.c[q].y; buf[3 * q + 2] = s->gradPhi.c[q].z; }
+        return need;
+    }
+    if (n == "A") {
+        long need = 7L * s->N;
+        if (buf && count >= need && dir == 0) {
+            const orc::Mesh& m = s->m;
+            for (int c = 0; c < s->N; ++c) {
+                int i = c % m.nI, j = (c / m.nI) % m.nJ, k = c / (m.nI * m.nJ);
+                const int nb[7] = {c, i < m.uI() ? c + 1 : -2, i > 0 ? c - 1 : -2, j < m.uJ() ? c + m.nI : -2,
+                                   j > 0 ? c - m.nI : -2, k < m.uK() ? c + m.nI * m.nJ : -2, k > 0 ? c - m.nI * m.nJ : -2};
+                for (int q = 0; q < 7; ++q) {
+                    double v = 0.;
+                    for (int p = 0; p < s->A.cnt[c]; ++p)
+                        if (s->A.col[(size_t)c * s->A.width + p] == nb[q]) v = s->A.val[(size_t)c * s->A.width + p];
+                    buf[7 * (size_t)c + q] = v;
+                }
+            }
+        }
+        return need;
+    }
+    return -1;
 }
 
 }  // extern "C"

@@ -67,6 +67,15 @@ def lib():
         L.oracle_inside_hex.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
         L.oracle_trilinear.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
         L.oracle_nearest_intersect.argtypes = [ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        L.oracle_diffusion_create.restype = ctypes.c_void_p
+        L.oracle_diffusion_create.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+                                              ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_double,
+                                              ctypes.c_int]
+        L.oracle_diffusion_destroy.argtypes = [ctypes.c_void_p]
+        L.oracle_diffusion_solve.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.POINTER(ctypes.c_double)]
+        L.oracle_diffusion_stats.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        L.oracle_diffusion_array.restype = ctypes.c_long
+        L.oracle_diffusion_array.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_void_p, ctypes.c_long, ctypes.c_int]
         L.oracle_set_threads.argtypes = [ctypes.c_int]
         L.oracle_get_threads.restype = ctypes.c_int
         _lib = L
@@ -174,6 +183,72 @@ class OracleSolver:
         if v.size != n:
             raise ValueError(f"{name}: expected {n} values, got {v.size}")
         L.oracle_array(self._h, name.encode(), _ptr(v), n, 1)
+
+
+DIFFUSION_BC = {"fixed": 0, "zeroGradient": 1, "empty": 2}
+
+
+class OracleDiffusion:
+    """CPU restatement of the reference's Diffusion solver (src/Solvers/Diffusion.cpp) on one
+    block: unit diffusivity, boundary types fixed / zeroGradient / empty per face (east, west,
+    north, south, top, bottom) with their reference values, a uniform initial phi.
+    ``solve(dt)`` assembles and solves one linear system and returns ||A x - b||_inf."""
+
+    def __init__(self, nodes: np.ndarray, bc_types, bc_values, time_accurate: bool = False, phi0: float = 0.0,
+                 method: str = "bicgstab_sgs", rtol: float = 1e-8, maxit: int = 10000):
+        from caffe_old_b200 import cases as C
+        L = lib()
+        nodes = np.ascontiguousarray(nodes, dtype=np.float64)
+        nK1, nJ1, nI1, _ = nodes.shape
+        self.shape = (nI1 - 1, nJ1 - 1, nK1 - 1)
+        self.ncells = self.shape[0] * self.shape[1] * self.shape[2]
+        types = np.array([DIFFUSION_BC[t] for t in bc_types], dtype=np.int32)
+        refs = np.ascontiguousarray(bc_values, dtype=np.float64)
+        if types.size != 6 or refs.size != 6:
+            raise ValueError("six boundary types and values (east, west, north, south, top, bottom)")
+        h = L.oracle_diffusion_create(_ptr(nodes), nI1, nJ1, nK1, _ptr(types), _ptr(refs), 1 if time_accurate else 0,
+                                      float(phi0), C.KSP_METHODS[method], float(rtol), int(maxit))
+        if not h:
+            raise RuntimeError("oracle_diffusion_create failed: " + L.oracle_last_error().decode())
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().oracle_diffusion_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def solve(self, dt: float = 1.0) -> float:
+        out = ctypes.c_double(0.0)
+        if lib().oracle_diffusion_solve(self._h, float(dt), ctypes.byref(out)) != 0:
+            raise RuntimeError("oracle_diffusion_solve: " + lib().oracle_last_error().decode())
+        return out.value
+
+    def stats(self) -> dict:
+        out = np.zeros(2)
+        lib().oracle_diffusion_stats(self._h, _ptr(out))
+        return {"iters": int(out[0]), "rel_res": float(out[1])}
+
+    def get(self, name: str) -> np.ndarray:
+        L = lib()
+        n = L.oracle_diffusion_array(self._h, name.encode(), None, 0, 0)
+        if n < 0:
+            raise KeyError(name)
+        out = np.zeros(n, dtype=np.float64)
+        L.oracle_diffusion_array(self._h, name.encode(), _ptr(out), n, 0)
+        return out
+
+    def set(self, name: str, values: np.ndarray) -> None:
+        L = lib()
+        n = L.oracle_diffusion_array(self._h, name.encode(), None, 0, 0)
+        if n < 0:
+            raise KeyError(name)
+        v = np.ascontiguousarray(values, dtype=np.float64).ravel()
+        if v.size != n:
+            raise ValueError(f"{name}: expected {n} values, got {v.size}")
+        L.oracle_diffusion_array(self._h, name.encode(), _ptr(v), n, 1)
 
 
 def ksp7(shape, coef7: np.ndarray, b: np.ndarray, method: str, rtol: float, maxit: int):
