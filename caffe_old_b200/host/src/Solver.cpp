@@ -21,6 +21,7 @@
 #include <iostream>
 
 #include "IbPiso.h"
+#include "MultiphasePiso.h"
 #include "InitialConditions.h"
 #include "Output.h"
 #include "Piso.h"
@@ -205,3 +206,6 @@ double Piso::solve(double timeStep) { return step(timeStep); }
 
 IbPiso::IbPiso(const Input& input, const HexaFvmMesh& mesh) : Piso(input, mesh, CAFFE_IBPISO) { name_ = "IbPiso"; }
 double IbPiso::solve(double timeStep) { return step(timeStep); }
+
+MultiphasePiso::MultiphasePiso(const Input& input, const HexaFvmMesh& mesh) : Piso(input, mesh, CAFFE_PISO) { name_ = "MultiphasePiso"; }
+double MultiphasePiso::solve(double timeStep) { return step(timeStep); }
