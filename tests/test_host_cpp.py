@@ -1,7 +1,8 @@
 """C++ host layer (caffe_old_b200/host): the reference's Input / RunControl / HexaFvmMesh /
 Solver interface over the device library.  CPU checks: the INFO-file parse maps every key
 to the same case record as the Python host; hexaMesh writes the same nodes; the reference's
-own module mains compile unchanged against these headers (when its sources are present)."""
+own module mains compile unchanged against these headers, and its shipped example cases and
+meshes parse (when its sources are present)."""
 import json
 import os
 import subprocess
@@ -87,3 +88,92 @@ def test_reference_module_mains_compile_unchanged(tmp_path, host_bins, module):
            os.path.join(REF_MODULES, module), "-o", str(exe), os.path.join(build, "libcaffe_host.a"), "-L", build, "-lcaffe_b200"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     assert r.returncode == 0, r.stderr[-2000:]
+
+
+REF_EXAMPLES = "/root/reference/ExampleCases"
+
+
+def _example_cases():
+    if not os.path.isdir(REF_EXAMPLES):
+        return []
+    out = []
+    for name in sorted(os.listdir(REF_EXAMPLES)):
+        case = os.path.join(REF_EXAMPLES, name, "case", "case.info")
+        if not os.path.isfile(case):
+            continue
+        text = open(case).read()
+        if "relaxationFactorMomentum" not in text:
+            continue                      # the diffusion example has no flow solver keys
+        kind = "ibpiso" if "ImmersedBoundaries" in text else ("piso" if "timeAccurate ON" in text else "simple")
+        out.append((name, kind))
+    return out
+
+
+def _info_value(text, block, key):
+    """The value of `key` inside `block { ... }` of an INFO file (plain text scan)."""
+    import re
+    body = text[text.index(block):]
+    return re.search(rf"^\s*{key}\s+(\S+)", body, flags=re.M).group(1)
+
+
+@pytest.mark.skipif(not os.path.isdir(REF_EXAMPLES), reason="reference example cases not present")
+@pytest.mark.parametrize("name,kind", _example_cases())
+def test_reference_example_cases_parse(tmp_path, host_bins, name, kind):
+    """Every flow example case the reference ships (ExampleCases/*/case), read where it lies,
+    parses with the host layer's INFO reader into the device library's case record, with
+    the values the files give.  An example without Boundaries.<face>.refValue is refused
+    with the missing key named: FlowBoundaryConditions.cpp reads refValue for every face
+    with no default, so the reference's own lookup throws on that file too."""
+    import shutil
+    shutil.copytree(os.path.join(REF_EXAMPLES, name, "case"), tmp_path / "case")
+    out = subprocess.run([os.path.join(host_bins, "caffeCaseInfo"), kind], cwd=tmp_path, capture_output=True, text=True)
+    text = (tmp_path / "case" / "case.info").read_text()
+    if text[text.index("Boundaries"):].count("refValue") < 6:
+        assert out.returncode == 1 and "refValue" in out.stderr, out.stderr
+        return
+    assert out.returncode == 0, out.stderr
+    got = json.loads(out.stdout)
+    assert got["rho"] == float(_info_value(text, "Solver", "rho"))
+    assert got["mu"] == float(_info_value(text, "Solver", "mu"))
+    assert got["omega_u"] == float(_info_value(text, "Solver", "relaxationFactorMomentum"))
+    assert got["omega_p"] == float(_info_value(text, "Solver", "relaxationFactorPCorr"))
+    assert got["time_accurate"] == (1 if _info_value(text, "Solver", "timeAccurate") == "ON" else 0)
+    faces = ["east", "west", "north", "south", "top", "bottom"]
+    types = {"inlet": 0, "outlet": 1, "wall": 2, "empty": 3, "zeroGradient": 4}
+    for f, face in enumerate(faces):
+        block = text[text.index("Boundaries"):]
+        assert got["bc_type"][f] == types[_info_value(block, face, "type")], face
+    if kind == "ibpiso":
+        assert got["ib_radius"] == float(_info_value(text, "ImmersedBoundaries", "radius"))
+
+
+def _example_meshes():
+    if not os.path.isdir(REF_EXAMPLES):
+        return []
+    return [n for n in sorted(os.listdir(REF_EXAMPLES)) if os.path.isfile(os.path.join(REF_EXAMPLES, n, "mesh", "structuredMesh.info"))]
+
+
+@pytest.mark.skipif(not os.path.isdir(REF_EXAMPLES), reason="reference example cases not present")
+@pytest.mark.parametrize("name", _example_meshes())
+def test_reference_example_meshes_generate(tmp_path, host_bins, name):
+    """hexaMesh reads every mesh/structuredMesh.info the reference ships (with its resolution
+    reduced to 6 x 5 x 4 nodes to keep the file small): the corner nodes are the file's
+    vertices times its MetricConversion."""
+    import re
+    src = open(os.path.join(REF_EXAMPLES, name, "mesh", "structuredMesh.info")).read()
+    small = re.sub(r"^(\s*Resolution\s+)\([^)]*\)", r"\1(6,5,4)", src, flags=re.M)
+    assert small != src
+    (tmp_path / "mesh").mkdir()
+    (tmp_path / "mesh" / "structuredMesh.info").write_text(small)
+    r = subprocess.run([os.path.join(host_bins, "hexaMesh")], cwd=tmp_path, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    with open(tmp_path / "mesh" / "structuredMesh.dat") as f:
+        body = f.read().split("DATAPACKING = BLOCK\n", 1)[1]
+    nodes = np.moveaxis(np.array([float(v) for v in body.split()]).reshape(3, 4, 5, 6), 0, -1)   # (k, j, i, xyz)
+    scale = float(re.search(r"^\s*MetricConversion\s*=?\s*(\S+)", src, flags=re.M).group(1))
+    verts = [np.array([float(x) for x in re.search(rf"^\s*v{q}\s+\(([^)]*)\)", src, flags=re.M).group(1).split(",")])
+             for q in range(1, 9)]
+    corners = [nodes[0, 0, 0], nodes[0, 0, -1], nodes[0, -1, -1], nodes[0, -1, 0],
+               nodes[-1, 0, 0], nodes[-1, 0, -1], nodes[-1, -1, -1], nodes[-1, -1, 0]]
+    for q in range(8):
+        assert np.allclose(corners[q], scale * verts[q], rtol=0, atol=1e-14), (name, q, corners[q], verts[q])
