@@ -1317,6 +1317,200 @@ struct Solver {
     }
 };
 
+// ----------------------------------------------------------------------------
+// Coupled (src/Solvers/Coupled.cpp): momentum and continuity in one linear system of
+// 4 N unknowns (u_x, u_y, u_z, p, blocked by variable: row = cell + var N, IndexMap.cpp:47-52),
+// on one block without an immersed boundary.  Momentum rows hold 7 velocity and 7 pressure
+// coefficients, continuity rows 3 x 7 velocity and 7 pressure coefficients (28).  The
+// reference's own conventions are kept: rho and mu are constant fields (Field::setAll,
+// Field.tpp:271-278), the face mass flux carries no rho (Coupled.cpp:282-314), the boundary
+// faces of the pressure-gradient field stay zero, p is never interpolated to interior faces
+// before its gradient (Coupled.cpp:257-258, so those faces keep their initial zero), and u and
+// p start at zero (the constructor applies no initial conditions).
+// ----------------------------------------------------------------------------
+struct Coupled {
+    Mesh m;
+    OracleCase cs;
+    int N = 0;
+    Field<V3> u, h, gradP, u0, uStar;
+    Field<double> p, d, mf;
+    BC<V3> uBc, hBc;
+    BC<double> pBc, dBc;
+    Rows A;
+    std::vector<double> b, x;
+    KspStats st{0, 0., 0};
+    int nInner = 1;
+    double omega = 1., rho = 1., mu = 1.;
+
+    // Coupled::Coupled (Coupled.cpp:5-34) with FlowBoundaryConditions (FlowBoundaryConditions.cpp:3-73)
+    void init(const double* xyz, int nNI, int nNJ, int nNK, const OracleCase& c) {
+        cs = c;
+        m.build(xyz, nNI, nNJ, nNK);
+        N = (int)m.N();
+        u.allocate(m.nI, m.nJ, m.nK); h.allocate(m.nI, m.nJ, m.nK); gradP.allocate(m.nI, m.nJ, m.nK);
+        u0.allocate(m.nI, m.nJ, m.nK); uStar.allocate(m.nI, m.nJ, m.nK);
+        p.allocate(m.nI, m.nJ, m.nK); d.allocate(m.nI, m.nJ, m.nK); mf.allocate(m.nI, m.nJ, m.nK);
+        uBc.init(&u); hBc.init(&h); pBc.init(&p); dBc.init(&d);
+        for (int f = 0; f < 6; ++f) {
+            int t = cs.bc_type[f];
+            V3 rv = v3(cs.ref_vec[f][0], cs.ref_vec[f][1], cs.ref_vec[f][2]);
+            double rp = cs.ref_val[f];
+            if (t == F_INLET || t == F_WALL) {
+                uBc.changeType(f, P_FIXED, rv); pBc.changeType(f, P_ZERO_GRADIENT, rp); hBc.changeType(f, P_FIXED, rv);
+            } else if (t == F_OUTLET) {
+                uBc.changeType(f, P_ZERO_GRADIENT, rv); pBc.changeType(f, P_FIXED, rp); hBc.changeType(f, P_ZERO_GRADIENT, rv);
+            } else if (t == F_EMPTY) {
+                uBc.changeType(f, P_EMPTY, rv); pBc.changeType(f, P_EMPTY, rp); hBc.changeType(f, P_EMPTY, rv);
+            } else if (t == F_ZERO_GRADIENT) {
+                uBc.changeType(f, P_ZERO_GRADIENT, rv); pBc.changeType(f, P_ZERO_GRADIENT, rp); hBc.changeType(f, P_ZERO_GRADIENT, rv);
+            } else throw std::runtime_error("invalid boundary type");
+            dBc.changeType(f, P_ZERO_GRADIENT, 0.);
+        }
+        nInner = cs.time_accurate ? cs.n_inner : 1;
+        omega = cs.omega_u; rho = cs.rho; mu = cs.mu;
+        A.allocate(4 * N, 28);
+        b.assign(4 * (size_t)N, 0.); x.assign(4 * (size_t)N, 0.);
+    }
+    int idx(int i, int j, int k, int var) const {  // IndexMap::operator(), one block, every cell active
+        if (i < 0 || j < 0 || k < 0 || i >= m.nI || j >= m.nJ || k >= m.nK) return -1;
+        return m.cid(i, j, k) + var * N;
+    }
+
+    // Coupled::solve (Coupled.cpp:38-50)
+    double solve(double dt) {
+        u0.c = u.c;
+        for (int it = 0; it < nInner; ++it) computeMomentumAndPressure(dt);
+        return computeContinuityError();
+    }
+
+    // Coupled::computeMomentumAndPressure (Coupled.cpp:54-280)
+    void computeMomentumAndPressure(double dt) {
+        uStar.c = u.c;
+        const int dI[7] = {0, 1, -1, 0, 0, 0, 0}, dJ[7] = {0, 0, 0, 1, -1, 0, 0}, dK[7] = {0, 0, 0, 0, 0, 1, -1};
+        // momentum rows
+        for (int k = 0; k < m.nK; ++k)
+            for (int j = 0; j < m.nJ; ++j)
+                for (int i = 0; i < m.nI; ++i) {
+                    int c = m.cid(i, j, k);
+                    double a0P = cs.time_accurate ? rho * m.vol[c] / dt : 0.;
+                    double FE = mf.faceE(i, j, k), FW = mf.faceW(i, j, k), FN = mf.faceN(i, j, k), FS = mf.faceS(i, j, k),
+                           FT = mf.faceT(i, j, k), FB = mf.faceB(i, j, k);
+                    double a[14];
+                    a[0] = (std::max(FE, 0.) + mu * m.d[0][c] - std::min(FW, 0.) + mu * m.d[1][c] + std::max(FN, 0.) + mu * m.d[2][c] -
+                            std::min(FS, 0.) + mu * m.d[3][c] + std::max(FT, 0.) + mu * m.d[4][c] - std::min(FB, 0.) + mu * m.d[5][c] +
+                            a0P) / omega;
+                    a[1] = std::min(FE, 0.) - mu * m.d[0][c];
+                    a[2] = -std::max(FW, 0.) - mu * m.d[1][c];
+                    a[3] = std::min(FN, 0.) - mu * m.d[2][c];
+                    a[4] = -std::max(FS, 0.) - mu * m.d[3][c];
+                    a[5] = std::min(FT, 0.) - mu * m.d[4][c];
+                    a[6] = -std::max(FB, 0.) - mu * m.d[5][c];
+                    V3 bu = a0P * u0.c[c];
+                    bu += (1. - omega) * a[0] * uStar.c[c];
+                    uBc.setImplicit(i, j, k, a, bu);
+                    for (int q = 0; q < 3; ++q) {
+                        double g[6], s[6];
+                        for (int f = 0; f < 6; ++f) { g[f] = m.g[f][c]; s[f] = comp(m.S(f, i, j, k), q); }
+                        a[7] = g[0] * s[0] + g[1] * s[1] + g[2] * s[2] + g[3] * s[3] + g[4] * s[4] + g[5] * s[5];
+                        for (int f = 0; f < 6; ++f) a[8 + f] = (1. - g[f]) * s[f];
+                        int cols[14];
+                        for (int e = 0; e < 7; ++e) {
+                            cols[e] = idx(i + dI[e], j + dJ[e], k + dK[e], q);
+                            cols[7 + e] = idx(i + dI[e], j + dJ[e], k + dK[e], 3);
+                        }
+                        pBc.setImplicit(i, j, k, &a[7], comp(bu, q));
+                        A.setRow(idx(i, j, k, q), 14, cols, a);
+                        b[idx(i, j, k, q)] = comp(bu, q);
+                    }
+                    d.c[c] = m.vol[c] / a[0];
+                }
+        dBc.setBoundaries();
+        interpolateInteriorFaces(m, d);
+        // continuity rows
+        for (int k = 0; k < m.nK; ++k)
+            for (int j = 0; j < m.nJ; ++j)
+                for (int i = 0; i < m.nI; ++i) {
+                    int c = m.cid(i, j, k);
+                    int rowNo = idx(i, j, k, 3);
+                    double bp = 0.;
+                    double a[7];
+                    int cols[7];
+                    for (int q = 0; q < 3; ++q) {
+                        double g[6], s[6];
+                        for (int f = 0; f < 6; ++f) { g[f] = m.g[f][c]; s[f] = comp(m.S(f, i, j, k), q); }
+                        a[0] = rho * g[0] * s[0] + rho * g[1] * s[1] + rho * g[2] * s[2] + rho * g[3] * s[3] + rho * g[4] * s[4] +
+                               rho * g[5] * s[5];
+                        for (int f = 0; f < 6; ++f) a[1 + f] = rho * (1. - g[f]) * s[f];
+                        for (int e = 0; e < 7; ++e) cols[e] = idx(i + dI[e], j + dJ[e], k + dK[e], q);
+                        V3 bu = zero3();
+                        uBc.setImplicit(i, j, k, a, bu);
+                        bp += comp(bu, q);
+                        A.setRow(rowNo, 7, cols, a);
+                    }
+                    // pressure part: the Rhie-Chow interpolation
+                    double rd[6] = {rho * d.faceE(i, j, k) * m.d[0][c], rho * d.faceW(i, j, k) * m.d[1][c],
+                                    rho * d.faceN(i, j, k) * m.d[2][c], rho * d.faceS(i, j, k) * m.d[3][c],
+                                    rho * d.faceT(i, j, k) * m.d[4][c], rho * d.faceB(i, j, k) * m.d[5][c]};
+                    a[0] = rd[0] + rd[1] + rd[2] + rd[3] + rd[4] + rd[5];
+                    for (int f = 0; f < 6; ++f) a[1 + f] = -rd[f];
+                    for (int e = 0; e < 7; ++e) cols[e] = idx(i + dI[e], j + dJ[e], k + dK[e], 3);
+                    bp -= rho * d.faceE(i, j, k) * dot(gradP.faceE(i, j, k), m.SE(i, j, k)) +
+                          rho * d.faceW(i, j, k) * dot(gradP.faceW(i, j, k), m.SW(i, j, k)) +
+                          rho * d.faceN(i, j, k) * dot(gradP.faceN(i, j, k), m.SN(i, j, k)) +
+                          rho * d.faceS(i, j, k) * dot(gradP.faceS(i, j, k), m.SS(i, j, k)) +
+                          rho * d.faceT(i, j, k) * dot(gradP.faceT(i, j, k), m.ST(i, j, k)) +
+                          rho * d.faceB(i, j, k) * dot(gradP.faceB(i, j, k), m.SB(i, j, k));
+                    pBc.setImplicit(i, j, k, a, bp);
+                    A.setRow(rowNo, 7, cols, a);
+                    b[rowNo] = bp;
+                }
+        st = kspSolve(cs.mom_method, A, b, x, cs.mom_rtol, cs.maxit);
+        for (int c = 0; c < N; ++c) {
+            u.c[c] = v3(x[c], x[c + N], x[c + 2 * (size_t)N]);
+            p.c[c] = x[c + 3 * (size_t)N];
+        }
+        pBc.setBoundaries();
+        cellGradients(m, p, gradP);
+        interpolateInteriorFaces(m, gradP);
+        for (int c = 0; c < N; ++c) h.c[c] = u.c[c] + d.c[c] * gradP.c[c];
+        hBc.setBoundaries();
+        interpolateInteriorFaces(m, h);
+        uBc.setBoundaries();
+        rhieChowInterpolateFaces();
+    }
+
+    // Coupled::rhieChowInterpolateFaces (Coupled.cpp:282-314): no rho in the face flux
+    void rhieChowInterpolateFaces() {
+        for (int k = 0; k < m.nK; ++k)
+            for (int j = 0; j < m.nJ; ++j)
+                for (int i = 0; i < m.nI; ++i) {
+                    int c = m.cid(i, j, k);
+                    if (i == 0)
+                        mf.faceW(i, j, k) = -dot(h.faceW(i, j, k), m.SW(i, j, k)) - d.faceW(i, j, k) * (p.at(i - 1, j, k) - p.c[c]) * m.d[1][c];
+                    if (j == 0)
+                        mf.faceS(i, j, k) = -dot(h.faceS(i, j, k), m.SS(i, j, k)) - d.faceS(i, j, k) * (p.at(i, j - 1, k) - p.c[c]) * m.d[3][c];
+                    if (k == 0)
+                        mf.faceB(i, j, k) = -dot(h.faceB(i, j, k), m.SB(i, j, k)) - d.faceB(i, j, k) * (p.at(i, j, k - 1) - p.c[c]) * m.d[5][c];
+                    mf.faceE(i, j, k) = dot(h.faceE(i, j, k), m.SE(i, j, k)) - d.faceE(i, j, k) * (p.at(i + 1, j, k) - p.c[c]) * m.d[0][c];
+                    mf.faceN(i, j, k) = dot(h.faceN(i, j, k), m.SN(i, j, k)) - d.faceN(i, j, k) * (p.at(i, j + 1, k) - p.c[c]) * m.d[2][c];
+                    mf.faceT(i, j, k) = dot(h.faceT(i, j, k), m.ST(i, j, k)) - d.faceT(i, j, k) * (p.at(i, j, k + 1) - p.c[c]) * m.d[4][c];
+                }
+    }
+
+    // Coupled::computeContinuityError (Coupled.cpp:316-339)
+    double computeContinuityError() {
+        double mx = 0.;
+        for (int k = 0; k < m.nK; ++k)
+            for (int j = 0; j < m.nJ; ++j)
+                for (int i = 0; i < m.nI; ++i) {
+                    double e = std::fabs(mf.faceE(i, j, k) - mf.faceW(i, j, k) + mf.faceN(i, j, k) - mf.faceS(i, j, k) +
+                                         mf.faceT(i, j, k) - mf.faceB(i, j, k)) / m.vol[m.cid(i, j, k)];
+                    if (e > mx) mx = e;
+                }
+        return mx;
+    }
+};
+
 }  // namespace orc
 
 // ----------------------------------------------------------------------------
@@ -1536,6 +1730,58 @@ void oracle_nearest_intersect(double radius, const double* center, const double*
     orc::V3 l = orc::unitv(orc::v3(pt[0], pt[1], pt[2]) - c);
     orc::V3 r = c + radius * l;
     out[0] = r.x; out[1] = r.y; out[2] = r.z;
+}
+
+// Coupled solver (kind is ignored; the boundary types, rho, mu, timeAccurate, relaxation of
+// momentum, inner iterations and the Krylov settings mom_method / mom_rtol / maxit are used).
+void* oracle_coupled_create(const double* xyz, int nNI, int nNJ, int nNK, const OracleCase* cs) {
+    try {
+        auto* s = new orc::Coupled();
+        s->init(xyz, nNI, nNJ, nNK, *cs);
+        return s;
+    } catch (const std::exception& e) { g_err = e.what(); return nullptr; }
+}
+void oracle_coupled_destroy(void* h) { delete static_cast<orc::Coupled*>(h); }
+int oracle_coupled_solve(void* h, double dt, double* continuity) {
+    try { *continuity = static_cast<orc::Coupled*>(h)->solve(dt); return 0; }
+    catch (const std::exception& e) { g_err = e.what(); return 1; }
+}
+// Krylov iterations, relative residual and status of the last coupled solve
+void oracle_coupled_stats(void* h, double* out) {
+    auto* s = static_cast<orc::Coupled*>(h);
+    out[0] = s->st.iters; out[1] = s->st.rel_res; out[2] = s->st.status;
+}
+// "u" (N x 3), "p", "d", "gradP" (N x 3), "massFlowI/J/K", "b" (4N); dir 0 out, 1 in
+long oracle_coupled_array(void* hh, const char* name, double* buf, long count, int dir) {
+    auto* s = static_cast<orc::Coupled*>(hh);
+    std::string n(name);
+    auto vecd = [&](std::vector<double>& v) -> long {
+        long need = (long)v.size();
+        if (buf && count >= need) {
+            if (dir == 0) std::memcpy(buf, v.data(), sizeof(double) * need);
+            else std::memcpy(v.data(), buf, sizeof(double) * need);
+        }
+        return need;
+    };
+    auto vecv = [&](std::vector<orc::V3>& v) -> long {
+        long need = (long)v.size() * 3;
+        if (buf && count >= need) {
+            for (size_t q = 0; q < v.size(); ++q) {
+                if (dir == 0) { buf[3 * q] = v[q].x; buf[3 * q + 1] = v[q].y; buf[3 * q + 2] = v[q].z; }
+                else v[q] = orc::v3(buf[3 * q], buf[3 * q + 1], buf[3 * q + 2]);
+            }
+        }
+        return need;
+    };
+    if (n == "u") return vecv(s->u.c);
+    if (n == "gradP") return vecv(s->gradP.c);
+    if (n == "p") return vecd(s->p.c);
+    if (n == "d") return vecd(s->d.c);
+    if (n == "massFlowI") return vecd(s->mf.fI);
+    if (n == "massFlowJ") return vecd(s->mf.fJ);
+    if (n == "massFlowK") return vecd(s->mf.fK);
+    if (n == "b") return vecd(s->b);
+    return -1;
 }
 
 // Diffusion solver.  types: per face E W N S T B, 0 fixed, 1 zeroGradient, 2 empty; refs:

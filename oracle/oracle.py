@@ -67,6 +67,13 @@ def lib():
         L.oracle_inside_hex.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
         L.oracle_trilinear.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
         L.oracle_nearest_intersect.argtypes = [ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        L.oracle_coupled_create.restype = ctypes.c_void_p
+        L.oracle_coupled_create.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(OracleCase)]
+        L.oracle_coupled_destroy.argtypes = [ctypes.c_void_p]
+        L.oracle_coupled_solve.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.POINTER(ctypes.c_double)]
+        L.oracle_coupled_stats.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        L.oracle_coupled_array.restype = ctypes.c_long
+        L.oracle_coupled_array.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_void_p, ctypes.c_long, ctypes.c_int]
         L.oracle_diffusion_create.restype = ctypes.c_void_p
         L.oracle_diffusion_create.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
                                               ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_double,
@@ -183,6 +190,55 @@ class OracleSolver:
         if v.size != n:
             raise ValueError(f"{name}: expected {n} values, got {v.size}")
         L.oracle_array(self._h, name.encode(), _ptr(v), n, 1)
+
+
+class OracleCoupled:
+    """CPU restatement of the reference's Coupled solver (src/Solvers/Coupled.cpp): momentum
+    and continuity in one linear system of 4 N unknowns.  The case record's boundary types,
+    rho, mu, timeAccurate, relaxationFactorMomentum, numberOfInnerIterations and the momentum
+    Krylov settings (method, tolerance, maxit) are used.  ``solve(dt)`` returns the maximum
+    continuity error."""
+
+    def __init__(self, nodes: np.ndarray, spec):
+        L = lib()
+        nodes = np.ascontiguousarray(nodes, dtype=np.float64)
+        nK1, nJ1, nI1, _ = nodes.shape
+        self.shape = (nI1 - 1, nJ1 - 1, nK1 - 1)
+        self.ncells = self.shape[0] * self.shape[1] * self.shape[2]
+        self.spec = spec
+        self._case = make_case(spec)
+        h = L.oracle_coupled_create(_ptr(nodes), nI1, nJ1, nK1, ctypes.byref(self._case))
+        if not h:
+            raise RuntimeError("oracle_coupled_create failed: " + L.oracle_last_error().decode())
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().oracle_coupled_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def solve(self, dt: float | None = None) -> float:
+        out = ctypes.c_double(0.0)
+        if lib().oracle_coupled_solve(self._h, float(self.spec.dt if dt is None else dt), ctypes.byref(out)) != 0:
+            raise RuntimeError("oracle_coupled_solve: " + lib().oracle_last_error().decode())
+        return out.value
+
+    def stats(self) -> dict:
+        out = np.zeros(3)
+        lib().oracle_coupled_stats(self._h, _ptr(out))
+        return {"iters": int(out[0]), "rel_res": float(out[1]), "status": int(out[2])}
+
+    def get(self, name: str) -> np.ndarray:
+        L = lib()
+        n = L.oracle_coupled_array(self._h, name.encode(), None, 0, 0)
+        if n < 0:
+            raise KeyError(name)
+        out = np.zeros(n, dtype=np.float64)
+        L.oracle_coupled_array(self._h, name.encode(), _ptr(out), n, 0)
+        return out
 
 
 DIFFUSION_BC = {"fixed": 0, "zeroGradient": 1, "empty": 2}
