@@ -26,8 +26,9 @@
 //
 // Pinning.  The geometry (hexahedron volume and centroid, face area, centroid and
 // vector, point-in-cell test, sphere intersection), the mesh metric arrays (D_f,
-// c_f), the cell storage order and the immersed-boundary geometry (solid cells,
-// ghost cells, image-point stencils) are pinned bit for bit against the reference's
+// c_f), the velocity-gradient tensor, the cell storage order and the
+// immersed-boundary geometry (solid cells, ghost cells, image-point stencils) are
+// pinned bit for bit against the reference's
 // own Geometry / Sphere / Vector3D / Tensor3D / Array3D code, compiled where it lies
 // (tests/test_oracle_pinned_reference.py; tests/golden/reference_geometry.npz keeps
 // the reference's outputs).  The rest -- the flow phases, the trilinear weights and
@@ -1622,6 +1623,15 @@ long oracle_array(void* hh, const char* name, double* buf, long count, int dir) 
     if (n == "h") return vecv(s->h.c);
     if (n == "gradP") return vecv(s->gradP.c);
     if (n == "gradPCorr") return vecv(s->gradPC.c);
+    if (n == "uFaceI") return vecv(s->u.fI);
+    if (n == "uFaceJ") return vecv(s->u.fJ);
+    if (n == "uFaceK") return vecv(s->u.fK);
+    if (n == "gradU") {   // N x 9, row-major xx xy xz / yx yy yz / zx zy zz (non-orthogonal correction only)
+        long need = 9L * (long)s->gradU.c.size();
+        if (buf && count >= need && dir == 0)
+            for (size_t q = 0; q < s->gradU.c.size(); ++q) std::memcpy(buf + 9 * q, s->gradU.c[q].m, 9 * sizeof(double));
+        return need;
+    }
     if (n == "u0") return vecv(s->uf0.c);
     if (n == "p") return vecd(s->p.c);
     if (n == "pCorr") return vecd(s->pc.c);

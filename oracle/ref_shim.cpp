@@ -6,6 +6,7 @@
 #include "Array3D.h"
 #include "Geometry.h"
 #include "Sphere.h"
+#include "Tensor3D.h"
 
 namespace {
 void load(const double* p, int n, Point3D* out) {
@@ -62,6 +63,20 @@ void ref_d_and_c(const double* s3, const double* r3, double* out) {
     double d = dot(s, s) / dot(s, r);
     Vector3D c = s - r * dot(s, s) / dot(s, r);
     out[0] = d; out[1] = c.x; out[2] = c.y; out[3] = c.z;
+}
+// divergence-theorem velocity gradient of one cell from its six face velocities and outward
+// face vectors (E W N S T B), in the reference's Vector3D / Tensor3D arithmetic
+// (FvVectorScheme.cpp:64-69): out = 9 entries, row-major
+void ref_grad_tensor(const double* uf18, const double* s18, double volume, double* out) {
+    Vector3D u[6], s[6];
+    for (int f = 0; f < 6; ++f) {
+        u[f] = Vector3D(uf18[3 * f], uf18[3 * f + 1], uf18[3 * f + 2]);
+        s[f] = Vector3D(s18[3 * f], s18[3 * f + 1], s18[3 * f + 2]);
+    }
+    Tensor3D g = (tensor(u[0], s[0]) + tensor(u[1], s[1]) + tensor(u[2], s[2]) + tensor(u[3], s[3]) + tensor(u[4], s[4]) +
+                  tensor(u[5], s[5])) / volume;
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) out[3 * r + c] = g(r, c);
 }
 // offset of element (i, j, k) in an Array3D of sizeI x sizeJ x sizeK, or -1 where the
 // reference's bounds-checked operator() throws

@@ -3,9 +3,10 @@
 oracle/_ref/libref_geometry.so by `make -C oracle ref`) on seeded sheared and jittered
 hexahedra, its Array3D container's element offsets, and the metric arrays (cell volumes and
 centroids, face centroids and face vectors, D_f and c_f) of a sheared, jittered mesh built
-from those routines, and the immersed-boundary geometry of the channel with a sphere (solid
-cells, ghost cells and their 8-cell stencils), so that the oracle stays pinned to them where
-the reference sources are absent.
+from those routines, the immersed-boundary geometry of the channel with a sphere (solid
+cells, ghost cells and their 8-cell stencils), and the velocity-gradient tensors of one step
+of the sheared cavity, so that the oracle stays pinned to them where the reference sources
+are absent.
 
   python tests/golden/make_geometry_golden.py
 """
@@ -193,9 +194,35 @@ def main():
                     ref.ref_d_and_c(p(np.ascontiguousarray(sv)), p(np.ascontiguousarray(r)), p(out))
                     dc[f, k, j, i] = out
     mesh["mesh_d_and_c"] = dc
+    # velocity-gradient tensors of the non-orthogonal correction (FvVectorScheme.cpp:64-69) by
+    # the reference's Tensor3D arithmetic, from the face velocities and face vectors of one
+    # oracle step on the sheared, jittered cavity of the parity tests (the inputs only)
+    sys.path.insert(0, os.path.dirname(HERE))
+    from helpers import small_skewed
+    from oracle.oracle import OracleSolver
+    ref.ref_grad_tensor.argtypes = [dp, dp, ctypes.c_double, dp]
+    gnodes, gspec = small_skewed()
+    o = OracleSolver(gnodes, gspec)
+    o.solve()
+    gK, gJ, gI = (d - 1 for d in gnodes.shape[:3])
+    uI = o.get("uFaceI").reshape(gK, gJ, gI + 1, 3)
+    uJ = o.get("uFaceJ").reshape(gK, gJ + 1, gI, 3)
+    uK = o.get("uFaceK").reshape(gK + 1, gJ, gI, 3)
+    SI = o.get("SI").reshape(gK, gJ, gI + 1, 3)
+    SJ = o.get("SJ").reshape(gK, gJ + 1, gI, 3)
+    SK = o.get("SK").reshape(gK + 1, gJ, gI, 3)
+    gvol = o.get("vol").reshape(gK, gJ, gI)
+    o.close()
+    gradU = np.zeros((gK, gJ, gI, 9))
+    for k in range(gK):
+        for j in range(gJ):
+            for i in range(gI):
+                uf = np.array([uI[k, j, i + 1], uI[k, j, i], uJ[k, j + 1, i], uJ[k, j, i], uK[k + 1, j, i], uK[k, j, i]])
+                sf = np.array([SI[k, j, i + 1], -SI[k, j, i], SJ[k, j + 1, i], -SJ[k, j, i], SK[k + 1, j, i], -SK[k, j, i]])
+                ref.ref_grad_tensor(p(uf), p(sf), float(gvol[k, j, i]), p(gradU[k, j, i]))
     ib_nodes, ib_r, ib_c = ib_case()
     solid, ghosts, stencils = ib_reference(ref, ib_nodes, ib_r, ib_c)
-    ib = {"ib_solid": solid, "ib_ghosts": ghosts, "ib_stencils": stencils}
+    ib = {"ib_solid": solid, "ib_ghosts": ghosts, "ib_stencils": stencils, "skewed_step1_gradU": gradU}
     np.savez(os.path.join(HERE, "reference_geometry.npz"), hexes=H, volume=vol, centroid=cen, faces=faces, face_area=area,
              sphere=sph, nearest=near, array3d_dims=np.array(dims), array3d_cells=cells, array3d_offsets=offs, **mesh, **ib)
     print("wrote", os.path.join(HERE, "reference_geometry.npz"))

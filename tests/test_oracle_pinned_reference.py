@@ -169,6 +169,15 @@ def test_oracle_matches_the_reference_golden_geometry():
     assert np.array_equal(g["ib_solid"].ravel(), status != 0)
     assert np.array_equal(g["ib_ghosts"], np.flatnonzero(status == 1))
     assert np.array_equal(g["ib_stencils"], stencil)
+    # velocity-gradient tensors after one step of the sheared, jittered cavity
+    import sys
+    sys.path.insert(0, HERE)
+    from helpers import small_skewed
+    nodes, spec = small_skewed()
+    s = O.OracleSolver(nodes, spec)
+    s.solve()
+    assert np.array_equal(s.get("gradU").reshape(g["skewed_step1_gradU"].shape), g["skewed_step1_gradU"])
+    s.close()
 
 
 def test_mesh_metric_arrays_are_the_references(libs):
@@ -291,3 +300,38 @@ def test_immersed_boundary_geometry_is_the_references(libs):
     assert np.array_equal(solid.ravel(), status != 0)
     assert np.array_equal(np.flatnonzero(status == 1), ghosts) and len(ghosts) > 0
     assert np.array_equal(stencil, stencils)
+
+
+def test_velocity_gradient_tensor_is_the_references(libs):
+    """The cell velocity gradient of the non-orthogonal correction, sum_f u_f (x) S_f / V
+    (FvVectorScheme.cpp:64-69), from the oracle's face velocities after a step on a sheared,
+    jittered cavity, equals the reference's Vector3D / Tensor3D arithmetic bit for bit."""
+    import sys
+    sys.path.insert(0, HERE)
+    from helpers import small_skewed
+    ref, _ = libs
+    dp = ctypes.POINTER(ctypes.c_double)
+    ref.ref_grad_tensor.argtypes = [dp, dp, ctypes.c_double, dp]
+    nodes, spec = small_skewed()
+    assert spec.nonorth
+    s = O.OracleSolver(nodes, spec)
+    s.solve()
+    nK, nJ, nI = (d - 1 for d in nodes.shape[:3])
+    gU = s.get("gradU").reshape(nK, nJ, nI, 9)
+    uI = s.get("uFaceI").reshape(nK, nJ, nI + 1, 3)
+    uJ = s.get("uFaceJ").reshape(nK, nJ + 1, nI, 3)
+    uK = s.get("uFaceK").reshape(nK + 1, nJ, nI, 3)
+    SI = s.get("SI").reshape(nK, nJ, nI + 1, 3)
+    SJ = s.get("SJ").reshape(nK, nJ + 1, nI, 3)
+    SK = s.get("SK").reshape(nK + 1, nJ, nI, 3)
+    vol = s.get("vol").reshape(nK, nJ, nI)
+    s.close()
+    assert np.abs(gU).max() > 0
+    for k in range(nK):
+        for j in range(nJ):
+            for i in range(nI):
+                uf = np.array([uI[k, j, i + 1], uI[k, j, i], uJ[k, j + 1, i], uJ[k, j, i], uK[k + 1, j, i], uK[k, j, i]])
+                sf = np.array([SI[k, j, i + 1], -SI[k, j, i], SJ[k, j + 1, i], -SJ[k, j, i], SK[k + 1, j, i], -SK[k, j, i]])
+                out = np.zeros(9)
+                ref.ref_grad_tensor(_p(uf), _p(sf), float(vol[k, j, i]), _p(out))
+                assert np.array_equal(out, gU[k, j, i]), (i, j, k)
