@@ -40,6 +40,7 @@ class CaffeCase(ctypes.Structure):
         ("ib_radius", ctypes.c_double), ("ib_center", ctypes.c_double * 3),
         ("u_init", ctypes.c_double * 3), ("p_init", ctypes.c_double),
         ("p_form", ctypes.c_int),
+        ("mom_atol", ctypes.c_double), ("p_atol", ctypes.c_double),
     ]
 
 
@@ -145,6 +146,7 @@ def make_case(spec: C.CaseSpec) -> CaffeCase:
         c.u_init[q] = float(spec.u_init[q])
     c.p_init = float(spec.p_init)
     c.p_form = C.P_FORMS[spec.p_form]
+    c.mom_atol, c.p_atol = float(spec.mom_atol), float(spec.p_atol)
     return c
 
 

@@ -58,6 +58,9 @@ class CaseSpec:
     p_init: float = 0.0
     dt: float = 1.0
     p_form: str = "fp64"
+    # absolute floors of the linear solves, ||b - A x|| <= max(rtol ||b||, atol) (PETSc's test)
+    mom_atol: float = 0.0
+    p_atol: float = 0.0
 
     def replace(self, **kw) -> "CaseSpec":
         return dataclasses.replace(self, **kw)
@@ -76,6 +79,8 @@ class CaseSpec:
             raise ValueError(f"unknown pressure-solve form {self.p_form!r}")
         if self.kind == "ibpiso" and self.ib_radius <= 0.0:
             raise ValueError("ibpiso needs a sphere radius > 0")
+        if not (self.mom_atol >= 0.0 and self.p_atol >= 0.0):
+            raise ValueError("absolute tolerances must be >= 0")
 
 
 # ---------------------------------------------------------------------------

@@ -19,6 +19,7 @@ namespace cb {
 
 static thread_local std::string g_err;
 void set_error(const std::string& msg) { g_err = msg; }
+void clear_error() { g_err.clear(); }
 std::string cuda_msg(cudaError_t e, const char* what, const char* file, int line) {
     return std::string(what) + " failed: " + cudaGetErrorString(e) + " (" + file + ":" + std::to_string(line) + ")";
 }
@@ -293,6 +294,13 @@ int setup_bcs(caffe_dev* h) {
     return 0;
 }
 
+// The reference preconditions with PETSc's lexicographic symmetric SOR sweep
+// (src/Math/SparseMatrix.cpp:95-100), which is sequential row by row; the device does not
+// substitute another preconditioner for it silently.
+const char* const SGS_UNAVAILABLE =
+    "BiCGStab with symmetric Gauss-Seidel (the reference's PETSc PCSOR) is a sequential sweep and is not "
+    "implemented on the device: choose CAFFE_KSP_BICGSTAB_JACOBI or CAFFE_KSP_CG_JACOBI";
+
 int validate_case(const caffe_case* c) {
     if (!c) { set_error("case is NULL"); return 1; }
     if (c->kind < 0 || c->kind > 2) { set_error("invalid solver kind"); return 1; }
@@ -301,6 +309,15 @@ int validate_case(const caffe_case* c) {
     if (c->n_pcorr < 1 && c->kind != CAFFE_SIMPLE) { set_error("numberOfPressureCorrections must be >= 1"); return 1; }
     if (c->convection < 0 || c->convection > 1) { set_error("invalid convection scheme"); return 1; }
     if (c->mom_method == CAFFE_KSP_CG_JACOBI) { set_error("the momentum matrix is not symmetric: CG cannot solve it"); return 1; }
+    if (c->mom_method == CAFFE_KSP_BICGSTAB_SGS || c->p_method == CAFFE_KSP_BICGSTAB_SGS) {
+        set_error(SGS_UNAVAILABLE);
+        return 1;
+    }
+    if (c->mom_method < 0 || c->mom_method > CAFFE_KSP_CG_JACOBI || c->p_method < 0 || c->p_method > CAFFE_KSP_CG_JACOBI) {
+        set_error("invalid Krylov method");
+        return 1;
+    }
+    if (!(c->mom_atol >= 0.) || !(c->p_atol >= 0.)) { set_error("absolute tolerances must be >= 0"); return 1; }
     if (c->maxit < 1) { set_error("maxit must be >= 1"); return 1; }
     if (c->kind == CAFFE_IBPISO && !(c->ib_radius > 0.)) { set_error("IbPiso needs a sphere radius > 0"); return 1; }
     if (c->p_form < 0 || c->p_form > 3) { set_error("invalid pressure-solve form"); return 1; }
@@ -360,7 +377,7 @@ int ph_assemble_momentum(caffe_dev* h, double dt) {
     return launch_momentum_assemble(h->geo(), h->bc, h->fields(), m, h->P, dt, h->st);
 }
 int ph_solve_momentum(caffe_dev* h) {
-    if (ksp_bicgstab(h->momOp(), 3, h->mb, h->u, h->L, h->kw, h->cs.mom_rtol, h->cs.maxit, h->st)) return 1;
+    if (ksp_bicgstab(h->momOp(), 3, h->mb, h->u, h->L, h->kw, h->cs.mom_rtol, h->cs.maxit, h->st, h->cs.mom_atol)) return 1;
     acc_kernel<<<1, 32, 0, h->st>>>(h->kw.out, h->acc, 0, 3);
     CB_CHECK_LAUNCH();
     return 0;
@@ -384,19 +401,20 @@ int ph_solve_pcorr(caffe_dev* h) {
         // reach the tolerance
         if (h->ensure_learned()) return 1;
         rc = learned_solve(h->lw, A, h->ib ? h->status : nullptr, h->pb, h->pc, h->L, h->cs.p_rtol, h->cs.maxit, LEARNED_INNER_RTOL,
-                           project, h->netMode, h->kw.out, h->st);
+                           project, h->netMode, h->kw.out, h->st, h->cs.p_atol);
         if (!rc) rc = ksp_fallback_sym(A, method, h->pb, h->pc, h->L, h->kw, h->cs.p_rtol, h->cs.maxit, h->st, 0,
-                                       &h->kw.out->status[0], &h->acc->fallbacks);
+                                       &h->kw.out->status[0], &h->acc->fallbacks, h->cs.p_atol);
     } else if (h->cs.p_form == CAFFE_P_MIXED) {
         // FP32 inner solves inside FP64 refinement; the plain FP64 solve re-runs on the device
         // when the refinement does not reach the tolerance
-        rc = ksp_mixed_sym(A, method, h->pb, h->pc, h->L, h->kw, h->cs.p_rtol, h->cs.maxit, MIXED_INNER_RTOL, h->st, project);
+        rc = ksp_mixed_sym(A, method, h->pb, h->pc, h->L, h->kw, h->cs.p_rtol, h->cs.maxit, MIXED_INNER_RTOL, h->st, project,
+                           h->cs.p_atol);
         if (!rc) rc = ksp_fallback_sym(A, method, h->pb, h->pc, h->L, h->kw, h->cs.p_rtol, h->cs.maxit, h->st, 0,
-                                       &h->kw.out->status[0], &h->acc->fallbacks);
+                                       &h->kw.out->status[0], &h->acc->fallbacks, h->cs.p_atol);
     } else if (method == CAFFE_KSP_CG_JACOBI) {
-        rc = ksp_cg(A, h->pb, h->pc, h->L, h->kw, h->cs.p_rtol, h->cs.maxit, h->st, project);
+        rc = ksp_cg(A, h->pb, h->pc, h->L, h->kw, h->cs.p_rtol, h->cs.maxit, h->st, project, h->cs.p_atol);
     } else {
-        rc = ksp_bicgstab_sym(A, h->pb, h->pc, h->L, h->kw, h->cs.p_rtol, h->cs.maxit, h->st, project);
+        rc = ksp_bicgstab_sym(A, h->pb, h->pc, h->L, h->kw, h->cs.p_rtol, h->cs.maxit, h->st, project, h->cs.p_atol);
     }
     if (rc) return rc;
     if (project) {
@@ -975,6 +993,8 @@ int caffe_ksp7_solve_device(int nI, int nJ, int nK, const double* d_coef7, const
     g_err.clear();
     if (nI < 1 || nJ < 1 || nK < 1 || !d_coef7 || !d_b || !d_x) { set_error("invalid arguments"); return 1; }
     if (maxit < 1) { set_error("maxit must be >= 1"); return 1; }
+    if (method == CAFFE_KSP_BICGSTAB_SGS) { set_error(SGS_UNAVAILABLE); return 1; }
+    if (method != CAFFE_KSP_BICGSTAB_JACOBI && method != CAFFE_KSP_CG_JACOBI) { set_error("invalid Krylov method"); return 1; }
     cudaStream_t st = (cudaStream_t)stream;
     Lat L = make_lat(nI, nJ, nK);
     std::vector<void*> tmp;

@@ -22,6 +22,7 @@ namespace cb {
 
 // ---------------------------------------------------------------- error handling
 void set_error(const std::string& msg);
+void clear_error();
 std::string cuda_msg(cudaError_t e, const char* what, const char* file, int line);
 
 #define CB_CUDA(call)                                                                   \

@@ -184,6 +184,7 @@ struct KArgs {
     KspOut* out;
     long long N, PS;
     double rtol;
+    double atol;   // absolute floor: converged when ||b - A x|| <= max(rtol ||b||, atol)
     int maxit;
     int project;   // remove the mean of b first (singular all-Neumann pressure systems)
     // fallback mode: when skip_if_ok is set the launch returns at once unless the status
@@ -201,6 +202,9 @@ __device__ __forceinline__ void project_mean(cg::grid_group& grid, double* b, lo
     grid_reduce<1>(grid, s, partials, par, tot);
     double mean = tot[0] / (double)N;
     for (long long c = t0; c < N; c += T) b[c] = b[c] - mean;
+    // the projected b is read at stencil neighbours owned by other blocks right after this
+    // (CG forms w = A D^-1 b): every block's subtraction must be visible first
+    grid.sync();
 }
 
 // ------------------------------------------------------------------ BiCGStab
@@ -244,11 +248,13 @@ __global__ void __launch_bounds__(KB) bicgstab_kernel(Op A, KArgs a) {
     double relres[NR];
 #pragma unroll
     for (int q = 0; q < NR; ++q) {
-        done[q] = !(bb[q] > 0.);
-        if (bb[q] != bb[q]) status[q] = 3; else status[q] = 0;
         rho[q] = bb[q]; rho_old[q] = 1.; alpha[q] = 1.; omega[q] = 1.;
-        tol2[q] = a.rtol * a.rtol * bb[q];
+        tol2[q] = fmax(a.rtol * a.rtol * bb[q], a.atol * a.atol);
         it[q] = 0; fresh[q] = true; needT[q] = false; relres[q] = 0.;
+        // x = 0 already meets the absolute floor: nothing to do (relative residual 1)
+        done[q] = !(bb[q] > 0.) || bb[q] <= tol2[q];
+        if (bb[q] > 0. && done[q]) relres[q] = 1.;
+        if (bb[q] != bb[q]) status[q] = 3; else status[q] = 0;
     }
     int cur = 0;
     while (true) {
@@ -443,11 +449,12 @@ __global__ void __launch_bounds__(KB, 4) cg1_kernel(Op A, KArgs a) {
     double tot[3];
     grid_reduce<3>(grid, acc, a.partials, par, tot);
     double gamma = tot[0], bb = tot[2];
-    double tol2 = a.rtol * a.rtol * bb;
+    double tol2 = fmax(a.rtol * a.rtol * bb, a.atol * a.atol);
     double alpha = tot[1] != 0. ? gamma / tot[1] : 0., beta = 0.;
     int it = 0, status = 0;
     double relres = 0.;
-    bool done = !(bb > 0.);
+    bool done = !(bb > 0.) || bb <= tol2;   // x = 0 already meets the absolute floor
+    if (bb > 0. && done) relres = 1.;
     if (bb != bb) status = 3;
     while (!done) {
         const double* r0 = rC;
@@ -582,6 +589,7 @@ struct MxArgs {
     KspOut* out;
     long long N;
     double rtol;
+    double atol;
     int maxit;
     double eta;
     int project;
@@ -605,7 +613,7 @@ __global__ void __launch_bounds__(KB, 4) mixed_kernel(Op64 A, OpSymF Af, MxArgs 
     }
     double tot1[1];
     grid_reduce<1>(grid, acc1, a.partials, par, tot1);
-    double bb = tot1[0], tol2 = a.rtol * a.rtol * bb;
+    double bb = tot1[0], tol2 = fmax(a.rtol * a.rtol * bb, a.atol * a.atol);
     int status = 0, inner_total = 0, outer = 0;
     double relres = 0.;
     bool done = !(bb > 0.);
@@ -631,7 +639,7 @@ __global__ void __launch_bounds__(KB, 4) mixed_kernel(Op64 A, OpSymF Af, MxArgs 
         ++outer;
         // inner target: as deep as FP32 allows on the first pass, then only the factor still
         // missing to the outer tolerance (with a safety margin)
-        double eta = 0.25 * a.rtol * sqrt(bb / rr);
+        double eta = 0.25 * sqrt(tol2 / rr);
         if (eta < a.eta) eta = a.eta;
         if (eta > 0.5) eta = 0.5;
         // ---- FP32 inner solve A32 e = r (e from zero), dots and norms in FP64
@@ -780,12 +788,12 @@ static int launch_coop(K kernel, int grid, KArgs& args, const void* op, cudaStre
     return 0;
 }
 
-static KArgs make_args(const Lat& L, const KspWork& w, const double* b, double* x, double rtol, int maxit) {
+static KArgs make_args(const Lat& L, const KspWork& w, const double* b, double* x, double rtol, int maxit, double atol) {
     KArgs a;
     a.b = b; a.x = x; a.r = w.r; a.rp = w.rp;
     a.p[0] = w.p[0]; a.p[1] = w.p[1]; a.v[0] = w.v[0]; a.v[1] = w.v[1];
     a.t = w.t; a.invD = w.invD; a.partials = w.partials; a.out = w.out;
-    a.N = L.N; a.PS = L.PS; a.rtol = rtol; a.maxit = maxit;
+    a.N = L.N; a.PS = L.PS; a.rtol = rtol; a.atol = atol; a.maxit = maxit;
     a.project = 0;
     a.skip_if_ok = nullptr;
     a.fallbacks = nullptr;
@@ -793,10 +801,10 @@ static KArgs make_args(const Lat& L, const KspWork& w, const double* b, double* 
 }
 
 int ksp_bicgstab(const Op7& A, int nr, const double* b, double* x, const Lat& L, const KspWork& w, double rtol, int maxit,
-                 cudaStream_t st) {
+                 cudaStream_t st, double atol) {
     inv_diag_kernel<Op7><<<grid_for(L.N, 256), 256, 0, st>>>(A, L.N, w.invD);
     CB_CHECK_LAUNCH();
-    KArgs a = make_args(L, w, b, x, rtol, maxit);
+    KArgs a = make_args(L, w, b, x, rtol, maxit, atol);
     if (nr == 3) {
         static int G = 0;
         if (!G) G = coop_grid(bicgstab_kernel<3, Op7>);
@@ -808,10 +816,10 @@ int ksp_bicgstab(const Op7& A, int nr, const double* b, double* x, const Lat& L,
 }
 
 int ksp_bicgstab_sym(const OpSym& A, const double* b, double* x, const Lat& L, const KspWork& w, double rtol, int maxit,
-                     cudaStream_t st, int project) {
+                     cudaStream_t st, int project, double atol) {
     inv_diag_kernel<OpSym><<<grid_for(L.N, 256), 256, 0, st>>>(A, L.N, w.invD);
     CB_CHECK_LAUNCH();
-    KArgs a = make_args(L, w, b, x, rtol, maxit);
+    KArgs a = make_args(L, w, b, x, rtol, maxit, atol);
     a.project = project;
     static int G = 0;
     if (!G) G = coop_grid(bicgstab_kernel<1, OpSym>);
@@ -819,20 +827,21 @@ int ksp_bicgstab_sym(const OpSym& A, const double* b, double* x, const Lat& L, c
 }
 
 int ksp_cg(const OpSym& A, const double* b, double* x, const Lat& L, const KspWork& w, double rtol, int maxit, cudaStream_t st,
-           int project) {
+           int project, double atol) {
     inv_diag_kernel<OpSym><<<grid_for(L.N, 256), 256, 0, st>>>(A, L.N, w.invD);
     CB_CHECK_LAUNCH();
-    KArgs a = make_args(L, w, b, x, rtol, maxit);
+    KArgs a = make_args(L, w, b, x, rtol, maxit, atol);
     a.project = project;
     static int G = 0;
     if (!G) G = coop_grid(cg1_kernel<OpSym>);
     return launch_coop(cg1_kernel<OpSym>, G, a, &A, st);
 }
 
-int ksp_cg7(const Op7& A, const double* b, double* x, const Lat& L, const KspWork& w, double rtol, int maxit, cudaStream_t st) {
+int ksp_cg7(const Op7& A, const double* b, double* x, const Lat& L, const KspWork& w, double rtol, int maxit, cudaStream_t st,
+            double atol) {
     inv_diag_kernel<Op7><<<grid_for(L.N, 256), 256, 0, st>>>(A, L.N, w.invD);
     CB_CHECK_LAUNCH();
-    KArgs a = make_args(L, w, b, x, rtol, maxit);
+    KArgs a = make_args(L, w, b, x, rtol, maxit, atol);
     static int G = 0;
     if (!G) G = coop_grid(cg1_kernel<Op7>);
     return launch_coop(cg1_kernel<Op7>, G, a, &A, st);
@@ -843,13 +852,14 @@ int krylov_grid_size(int which) {
         case 0: return coop_grid(bicgstab_kernel<3, Op7>);
         case 1: return coop_grid(bicgstab_kernel<1, OpSym>);
         case 2: return coop_grid(cg1_kernel<OpSym>);
+        case 4: return coop_grid(cg1_kernel<Op7>);
         default: return coop_grid(bicgstab_kernel<1, Op7>);
     }
 }
 
 
 int ksp_mixed_sym(const OpSym& A, int method, const double* b, double* x, const Lat& L, const KspWork& w, double rtol, int maxit,
-                  double inner_rtol, cudaStream_t st, int project) {
+                  double inner_rtol, cudaStream_t st, int project, double atol) {
     cast_sym_kernel<<<grid_for(L.N, 256), 256, 0, st>>>(A, L.N, w.fA[0], w.fA[1], w.fA[2], w.fA[3], w.finvD);
     CB_CHECK_LAUNCH();
     OpSymF Af;
@@ -859,7 +869,7 @@ int ksp_mixed_sym(const OpSym& A, int method, const double* b, double* x, const 
     m.b = b; m.x = x;
     m.r[0] = w.fr[0]; m.r[1] = w.fr[1]; m.w[0] = w.fw[0]; m.w[1] = w.fw[1]; m.s[0] = w.fs[0]; m.s[1] = w.fs[1];
     m.p = w.fp; m.e = w.fe; m.v[0] = w.fv[0]; m.v[1] = w.fv[1]; m.t = w.ft; m.invD = w.finvD;
-    m.partials = w.partials; m.out = w.out; m.N = L.N; m.rtol = rtol; m.maxit = maxit; m.eta = inner_rtol;
+    m.partials = w.partials; m.out = w.out; m.N = L.N; m.rtol = rtol; m.atol = atol; m.maxit = maxit; m.eta = inner_rtol;
     m.project = project; m.inner_max = 100000;
     void* params[3] = {const_cast<OpSym*>(&A), &Af, &m};
     if (method == CAFFE_KSP_CG_JACOBI_INT) {
@@ -875,11 +885,11 @@ int ksp_mixed_sym(const OpSym& A, int method, const double* b, double* x, const 
 }
 
 int ksp_fallback_sym(const OpSym& A, int method, const double* b, double* x, const Lat& L, const KspWork& w, double rtol, int maxit,
-                     cudaStream_t st, int project, const int* status, int* fallbacks) {
+                     cudaStream_t st, int project, const int* status, int* fallbacks, double atol) {
     // plain FP64 re-solve from zero, executed only when *status (the previous solve's) is non-zero
     inv_diag_kernel<OpSym><<<grid_for(L.N, 256), 256, 0, st>>>(A, L.N, w.invD);
     CB_CHECK_LAUNCH();
-    KArgs a = make_args(L, w, b, x, rtol, maxit);
+    KArgs a = make_args(L, w, b, x, rtol, maxit, atol);
     a.project = project;
     a.skip_if_ok = status;
     a.fallbacks = fallbacks;

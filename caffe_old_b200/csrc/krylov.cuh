@@ -63,24 +63,30 @@ struct KspWork {
     float* ft;
 };
 
+// Every solve stops once ||b - A x|| <= max(rtol ||b||, atol) in the FP64 true residual (the
+// convergence test of PETSc's KSP, rtol and atol; atol = 0 leaves the relative test alone).
 int ksp_bicgstab(const Op7& A, int nr, const double* b, double* x, const Lat& L, const KspWork& w, double rtol, int maxit,
-                 cudaStream_t st);
+                 cudaStream_t st, double atol = 0.);
 // project != 0: remove the mean of b first (b is modified), for singular all-Neumann systems
 int ksp_bicgstab_sym(const OpSym& A, const double* b, double* x, const Lat& L, const KspWork& w, double rtol, int maxit,
-                     cudaStream_t st, int project = 0);
+                     cudaStream_t st, int project = 0, double atol = 0.);
 int ksp_cg(const OpSym& A, const double* b, double* x, const Lat& L, const KspWork& w, double rtol, int maxit, cudaStream_t st,
-           int project = 0);
-int ksp_cg7(const Op7& A, const double* b, double* x, const Lat& L, const KspWork& w, double rtol, int maxit, cudaStream_t st);
+           int project = 0, double atol = 0.);
+int ksp_cg7(const Op7& A, const double* b, double* x, const Lat& L, const KspWork& w, double rtol, int maxit, cudaStream_t st,
+            double atol = 0.);
 // FP64 iterative refinement around FP32 inner solves on the symmetric p' operator: CG inner
 // (method CAFFE_KSP_CG_JACOBI, symmetric systems) or BiCGStab inner (ghost rows).
 // inner_rtol: relative reduction each inner solve aims for.  out->iters counts inner
 // iterations; the outer count goes to *outer_iters (device int, may be null).
 int ksp_mixed_sym(const OpSym& A, int method, const double* b, double* x, const Lat& L, const KspWork& w, double rtol, int maxit,
-                  double inner_rtol, cudaStream_t st, int project);
+                  double inner_rtol, cudaStream_t st, int project, double atol = 0.);
 // Plain FP64 re-solve that runs only when *status is non-zero (the fallback of a mixed or
 // learned solve), decided on the device without a host round trip.
 int ksp_fallback_sym(const OpSym& A, int method, const double* b, double* x, const Lat& L, const KspWork& w, double rtol, int maxit,
-                     cudaStream_t st, int project, const int* status, int* fallbacks);
+                     cudaStream_t st, int project, const int* status, int* fallbacks, double atol = 0.);
+// Blocks of the cooperative grid a solve launches: 0 BiCGStab on 3 right-hand sides (Op7),
+// 1 BiCGStab (OpSym), 2 CG (OpSym), 3 BiCGStab (Op7), 4 CG (Op7).  The block partials of a
+// solve take 2 x grid x 8 doubles.
 int krylov_grid_size(int which);
 
 }  // namespace cb

@@ -1062,7 +1062,7 @@ int fg_alloc(LearnedWork& lw, int m) {
 }  // namespace
 
 int learned_solve(LearnedWork& lw, const OpSym& A, const uint8_t* status, const double* b, double* x, const Lat& L, double rtol, int maxit,
-                  double eta, int project, int mode, KspOut* out, cudaStream_t st) {
+                  double eta, int project, int mode, KspOut* out, cudaStream_t st, double atol) {
     const long long N = L.N;
     const int nb = nblocks(N);
     const int G = grid_for(N, 256);
@@ -1109,7 +1109,7 @@ int learned_solve(LearnedWork& lw, const OpSym& A, const uint8_t* status, const 
         Scal* hs = static_cast<Scal*>(lw.hostScal);
         if (outer == 0) {
             // the tolerance needs ||b||^2: the first outer residual (x = 0) is b itself
-            double tol2 = rtol * rtol * hs->bb;
+            double tol2 = std::max(rtol * rtol * hs->bb, atol * atol);
             bool fin = hs->rr64 <= tol2 || !(hs->bb > 0.);
             CB_CUDA(cudaMemcpyAsync(&S->tol2, &tol2, sizeof(double), cudaMemcpyHostToDevice, st));
             if (fin) {
@@ -1123,7 +1123,7 @@ int learned_solve(LearnedWork& lw, const OpSym& A, const uint8_t* status, const 
         // inner target: deep first, then only the factor still missing
         double etaK = eta;
         if (hs->bb > 0. && hs->rr64 > 0.) {
-            double need = 0.25 * rtol * sqrt(hs->bb / hs->rr64);
+            double need = 0.25 * sqrt(std::max(rtol * rtol * hs->bb, atol * atol) / hs->rr64);
             if (need > etaK) etaK = need;
         }
         if (etaK > 0.5) etaK = 0.5;

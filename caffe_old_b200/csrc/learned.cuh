@@ -82,7 +82,7 @@ void learned_free_host(LearnedWork& lw);
 //   y_l = R_l D^-1 r / s (mode LEVELS), nothing (mode JACOBI).
 // Writes iterations / outer passes / relative residual / status to *out (device).
 int learned_solve(LearnedWork& lw, const OpSym& A, const uint8_t* status, const double* b, double* x, const Lat& L, double rtol,
-                  int maxit, double eta, int project, int mode, KspOut* out, cudaStream_t st);
+                  int maxit, double eta, int project, int mode, KspOut* out, cudaStream_t st, double atol = 0.);
 // Train the network on pairs (b, x*) stored as FP32 halo-padded planes [n][PS] in device memory.
 int learned_train(LearnedWork& lw, const OpSym& A, const uint8_t* status, const Lat& L, const float* pairsB, const float* pairsX,
                   int nPairs, int steps, int batch, float lr, unsigned seed, float* lossHost, cudaStream_t st);

@@ -33,7 +33,9 @@ namespace cb {
 namespace {
 
 constexpr size_t SCRATCH_BYTES = size_t(16) << 20;
-constexpr size_t PARTIAL_BYTES = size_t(128) << 10;   // 2 x 8 x 1024 doubles of block partials
+// 2 buffers x 8 doubles x up to 1024 blocks of partials: the cooperative grid is capped at 4
+// blocks per SM, so this covers GPUs of up to 256 SMs (B200: 148); checked per call
+constexpr size_t PARTIAL_BYTES = size_t(128) << 10;
 constexpr int MAX_DEVICES = 64;
 
 static __device__ __align__(256) unsigned char g_ksp_scratch[SCRATCH_BYTES];
@@ -69,8 +71,13 @@ using namespace cb;
 
 extern "C" int caffe_ksp7_solve_device_noalloc(int nI, int nJ, int nK, const double* d_coef7, const double* d_b, double* d_x,
                                                int method, double rtol, int maxit, void* stream, int* iters, double* rel_res) {
+    clear_error();
     if (nI < 1 || nJ < 1 || nK < 1 || !d_coef7 || !d_b || !d_x) { set_error("invalid arguments"); return 1; }
     if (maxit < 1) { set_error("maxit must be >= 1"); return 1; }
+    if (method != CAFFE_KSP_BICGSTAB_JACOBI && method != CAFFE_KSP_CG_JACOBI) {
+        set_error("caffe_ksp7_solve_device_noalloc: only CAFFE_KSP_BICGSTAB_JACOBI and CAFFE_KSP_CG_JACOBI run on the device");
+        return 1;
+    }
     Lat L = make_lat(nI, nJ, nK);
     // workspace: b and x copies, r (2 planes), rp, p[2], v[2], t, invD -- 11 halo-padded planes
     // planes are packed at exactly one plane stride (PS doubles): the CG's second r buffer is
@@ -82,6 +89,14 @@ extern "C" int caffe_ksp7_solve_device_noalloc(int nI, int nJ, int nK, const dou
         set_error("caffe_ksp7_solve_device_noalloc: a " + std::to_string(nI) + "x" + std::to_string(nJ) + "x" +
                   std::to_string(nK) + " lattice needs " + std::to_string(need) + " bytes of workspace, more than the " +
                   std::to_string(SCRATCH_BYTES) + " the no-allocation solver holds; use caffe_ksp7_solve_device");
+        return 1;
+    }
+    // the block partials of the cooperative solve (2 buffers x grid x 8 doubles) must fit their
+    // fixed slice: the grid is at most 4 blocks per SM
+    const int grid = krylov_grid_size(method == CAFFE_KSP_CG_JACOBI ? 4 : 3);
+    if ((size_t)2 * grid * 8 * sizeof(double) > PARTIAL_BYTES) {
+        set_error("caffe_ksp7_solve_device_noalloc: the solver's grid of " + std::to_string(grid) +
+                  " blocks needs more block-partial space than the no-allocation workspace holds");
         return 1;
     }
     void* base = nullptr;

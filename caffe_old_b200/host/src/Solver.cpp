@@ -7,6 +7,7 @@
 //   Solver.nonOrthogonalCorrection     OFF (the reference) | ON
 //   LinearSolvers.momentum / .pressureCorrection   bicgstab_jacobi | cg_jacobi
 //   LinearSolvers.tolerance            relative true residual (default 1e-8)
+//   LinearSolvers.absoluteTolerance    absolute floor of ||b - A x|| (PETSc's atol; default 0)
 //   LinearSolvers.maxIterations        (default 20000)
 //   LinearSolvers.pressureCorrectionForm   fp64 | mixed | learned | learned_mixed
 //   LearnedPreconditioner.mode         levels | network | jacobi
@@ -106,6 +107,7 @@ caffe_case Solver::caseFromInput(const Input& input, int kind) {
     cs.mom_method = ksp_method(c.get<std::string>("LinearSolvers.momentum", std::string("bicgstab_jacobi")));
     cs.p_method = ksp_method(c.get<std::string>("LinearSolvers.pressureCorrection", std::string("bicgstab_jacobi")));
     cs.mom_rtol = cs.p_rtol = c.get<double>("LinearSolvers.tolerance", 1e-8);
+    cs.mom_atol = cs.p_atol = c.get<double>("LinearSolvers.absoluteTolerance", 0.);
     cs.maxit = c.get<int>("LinearSolvers.maxIterations", 20000);
     cs.p_form = p_form(c.get<std::string>("LinearSolvers.pressureCorrectionForm", std::string("fp64")));
     if (kind == CAFFE_IBPISO) {

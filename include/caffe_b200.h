@@ -52,6 +52,12 @@ typedef struct caffe_case {
     double u_init[3];       /* uniform initial u (InitialConditions, uniform) */
     double p_init;          /* uniform initial p */
     int p_form;             /* caffe_p_form */
+    /* Absolute floors of the momentum and p' solves: a solve stops once
+     * ||b - A x||_2 <= max(rtol ||b||_2, atol), the convergence test of PETSc's KSP, whose
+     * defaults the reference keeps (atol 1e-50, src/Math/SparseMatrix.cpp:95-105).  0 leaves
+     * the relative test alone.  A right-hand side that is round-off noise (the second PISO
+     * corrector of a converged first one) meets a floor at its round-off level at once. */
+    double mom_atol, p_atol;
 } caffe_case;
 
 /* Per-step statistics (what Simple::displayUpdateMessage prints, Simple.cpp:93-100, plus

@@ -674,9 +674,11 @@ static double trueRelRes(const Rows& A, const std::vector<double>& b, const std:
     return bn == 0. ? 0. : std::sqrt(dotv(r, r)) / bn;
 }
 
-// BiCGStab right-preconditioned with Jacobi; tests ||b - A x|| <= rtol ||b|| on the
-// recursive residual and confirms with the true residual, restarting from it.
-static KspStats bicgstabJacobi(const Rows& A, const std::vector<double>& b, std::vector<double>& x, double rtol, int maxit) {
+// BiCGStab right-preconditioned with Jacobi; tests ||b - A x|| <= max(rtol ||b||, atol) (the
+// test of PETSc's KSPConvergedDefault, with its rtol and atol) on the recursive residual and
+// confirms with the true residual, restarting from it.
+static KspStats bicgstabJacobi(const Rows& A, const std::vector<double>& b, std::vector<double>& x, double rtol, int maxit,
+                               double atol) {
     int n = A.n;
     std::vector<double> idg(n), r(n), rp(n), p(n), v(n), s(n), t(n), ph(n), sh(n);
     for (int q = 0; q < n; ++q) { double dg = A.diag(q); idg[q] = dg != 0. ? 1. / dg : 1.; }
@@ -684,6 +686,8 @@ static KspStats bicgstabJacobi(const Rows& A, const std::vector<double>& b, std:
     double bn = std::sqrt(dotv(b, b));
     KspStats st{0, 0., 0};
     if (bn == 0.) return st;
+    const double tol = std::max(rtol * bn, atol);
+    if (bn <= tol) { st.rel_res = 1.; return st; }   // x = 0 already meets the absolute floor
     int it = 0;
     r = b;
     double rnorm = bn;
@@ -710,20 +714,20 @@ static KspStats bicgstabJacobi(const Rows& A, const std::vector<double>& b, std:
             omega = tt == 0. ? 0. : dotv(t, s) / tt;
             for (int q = 0; q < n; ++q) { x[q] += alpha * ph[q] + omega * sh[q]; r[q] = s[q] - omega * t[q]; }
             rnorm = std::sqrt(dotv(r, r));
-            if (rnorm <= rtol * bn) break;
+            if (rnorm <= tol) break;
             if (omega == 0.) { restart = true; break; }
             rho_old = rho;
         }
         double tr = trueRelRes(A, b, x, r);
         rnorm = tr * bn;
-        if (tr <= rtol) { st.iters = it; st.rel_res = tr; return st; }
+        if (rnorm <= tol) { st.iters = it; st.rel_res = tr; return st; }
         (void)restart;
     }
     st.iters = it; st.rel_res = rnorm / bn; st.status = 1;
     return st;
 }
 
-static KspStats cgJacobi(const Rows& A, const std::vector<double>& b, std::vector<double>& x, double rtol, int maxit) {
+static KspStats cgJacobi(const Rows& A, const std::vector<double>& b, std::vector<double>& x, double rtol, int maxit, double atol) {
     int n = A.n;
     std::vector<double> idg(n), r(n), z(n), p(n), q(n);
     for (int i = 0; i < n; ++i) { double dg = A.diag(i); idg[i] = dg != 0. ? 1. / dg : 1.; }
@@ -731,6 +735,8 @@ static KspStats cgJacobi(const Rows& A, const std::vector<double>& b, std::vecto
     double bn = std::sqrt(dotv(b, b));
     KspStats st{0, 0., 0};
     if (bn == 0.) return st;
+    const double tol = std::max(rtol * bn, atol);
+    if (bn <= tol) { st.rel_res = 1.; return st; }   // x = 0 already meets the absolute floor
     r = b;
     int it = 0;
     double rnorm = bn;
@@ -747,23 +753,26 @@ static KspStats cgJacobi(const Rows& A, const std::vector<double>& b, std::vecto
             for (int i = 0; i < n; ++i) { x[i] += alpha * p[i]; r[i] -= alpha * q[i]; z[i] = idg[i] * r[i]; }
             double rzn = dotv(r, z);
             rnorm = std::sqrt(dotv(r, r));
-            if (rnorm <= rtol * bn) break;
+            if (rnorm <= tol) break;
             double beta = rzn / rz;
             rz = rzn;
             for (int i = 0; i < n; ++i) p[i] = z[i] + beta * p[i];
         }
         double tr = trueRelRes(A, b, x, r);
         rnorm = tr * bn;
-        if (tr <= rtol) { st.iters = it; st.rel_res = tr; return st; }
+        if (rnorm <= tol) { st.iters = it; st.rel_res = tr; return st; }
     }
     st.iters = it; st.rel_res = rnorm / bn; st.status = 1;
     return st;
 }
 
-static KspStats kspSolve(int method, const Rows& A, const std::vector<double>& b, std::vector<double>& x, double rtol, int maxit) {
-    if (method == K_BICGSTAB_SGS) return bicgstabSgs(A, b, x, rtol, 1e-50, maxit);
-    if (method == K_BICGSTAB_JACOBI) return bicgstabJacobi(A, b, x, rtol, maxit);
-    return cgJacobi(A, b, x, rtol, maxit);
+// atol: absolute floor of the stopping test; the reference leaves PETSc's default 1e-50
+// (src/Math/SparseMatrix.cpp:95-105), which the SGS form keeps when atol is 0.
+static KspStats kspSolve(int method, const Rows& A, const std::vector<double>& b, std::vector<double>& x, double rtol, int maxit,
+                         double atol = 0.) {
+    if (method == K_BICGSTAB_SGS) return bicgstabSgs(A, b, x, rtol, atol > 0. ? atol : 1e-50, maxit);
+    if (method == K_BICGSTAB_JACOBI) return bicgstabJacobi(A, b, x, rtol, maxit, atol);
+    return cgJacobi(A, b, x, rtol, maxit, atol);
 }
 
 // ----------------------------------------------------------------------------
@@ -905,6 +914,7 @@ struct OracleCase {
     double ib_center[3];
     double u_init[3];
     double p_init;
+    double mom_atol, p_atol;   // absolute floors of the linear solves (0: relative test only)
 };
 }
 
@@ -1129,7 +1139,7 @@ struct Solver {
     }
     void solveMomentum() {  // Simple.cpp:184-207
         for (int comp = 0; comp < 3; ++comp) {
-            momStats[comp] = kspSolve(cs.mom_method, A[0], bv[comp], xv[comp], cs.mom_rtol, cs.maxit);
+            momStats[comp] = kspSolve(cs.mom_method, A[0], bv[comp], xv[comp], cs.mom_rtol, cs.maxit, cs.mom_atol);
             momItersTotal += momStats[comp].iters;
             momResMax = std::max(momResMax, momStats[comp].rel_res);
 #pragma omp parallel for schedule(static)
@@ -1225,7 +1235,7 @@ struct Solver {
             double mean = dotv(bv[0], ones) / (double)bv[0].size();
             for (double& v : bv[0]) v -= mean;
         }
-        pStats = kspSolve(cs.p_method, A[1], bv[0], xv[0], cs.p_rtol, cs.maxit);
+        pStats = kspSolve(cs.p_method, A[1], bv[0], xv[0], cs.p_rtol, cs.maxit, cs.p_atol);
         if (pSingular()) {
             // the solution is defined up to a constant, and on meshes with non-planar faces the
             // discrete gradient (sum of face values times area vectors) is not blind to that
@@ -1694,7 +1704,7 @@ long oracle_array(void* hh, const char* name, double* buf, long count, int dir) 
 // (aP, aE, aW, aN, aS, aT, aB; zero where a neighbour does not exist) on an
 // nI x nJ x nK lattice.  Used to check the device Krylov kernels.
 int oracle_ksp7(int nI, int nJ, int nK, const double* coef7, const double* b, double* x,
-                int method, double rtol, int maxit, int* iters, double* rel_res) {
+                int method, double rtol, int maxit, int* iters, double* rel_res, double atol) {
     int n = nI * nJ * nK;
     orc::Rows A; A.allocate(n, 7);
     for (int k = 0; k < nK; ++k)
@@ -1708,7 +1718,7 @@ int oracle_ksp7(int nI, int nJ, int nK, const double* coef7, const double* b, do
                 A.setRow(c, 7, cols, vals);
             }
     std::vector<double> bb(b, b + n), xx(n, 0.);
-    orc::KspStats st = orc::kspSolve(method, A, bb, xx, rtol, maxit);
+    orc::KspStats st = orc::kspSolve(method, A, bb, xx, rtol, maxit, atol);
     std::memcpy(x, xx.data(), sizeof(double) * n);
     *iters = st.iters; *rel_res = st.rel_res;
     return st.status;

@@ -39,6 +39,7 @@ class OracleCase(ctypes.Structure):
         ("maxit", ctypes.c_int),
         ("ib_radius", ctypes.c_double), ("ib_center", ctypes.c_double * 3),
         ("u_init", ctypes.c_double * 3), ("p_init", ctypes.c_double),
+        ("mom_atol", ctypes.c_double), ("p_atol", ctypes.c_double),
     ]
 
 
@@ -58,7 +59,8 @@ def lib():
         L.oracle_array.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_void_p, ctypes.c_long, ctypes.c_int]
         L.oracle_last_error.restype = ctypes.c_char_p
         L.oracle_ksp7.argtypes = [ctypes.c_int] * 3 + [ctypes.c_void_p] * 3 + [ctypes.c_int, ctypes.c_double, ctypes.c_int,
-                                                                              ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)]
+                                                                              ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double),
+                                                                              ctypes.c_double]
         L.oracle_hex_volume.restype = ctypes.c_double
         L.oracle_hex_volume.argtypes = [ctypes.c_void_p]
         L.oracle_quad_area.restype = ctypes.c_double
@@ -118,6 +120,7 @@ def make_case(spec) -> OracleCase:
         oc.ib_center[q] = float(spec.ib_center[q])
         oc.u_init[q] = float(spec.u_init[q])
     oc.p_init = float(spec.p_init)
+    oc.mom_atol, oc.p_atol = float(spec.mom_atol), float(spec.p_atol)
     return oc
 
 
@@ -307,7 +310,7 @@ class OracleDiffusion:
         L.oracle_diffusion_array(self._h, name.encode(), _ptr(v), n, 1)
 
 
-def ksp7(shape, coef7: np.ndarray, b: np.ndarray, method: str, rtol: float, maxit: int):
+def ksp7(shape, coef7: np.ndarray, b: np.ndarray, method: str, rtol: float, maxit: int, atol: float = 0.0):
     from caffe_old_b200 import cases as C
     nI, nJ, nK = shape
     coef7 = np.ascontiguousarray(coef7, dtype=np.float64)
@@ -316,7 +319,7 @@ def ksp7(shape, coef7: np.ndarray, b: np.ndarray, method: str, rtol: float, maxi
     it = ctypes.c_int(0)
     rr = ctypes.c_double(0.0)
     st = lib().oracle_ksp7(nI, nJ, nK, _ptr(coef7), _ptr(b), _ptr(x), C.KSP_METHODS[method], float(rtol), int(maxit),
-                           ctypes.byref(it), ctypes.byref(rr))
+                           ctypes.byref(it), ctypes.byref(rr), ctypes.c_double(float(atol)))
     return x, it.value, rr.value, st
 
 

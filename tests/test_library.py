@@ -102,9 +102,16 @@ def test_c_abi_rejects_invalid_arguments_before_any_device_call(built):
     bad = [("kind", 7, "invalid solver kind"), ("omega_p", 0.0, "relaxation factors must be positive"),
            ("n_pcorr", 0, "numberOfPressureCorrections must be >= 1"), ("maxit", 0, "maxit must be >= 1"),
            ("mom_method", C.KSP_METHODS["cg_jacobi"], "the momentum matrix is not symmetric: CG cannot solve it"),
-           ("p_form", 9, "invalid pressure-solve form")]
+           ("p_form", 9, "invalid pressure-solve form"),
+           ("p_atol", -1.0, "absolute tolerances must be >= 0")]
     for field, value, msg in bad:
         c = _lib.make_case(spec)
         setattr(c, field, value)
         assert create(c) == (1, msg), field
     assert not h.value
+    # the reference's own preconditioner (PETSc's sequential SOR sweep) is refused, not replaced
+    for field in ("mom_method", "p_method"):
+        c = _lib.make_case(spec)
+        setattr(c, field, C.KSP_METHODS["bicgstab_sgs"])
+        rc, msg = create(c)
+        assert rc == 1 and "symmetric Gauss-Seidel" in msg and "not implemented on the device" in msg

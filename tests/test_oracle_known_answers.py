@@ -138,3 +138,42 @@ def test_sphere_crossing_the_boundary():
     with pytest.raises(RuntimeError, match="outside the cell-centre lattice"):
         o.phase("ib_coeffs")
     o.close()
+
+
+def _neumann_laplacian(shape, seed=5):
+    """7-point p'-like operator with zero row sums (all-Neumann: singular, constant null space)."""
+    rng = np.random.default_rng(seed)
+    nI, nJ, nK = shape
+    N = nI * nJ * nK
+    idx = np.arange(N)
+    i, j, k = idx % nI, (idx // nI) % nJ, idx // (nI * nJ)
+    aE = rng.uniform(0.5, 1.5, N); aN = rng.uniform(0.5, 1.5, N); aT = rng.uniform(0.5, 1.5, N)
+    aE[i == nI - 1] = 0; aN[j == nJ - 1] = 0; aT[k == nK - 1] = 0
+    aW = np.zeros(N); aW[1:] = aE[:-1]; aW[i == 0] = 0
+    aS = np.zeros(N); aS[nI:] = aN[:-nI]; aS[j == 0] = 0
+    aB = np.zeros(N); aB[nI * nJ:] = aT[:-nI * nJ]; aB[k == 0] = 0
+    aP = -(aE + aW + aN + aS + aT + aB)
+    return np.stack([aP, aE, aW, aN, aS, aT, aB])
+
+
+@pytest.mark.parametrize("method", ["cg_jacobi", "bicgstab_jacobi"])
+def test_absolute_floor_accepts_round_off_right_hand_side(method):
+    """A second PISO corrector's right-hand side is round-off (||b|| ~ 1e-19 here), partly along
+    the null space of the singular all-Neumann operator, so no Krylov method can reduce it by a
+    relative 1e-13.  With the absolute floor atol (PETSc's ||r|| <= max(rtol ||b||, atol)) at
+    the round-off level the solve is converged at once (status 0, x = 0); without it, it can
+    only run to maxit."""
+    shape = (9, 7, 5)
+    coef = _neumann_laplacian(shape)
+    rng = np.random.default_rng(11)
+    b = 1e-19 * rng.standard_normal(int(np.prod(shape)))   # mean not removed: inconsistent
+    floor = 1e-16
+    x, it, rr, st = O.ksp7(shape, coef, b, method, 1e-13, 200, atol=floor)
+    assert st == 0 and it == 0 and not np.any(x)
+    x, it, rr, st = O.ksp7(shape, coef, b, method, 1e-13, 200)
+    assert st == 1 and it == 200
+    # a consistent right-hand side far above the floor is still solved to the relative tolerance
+    b = rng.standard_normal(b.size)
+    b -= b.mean()
+    x, it, rr, st = O.ksp7(shape, coef, b, method, 1e-10, 5000, atol=floor)
+    assert st == 0 and rr <= 1e-10 and it > 0
