@@ -27,15 +27,22 @@ def build_oracle() -> str:
     return os.path.join(_ROOT, "oracle", "_build", "liboracle.so")
 
 
-REFERENCE = "/root/reference"
+def reference_root() -> str:
+    """Where the reference's sources are looked for: the oracle recipe's REF (environment variable
+    CAFFE_REFERENCE, else the recipe's default)."""
+    r = subprocess.run(["make", "-C", os.path.join(_ROOT, "oracle"), "-s", "--no-print-directory", "refpath"],
+                       capture_output=True, text=True, check=True)
+    return r.stdout.strip()
 
 
-def build_oracle_ref(reference: str = REFERENCE) -> bool:
-    """The reference's own geometry sources, compiled where they lie into oracle/_ref/ (a pin for
-    the oracle's geometry).  Returns False when the reference sources are not present."""
+def build_oracle_ref(reference: str | None = None) -> bool:
+    """The reference's own geometry sources and its solver path (with stand-in PETSc / MPI /
+    LAPACKE / Boost headers), compiled where they lie into oracle/_ref/: pins for the oracle.
+    Returns False when the reference sources are not present."""
+    reference = reference or reference_root()
     if not os.path.exists(os.path.join(reference, "src", "Math", "Geometry.cpp")):
         return False
-    subprocess.run(["make", "-C", os.path.join(_ROOT, "oracle"), "-s", "ref", f"REF={reference}"], check=True)
+    subprocess.run(["make", "-C", os.path.join(_ROOT, "oracle"), "-s", "-j8", "ref", "refsolver", f"REF={reference}"], check=True)
     return True
 
 

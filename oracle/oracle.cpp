@@ -1598,6 +1598,23 @@ int oracle_phase(void* hh, const char* name, double dt) {
 
 // Scalar statistics: continuity, courant, momentum iterations (sum of 3), last p' iterations,
 // total p' iterations, p' solves, worst p' relative residual, worst momentum residual, ghosts, rows
+// The assembled system `which` (0 momentum, 1 pressure correction) as the rows were set, in
+// the row numbering of IndexMap: rows, row width, entries per row, columns, values (row-major,
+// width per row); b receives right-hand side `comp` (the momentum component, 0 for p').  Called
+// with null arrays it returns the row count and width only.  For pinning against the
+// reference's own assembly (its KSPSolve inputs), right after an assemble phase.
+int oracle_system(void* hh, int which, int comp, int* width, int* cnt, int* col, double* val, double* b) {
+    auto* s = static_cast<orc::Solver*>(hh);
+    if (which < 0 || which > 1 || comp < 0 || comp > 2) return -1;
+    const orc::Rows& A = s->A[which];
+    if (width) *width = A.width;
+    if (cnt) std::memcpy(cnt, A.cnt.data(), sizeof(int) * A.cnt.size());
+    if (col) std::memcpy(col, A.col.data(), sizeof(int) * A.col.size());
+    if (val) std::memcpy(val, A.val.data(), sizeof(double) * A.val.size());
+    if (b) std::memcpy(b, s->bv[comp].data(), sizeof(double) * s->bv[comp].size());
+    return A.n;
+}
+
 void oracle_stats(void* hh, double* out) {
     auto* s = static_cast<orc::Solver*>(hh);
     out[0] = s->continuity; out[1] = s->courant; out[2] = s->momItersTotal; out[3] = s->pItersLast;

@@ -61,6 +61,7 @@ def lib():
         L.oracle_ksp7.argtypes = [ctypes.c_int] * 3 + [ctypes.c_void_p] * 3 + [ctypes.c_int, ctypes.c_double, ctypes.c_int,
                                                                               ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double),
                                                                               ctypes.c_double]
+        L.oracle_system.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int] + [ctypes.c_void_p] * 5
         L.oracle_hex_volume.restype = ctypes.c_double
         L.oracle_hex_volume.argtypes = [ctypes.c_void_p]
         L.oracle_quad_area.restype = ctypes.c_double
@@ -193,6 +194,25 @@ class OracleSolver:
         if v.size != n:
             raise ValueError(f"{name}: expected {n} values, got {v.size}")
         L.oracle_array(self._h, name.encode(), _ptr(v), n, 1)
+
+    def system(self, which: int, comp: int = 0):
+        """Assembled system `which` (0 momentum, 1 p') as {row: {col: value}} and right-hand side
+        `comp`, in IndexMap row numbering; read right after the matching assemble phase."""
+        L = lib()
+        width = ctypes.c_int(0)
+        n = L.oracle_system(self._h, which, comp, ctypes.byref(width), None, None, None, None)
+        if n < 0:
+            raise ValueError("invalid system")
+        w = width.value
+        cnt = np.zeros(n, dtype=np.int32)
+        col = np.zeros(n * w, dtype=np.int32)
+        val = np.zeros(n * w, dtype=np.float64)
+        b = np.zeros(n, dtype=np.float64)
+        L.oracle_system(self._h, which, comp, None, _ptr(cnt), _ptr(col), _ptr(val), _ptr(b))
+        rows = []
+        for r in range(n):
+            rows.append({int(col[r * w + p]): float(val[r * w + p]) for p in range(cnt[r])})
+        return rows, b
 
 
 class OracleCoupled:

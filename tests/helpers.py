@@ -17,6 +17,19 @@ KSP_RTOL_IB = 1e-12
 FIELD_RTOL = 1e-10
 
 
+# Configuration 1 exactly (64 x 64 x 1 SIMPLE cavity, Re = 100, upwind, 0.7 / 0.3, 500 outer
+# iterations) with every solve taken to KSP_RTOL; the p' solves also stop at the absolute floor
+# C1_P_ATOL = 1e-13 x the first iteration's ||b|| (9.1e-5).  Without it the relative 1e-13 is
+# below this p' system's round-off floor (condition number ~4e3) once SIMPLE has converged a few
+# decades, and Jacobi-BiCGStab diverges there (iteration ~375) instead of stagnating.
+C1_P_ATOL = 1e-17
+
+
+def c1_parity():
+    nodes, spec, iters = C.config1_cavity2d(n=64)
+    return nodes, spec.replace(mom_rtol=KSP_RTOL, p_rtol=KSP_RTOL, p_atol=C1_P_ATOL), iters
+
+
 def small_cavity2d(n=12, m=10):
     nodes = C.cartesian_nodes((n, m, 1), (1.0, 1.0, 1.0 / n))
     bc, ref = C.lid_cavity_bcs("north", two_d=True)

@@ -16,7 +16,8 @@ from caffe_old_b200._lib import make_case
 from host_cases import write_case
 
 BIN = os.path.join(os.path.dirname(B.__file__), "_build", "bin")
-REF_MODULES = "/root/reference/Modules"
+REF_ROOT = B.reference_root()
+REF_MODULES = os.path.join(REF_ROOT, "Modules")
 
 
 @pytest.fixture(scope="module")
@@ -90,7 +91,7 @@ def test_reference_module_mains_compile_unchanged(tmp_path, host_bins, module):
     assert r.returncode == 0, r.stderr[-2000:]
 
 
-REF_EXAMPLES = "/root/reference/ExampleCases"
+REF_EXAMPLES = os.path.join(REF_ROOT, "ExampleCases")
 
 
 def _example_cases():
