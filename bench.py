@@ -4,19 +4,24 @@ solve taken to a 1e-8 true relative residual (FP64), on one GPU per rank.
 
 Default workload: flow over an immersed-boundary sphere, 384 x 256 x 256 = 25.2M cells,
 Re = 300, IB-PISO (2 inner iterations, 3 pressure corrections), dt = 2e-3, synthetic
-(seeded mesh and case, no dataset), pressure correction in the learned + mixed-precision
-form (FP32 inner Krylov solve with the level-pyramid preconditioner inside FP64 iterative
-refinement).  The same steps from rest are also run with the plain FP64 pressure solve
+(seeded mesh and case, no dataset), pressure correction in the learned + mixed-precision form:
+FP32 flexible Krylov (FGMRES) preconditioned by the level pyramid with the trained BF16
+tensor-core network, inside FP64 iterative refinement; a solve whose network stage stalls
+continues with the pyramid alone (counted as a cascade), and only then with plain FP64 (counted
+as a fallback).  The same steps from rest are also run with the plain FP64 pressure solve
 (--compare-fp64 steps) and both are reported.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
                   [--workload c5|c2|c1|c3] [--p-form learned_mixed|fp64|mixed|learned]
-                  [--precond levels|network|jacobi] [--inner auto|fcg|bicgstab|fgmres]
+                  [--precond network|levels|jacobi] [--inner auto|fcg|bicgstab|fgmres]
                   [--params file.npy] [--size n] [--compare-fp64 K]
 
-One JSON line on rank 0.  --impl reference times the CPU restatement of the reference
-path (the reference itself cannot be built here: it needs MPI, PETSc and Boost) on the
-host cores, on a reduced lattice of the same workload, scaled to the full lattice.
+One JSON line on rank 0.  The CPU numbers (--impl reference, and cpu_baseline in the GPU line)
+time the CPU restatement of the reference path (the reference itself needs MPI, PETSc and Boost,
+which this image lacks) on the host cores.  A step of the 25.2M-cell case does not fit a CPU
+budget of minutes (about 57,000 FP64 Krylov iterations per step), so they time whole steps of the
+same case on a smaller lattice and say so; nothing is extrapolated.  The GPU line adds the GPU on
+that same smaller lattice, and a fully measured 128^3 cavity (configuration 2) on both.
 """
 from __future__ import annotations
 
@@ -75,17 +80,18 @@ def workload(name: str, size: int | None, p_form: str):
     return nodes, spec, label + f"_{p_form}"
 
 
+# the CPU sample of the immersed-sphere case: the same case on a lattice of 72 x 48 x 48 cells
+# (1/152 of the 25.2M cells), small enough for whole plain-FP64 steps on the host cores
+CPU_SAMPLE_SIZE = 48
+
+
 def sample_workload(name: str, size: int | None):
-    """Reduced lattice of the same workload for the CPU baseline (1/512 of the cells for the
-    25M-cell sphere, 1/64 for the cavities)."""
+    """The same case on the smaller lattice the CPU times fully."""
     if name == "c5":
-        full = (384, 256, 256) if not size else (size * 3 // 2, size, size)
-        return workload(name, max(8, full[1] // 8), "fp64"), full
+        return workload(name, CPU_SAMPLE_SIZE, "fp64")
     if name in ("c2", "c3"):
-        n = size or 128
-        return workload(name, max(8, n // 4), "fp64"), (n, n, n)
-    n = size or 64
-    return workload(name, n, "fp64"), (n, n, 1)
+        return workload(name, max(8, (size or 128) // 4), "fp64")
+    return workload(name, size or 64, "fp64")
 
 
 class ClockSampler:
@@ -167,6 +173,8 @@ def barrier(pg):
 
 
 def _oracle_steps(nodes, spec, steps: int, budget_s: float):
+    """Whole steps of the CPU restatement (plain FP64 solves) from rest, on every host core;
+    stops after `steps` or once `budget_s` is spent (at least one step)."""
     from oracle import oracle as O
     O.build()
     threads = os.cpu_count() or 1
@@ -185,24 +193,20 @@ def _oracle_steps(nodes, spec, steps: int, budget_s: float):
     return times, iters, threads
 
 
-def scaled_cpu(args, steps: int, budget_s: float) -> dict:
-    """The CPU restatement of the reference path (oracle, C++ -O2 with OpenMP on every host
-    core) timed on a reduced lattice of the same workload, scaled to the full lattice by
-    cells x Krylov iterations: time per step grows with the cell count and, for these
-    Jacobi-preconditioned Krylov solves, iterations grow with the lattice's linear size."""
-    (nodes, spec, label), full = sample_workload(args.workload, args.size)
-    sample_cells = int(np.prod([d - 1 for d in nodes.shape[:3]]))
-    full_cells = int(np.prod(full))
+def measured_cpu(args, steps: int, budget_s: float) -> dict:
+    """The CPU restatement timed on whole steps of the same case on the smaller CPU lattice:
+    measured, not scaled."""
+    nodes, spec, label = sample_workload(args.workload, args.size)
+    cells = int(np.prod([d - 1 for d in nodes.shape[:3]]))
     times, iters, threads = _oracle_steps(nodes, spec, steps, budget_s)
     t_step = sum(times) / len(times)
-    linear = (full_cells / sample_cells) ** (1.0 / 3.0) if full[2] > 1 else (full_cells / sample_cells) ** 0.5
-    scale = (full_cells / sample_cells) * linear
-    value = 1.0 / (t_step * scale)
-    return {"value": value, "unit": "time-steps/s", "cores": threads, "kind": "port",
-            "sample": f"{len(times)} step(s) from rest of the same case on a {nodes.shape[2]-1}x{nodes.shape[1]-1}x{nodes.shape[0]-1} "
-                      f"lattice ({sample_cells} cells): {t_step:.2f} s/step, p' iterations/step {iters}; scaled to "
-                      f"{full_cells} cells by cells x linear size = x{scale:.0f} (oracle restatement, C++ -O2, OpenMP)",
-            "sample_s_per_step": t_step, "scale_factor": scale}
+    return {"value": 1.0 / t_step, "unit": "time-steps/s", "cores": threads, "kind": "port",
+            "workload": label, "cells": cells,
+            "sample": f"{len(times)} whole step(s) from rest of the same case on a {nodes.shape[2]-1}x{nodes.shape[1]-1}x"
+                      f"{nodes.shape[0]-1} lattice ({cells} cells), plain FP64 solves to 1e-8: {t_step:.2f} s/step, p' "
+                      f"iterations/step {iters}; measured on that lattice, not scaled to the full one "
+                      f"(oracle restatement, C++ -O2, OpenMP on {threads} threads)",
+            "s_per_step": t_step}
 
 
 def case_label(args) -> str:
@@ -213,27 +217,88 @@ def case_label(args) -> str:
 
 
 def run_reference(args, world, rank, pg):
+    """The CPU restatement of the reference path (plain FP64) on the host cores.  Rank 0 alone
+    measures; the other ranks exit without work."""
     if rank != 0:
         return
-    budget = float(os.environ.get("CAFFE_REF_BUDGET_S", "120"))
-    cpu = scaled_cpu(args, max(1, args.steps), budget)
-    full_label = case_label(args)
+    budget = float(os.environ.get("CAFFE_REF_BUDGET_S", "60"))
+    cpu = measured_cpu(args, max(1, args.steps), budget)
     value = cpu["value"]
     line = {
         "impl": "reference", "metric": "time-steps/s at 1e-8 true relative residual", "value": value,
         "unit": "time-steps/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": 0,
         "ms_per_step": 1e3 / value, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64", "data": "synthetic", "config": {"workload": full_label, "reference_path": "plain FP64 (CPU restatement)"},
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": case_label(args), "reference_path": "plain FP64 (CPU restatement of the reference, oracle)",
+                   "timed_lattice": cpu["workload"], "timed_cells": cpu["cells"],
+                   "note": "whole steps measured on the smaller lattice of the same case; a step of the full lattice "
+                           "does not fit a CPU budget of minutes; not scaled"},
         "cpu_baseline": {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")},
         "e2e": {"value": value, "unit": "time-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
 
 
+def gpu_steps(nodes, spec, steps: int, local: int, precond_args=None) -> dict:
+    """Steps from rest on the GPU, each timed on the device (the handle's own CUDA events)."""
+    from caffe_old_b200.solver import make_solver
+    dev = make_solver(nodes, spec, device=local)
+    if precond_args is not None:
+        configure_precond(dev, precond_args)
+    rows = []
+    for _ in range(steps):
+        dev.solve()
+        st = dev.last_stats
+        rows.append({"step_ms": st["step_ms"], "p_iters": st["p_iters_total"], "fallbacks": st["fallbacks"],
+                     "cascades": st["cascades"], "status": st["status"]})
+    dev.close()
+    return {"s_per_step": sum(r["step_ms"] for r in rows) / len(rows) / 1e3, "rows": rows}
+
+
+def same_inputs_comparison(args, local: int, cpu: dict) -> dict:
+    """GPU and CPU on the identical smaller lattice of the default case: the GPU's plain FP64 and
+    learned forms against the CPU restatement's measured steps (cpu_baseline's run)."""
+    nodes, spec, label = sample_workload(args.workload, args.size)
+    out = {"workload": label, "cpu_s_per_step": cpu["s_per_step"]}
+    fp64 = gpu_steps(nodes, spec.replace(p_form="fp64"), 3, local)
+    out["gpu_fp64_s_per_step"] = fp64["s_per_step"]
+    out["gpu_fp64_over_cpu_time_steps_per_s"] = cpu["s_per_step"] / fp64["s_per_step"]
+    if args.p_form.startswith("learned"):
+        lrn = gpu_steps(nodes, spec.replace(p_form=args.p_form), 3, local, args)
+        out["gpu_learned_s_per_step"] = lrn["s_per_step"]
+        out["gpu_learned_over_cpu_time_steps_per_s"] = cpu["s_per_step"] / lrn["s_per_step"]
+        out["gpu_learned_rows"] = lrn["rows"]
+    return out
+
+
+def c2_full_line(local: int, cpu_budget_s: float) -> dict:
+    """Configuration 2 (128^3 lid-driven cavity, PISO, central, Jacobi-PCG, plain FP64) measured in
+    full on both: steps from rest on the GPU and on the CPU restatement, compared over the same
+    steps."""
+    nodes, spec, _ = C.config2_cavity3d(n=128)
+    cpu_times, cpu_iters, threads = _oracle_steps(nodes, spec, 3, cpu_budget_s)
+    k = len(cpu_times)
+    gpu = gpu_steps(nodes, spec, max(3, k), local)
+    g = [r["step_ms"] / 1e3 for r in gpu["rows"][:k]]
+    c = sum(cpu_times) / k
+    return {"workload": "piso_lid_cavity3d_128^3_re400_central_jacobi_pcg_fp64", "steps_from_rest": k,
+            "cpu_s_per_step": c, "cpu_cores": threads, "cpu_p_iters": cpu_iters,
+            "gpu_s_per_step": sum(g) / k, "gpu_p_iters": [r["p_iters"] for r in gpu["rows"][:k]],
+            "gpu_over_cpu_time_steps_per_s": c / (sum(g) / k)}
+
+
 # algorithmic bytes per cell and inner iteration of the learned solve (FP32 vectors, the
 # level pyramid's restriction reads and the prolonged term's reads included; coarse levels
 # excluded): flexible BiCGStab 170 B (two preconditioner applications), flexible CG 110 B
 LEARNED_BYTES = {"bicgstab": 170.0, "fcg": 110.0}
+
+
+def fgmres_bytes_per_cell(m: int) -> float:
+    """Algorithmic bytes per cell of one FGMRES(m) iteration j (FP32 vectors), averaged over a full
+    cycle j = 0 .. m-1: network scale of v_j 9 + restriction to level 1 9 + z_j = M(v_j) 13.5 +
+    w = A z_j 24 + two classical Gram-Schmidt passes, each reading w and v_0..v_j for the dots and
+    again for the update and writing w (12 (j+1) + 8) + v_(j+1) = w / h 8."""
+    return 79.5 + 12.0 * (m + 1)
 # DRAM bytes per cell and inner BiCGStab iteration of the fine-lattice kernels, from one ncu
 # capture (dram__bytes_read.sum + dram__bytes_write.sum, 240x160x160 case, per cell;
 # profiles/c5_ibsphere_learned_traffic.md); traffic grows with the cell count
@@ -283,7 +348,8 @@ def run_b200(args, world, rank, local, pg):
     def record(tag):
         st = dev.last_stats
         per_step.append({"phase": tag, "p_ms": round(st["p_ms"], 2), "p_iters": st["p_iters_total"], "p_solves": st["p_solves"],
-                         "fallbacks": st["fallbacks"], "step_ms": round(st["step_ms"], 2), "p_res_max": st["p_res_max"]})
+                         "fallbacks": st["fallbacks"], "cascades": st["cascades"], "step_ms": round(st["step_ms"], 2),
+                         "p_res_max": st["p_res_max"]})
 
     for _ in range(args.warmup):
         dev.solve()
@@ -296,6 +362,7 @@ def run_b200(args, world, rank, local, pg):
     t0 = torch.cuda.Event(enable_timing=True)
     t1 = torch.cuda.Event(enable_timing=True)
     p_ms, p_iters, p_solves, mom_ms, mom_iters, status, fallbacks, res_max = 0.0, 0, 0, 0.0, 0, 0, 0, 0.0
+    cascades = 0
     conts = []
     l0 = _lib.lib().caffe_launch_count()
     t0.record(stream)
@@ -305,7 +372,7 @@ def run_b200(args, world, rank, local, pg):
         record("timed")
         p_ms += st["p_ms"]; p_iters += st["p_iters_total"]; p_solves += st["p_solves"]
         mom_ms += st["mom_ms"]; mom_iters += sum(st["mom_iters"]); status = max(status, st["status"])
-        fallbacks += st["fallbacks"]; res_max = max(res_max, st["p_res_max"])
+        fallbacks += st["fallbacks"]; res_max = max(res_max, st["p_res_max"]); cascades += st["cascades"]
     t1.record(stream)
     t1.synchronize()
     launches = _lib.lib().caffe_launch_count() - l0
@@ -320,9 +387,10 @@ def run_b200(args, world, rank, local, pg):
     learned = args.p_form.startswith("learned")
     method = inner_method(spec, args) if learned else ("pcg" if spec.p_method == "cg_jacobi" else "bicgstab64")
     if learned:
-        per_row = LEARNED_BYTES.get(method)
+        per_row = LEARNED_BYTES.get(method) if method != "fgmres" else fgmres_bytes_per_cell(args.restart)
         kname = {"bicgstab": "learned inner flexible BiCGStab iteration (FP32, level pyramid)",
-                 "fcg": "learned inner flexible CG iteration (FP32, level pyramid)"}.get(method, "learned inner FGMRES iteration")
+                 "fcg": "learned inner flexible CG iteration (FP32, level pyramid)"}.get(
+            method, f"learned inner FGMRES({args.restart}) iteration (FP32, level pyramid + network, CGS2)")
     else:
         per_row = PCG_BYTES_PER_ROW if method == "pcg" else BICGSTAB_BYTES_PER_ROW
         kname = "cg1_kernel (persistent Jacobi-PCG, FP64)" if method == "pcg" else "bicgstab_kernel (persistent Jacobi-BiCGStab, FP64)"
@@ -348,7 +416,7 @@ def run_b200(args, world, rank, local, pg):
         dev.synchronize()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
-        ke = max(1, args.e2e_steps)
+        ke = max(1, args.e2e_steps if args.e2e_steps is not None else args.steps)
         e0.record(stream)
         for _ in range(ke):
             for nm in up:
@@ -389,9 +457,15 @@ def run_b200(args, world, rank, local, pg):
                    "time_steps_per_s_ratio_learned_over_fp64": sf / sl if sl > 0 else None}
 
     cpu = None
+    same_inputs = None
+    c2_line = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = scaled_cpu(args, 1, 60.0)
-        cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        cpu_full = measured_cpu(args, 3, 30.0)
+        cpu = {k: cpu_full[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        if args.workload == "c5":
+            same_inputs = same_inputs_comparison(args, local, cpu_full)
+            if not args.no_c2_line:
+                c2_line = c2_full_line(local, 60.0)
 
     if rank == 0:
         working_set = N * 8 * 60
@@ -407,11 +481,18 @@ def run_b200(args, world, rank, local, pg):
                        "l2": f"inputs larger than L2: working set ~{working_set / 2**30:.1f} GiB > 126 MB"},
             "p_solve_ms": p_ms / args.steps, "momentum_solve_ms": mom_ms / args.steps,
             "p_iters_per_step": p_iters / args.steps, "mom_iters_per_step": mom_iters / args.steps,
-            "p_res_max": res_max, "fallbacks": fallbacks,
+            "p_res_max": res_max, "fallbacks": fallbacks, "cascades": cascades,
             "continuity_last": conts[-1], "solver_status": status,
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
             "gpu_launches": launches, "compare": compare, "per_step": per_step,
+            "cpu_vs_gpu_same_lattice": same_inputs, "c2_128cubed_fully_measured": c2_line,
         }
+        if compare:
+            print("compare (same steps from rest): p-solve ms fp64/learned %.2f, Krylov iterations fp64/learned %.2f, "
+                  "time-steps/s learned/fp64 %.2f" % (compare["p_solve_ms_ratio_fp64_over_learned"] or 0,
+                                                      compare["krylov_iterations_ratio_fp64_over_learned"] or 0,
+                                                      compare["time_steps_per_s_ratio_learned_over_fp64"] or 0),
+                  file=sys.stderr, flush=True)
         print(json.dumps(line), flush=True)
 
 
@@ -423,7 +504,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=("b200", "reference"))
     ap.add_argument("--workload", default="c5", choices=("c1", "c2", "c3", "c5"))
     ap.add_argument("--p-form", default="learned_mixed", choices=tuple(C.P_FORMS))
-    ap.add_argument("--precond", default="levels", choices=("levels", "network", "jacobi"))
+    ap.add_argument("--precond", default="network", choices=("levels", "network", "jacobi"))
     ap.add_argument("--inner", default="auto", choices=("auto", "fcg", "bicgstab", "fgmres"))
     ap.add_argument("--net-from", type=int, default=None, help="first pyramid level that runs the network "
                     "(default: the one the shipped parameters were trained for)")
@@ -431,9 +512,10 @@ def main():
     ap.add_argument("--params", default=None, help="network parameters (.npy); default: the shipped ones")
     ap.add_argument("--size", type=int, default=None)
     ap.add_argument("--compare-fp64", type=int, default=1, help="plain FP64 steps from rest to compare with")
-    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--e2e-steps", type=int, default=None, help="end-to-end steps (default: --steps)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-c2-line", action="store_true", help="skip the fully measured 128^3 cavity comparison")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "b200":
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)

@@ -32,6 +32,7 @@ struct StepAcc {
     int p_solves;
     int status;
     int fallbacks;
+    int cascades;
     double p_res_max;
     double mom_res_max;
     double continuity;
@@ -84,6 +85,7 @@ __global__ void acc_kernel(const KspOut* o, StepAcc* acc, int kind, int nr) {
             acc->mom_iters[q] = o->iters[q];
             if (rr > acc->mom_res_max) acc->mom_res_max = rr;
         } else {
+            if (kind == 2) acc->cascades += o->cascades;
             acc->p_iters_last = o->iters[q];
             acc->p_iters_total += o->iters[q];
             acc->p_solves += 1;
@@ -395,7 +397,8 @@ int ph_solve_pcorr(caffe_dev* h) {
     int method = h->cs.p_method;
     if (method == CAFFE_KSP_CG_JACOBI && !sym) method = CAFFE_KSP_BICGSTAB_JACOBI;   // ghost rows are not symmetric
     int project = p_singular(h);
-    if (h->cs.p_form == CAFFE_P_LEARNED || h->cs.p_form == CAFFE_P_LEARNED_MIXED) {
+    const bool learned = h->cs.p_form == CAFFE_P_LEARNED || h->cs.p_form == CAFFE_P_LEARNED_MIXED;
+    if (learned) {
         // FP64 refinement around an FP32 flexible Krylov solve preconditioned through the level
         // pyramid and the network; the plain FP64 solve re-runs on the device if it does not
         // reach the tolerance
@@ -427,7 +430,7 @@ int ph_solve_pcorr(caffe_dev* h) {
         gauge_apply_kernel<<<grid_for(h->L.N, 256), 256, 0, h->st>>>(h->pc, h->L.N, h->gaugePart + nb);
         CB_CHECK_LAUNCH();
     }
-    acc_kernel<<<1, 32, 0, h->st>>>(h->kw.out, h->acc, 1, 1);
+    acc_kernel<<<1, 32, 0, h->st>>>(h->kw.out, h->acc, learned ? 2 : 1, 1);
     CB_CHECK_LAUNCH();
     if (h->recording && h->pairCount < h->pairCap) {
         // (b, x*) of this solve, then (b - A x_k, x* - x_k) for iterates x_k of truncated plain
@@ -529,6 +532,7 @@ int read_stats(caffe_dev* h, caffe_step_stats* s) {
     o.mom_res_max = a.mom_res_max;
     o.status = a.status;
     o.fallbacks = a.fallbacks;
+    o.cascades = a.cascades;
     o.n_ghost = h->ib ? h->ibs.nGhostHost : 0;
     o.n_rows = (int)(h->L.N - (h->ib ? h->ibs.nInactiveHost : 0));
     float ms = 0.f;

@@ -38,6 +38,7 @@ struct KspOut {
     int iters[3];
     double relres[3];
     int status[3];      // 0 converged, 1 maxit, 2 breakdown, 3 non-finite
+    int cascades;       // learned solve only: 1 when its network stage handed over to the pyramid stage
 };
 
 // Workspace for up to NR = 3 right-hand sides; every array is a halo-padded cell array of

@@ -768,6 +768,12 @@ __global__ void cast_kernel(OpSym A, long long N, float* aP, float* aE, float* a
     aP[c] = (float)d; aE[c] = (float)A.aE[c]; aN[c] = (float)A.aN[c]; aT[c] = (float)A.aT[c];
     invD[c] = d != 0. ? (float)(1. / d) : 1.f;
 }
+// the next stage of a cascade starts its own refinement passes (||b||^2 and the tolerance stay)
+__global__ void reopen_kernel(Scal* S) {
+    if (threadIdx.x != 0) return;
+    S->odone = 0; S->done = 0; S->status = 0; S->stall = 0; S->outer = 0; S->first = 0;
+}
+
 __global__ void publish_kernel(const Scal* S, KspOut* out) {
     if (threadIdx.x != 0) return;
     out->iters[0] = S->iters;
@@ -1082,138 +1088,164 @@ int learned_solve(LearnedWork& lw, const OpSym& A, const uint8_t* status, const 
     CB_CUDA(cudaMemcpyAsync(S, &init, sizeof(Scal), cudaMemcpyHostToDevice, st));
     CB_CHECK_LAUNCH();
     const Dims3 fd = dims_of(lw.lev[0]), cd = level1_dims(lw);
-    const float* w1 = level_w1(lw, mode);
     const bool nonsym = A.gh.n > 0;
     int method = lw.inner;
     if (method == LEARN_INNER_AUTO)
         method = !nonsym ? LEARN_INNER_FCG : (mode == NET_MODE_NETWORK ? LEARN_INNER_FGMRES : LEARN_INNER_BICGSTAB);
-    const bool symmetric = method == LEARN_INNER_FCG;
-    const bool fgmres = method == LEARN_INNER_FGMRES;
     const int m = lw.restart < 1 ? 1 : (lw.restart > FGM ? FGM : lw.restart);
-    if (fgmres && fg_alloc(lw, m)) return 1;
+    if (method == LEARN_INNER_FGMRES && fg_alloc(lw, m)) return 1;
     FgScal* F = static_cast<FgScal*>(lw.fgScal);
     const long long PS = L.PS;
-    if (!symmetric) {
+    if (method != LEARN_INNER_FCG) {
         count_active_kernel<<<nb, LB, 0, st>>>(N, status, lw.part);
         count_finish<<<1, LB, 0, st>>>(lw.part, nb, lw.mean + 1);
     }
-    // FGMRES: one restart cycle per refinement pass, as many cycles as the iteration budget
-    // allows, at most 100
-    const int max_outer = fgmres ? std::min(100, std::max(12, maxit / m + 1)) : 12;
-    const int chunk = 8;
-    for (int outer = 0; outer <= max_outer; ++outer) {
-        outer_residual_kernel<<<nb, LB, 0, st>>>(A, N, b, x, lw.r, lw.part, S);
-        outer_check_kernel<<<1, LB, 0, st>>>(lw.part, nb, S, max_outer);
-        CB_CUDA(cudaMemcpyAsync(lw.hostScal, S, sizeof(Scal), cudaMemcpyDeviceToHost, st));
-        CB_CUDA(cudaStreamSynchronize(st));
-        Scal* hs = static_cast<Scal*>(lw.hostScal);
-        if (outer == 0) {
-            // the tolerance needs ||b||^2: the first outer residual (x = 0) is b itself
-            double tol2 = std::max(rtol * rtol * hs->bb, atol * atol);
-            bool fin = hs->rr64 <= tol2 || !(hs->bb > 0.);
-            CB_CUDA(cudaMemcpyAsync(&S->tol2, &tol2, sizeof(double), cudaMemcpyHostToDevice, st));
-            if (fin) {
-                int one = 1;
-                CB_CUDA(cudaMemcpyAsync(&S->odone, &one, sizeof(int), cudaMemcpyHostToDevice, st));
-                break;
-            }
-        } else if (hs->odone) {
-            break;
-        }
-        // inner target: deep first, then only the factor still missing
-        double etaK = eta;
-        if (hs->bb > 0. && hs->rr64 > 0.) {
-            double need = 0.25 * sqrt(std::max(rtol * rtol * hs->bb, atol * atol) / hs->rr64);
-            if (need > etaK) etaK = need;
-        }
-        if (etaK > 0.5) etaK = 0.5;
-        int cur = 0;
-        if (fgmres) {
-            fg_init_kernel<<<G, 256, 0, st>>>(N, lw.r, lw.fgV + L.H, lw.e, S, F);
-            fg_start_finish<<<1, 32, 0, st>>>(S, etaK, lw.mean + 1);
-            CB_CHECK_LAUNCH();
-            for (int j = 0; j < m; ++j) {
-                float* vj = lw.fgV + j * PS + L.H;
-                float* zj = lw.fgZ + j * PS + L.H;
-                scale_partial_kernel<<<nb, LB, 0, st>>>(N, vj, lw.invD, status, lw.part, S);
-                scale_finish<<<1, LB, 0, st>>>(lw.part, nb, S);
-                if (apply_levels(lw, vj, status, mode, S, st)) return 1;
-                bs_z_kernel<<<nb, LB, 0, st>>>(N, fd, cd, vj, lw.invD, status, w1, zj, S);
-                fg_spmv_kernel<<<nb, LB, 0, st>>>(Af, N, zj, lw.t, S);
-                // classical Gram-Schmidt with one re-orthogonalisation (CGS2): FP32 vectors lose
-                // orthogonality in a single pass once the preconditioner is strong
-                for (int pass = 0; pass < 2; ++pass) {
-                    double* hc = pass == 0 ? F->h1 : F->h2;
-                    fg_dots_kernel<<<dim3(j + 1, FG_DOT_BLOCKS), LB, 0, st>>>(N, lw.t, lw.fgV + L.H, PS, lw.fgPart, S);
-                    fg_dots_finish<<<j + 1, LB, 0, st>>>(lw.fgPart, FG_DOT_BLOCKS, hc, S);
-                    fg_orth_kernel<<<nb, LB, 0, st>>>(N, lw.t, lw.fgV + L.H, PS, j, hc, lw.part, S);
-                }
-                fg_step_finish<<<1, LB, 0, st>>>(lw.part, nb, j, m, maxit, F, S);
-                fg_scale_kernel<<<G, 256, 0, st>>>(N, lw.t, lw.fgV + (j + 1) * PS + L.H, S);
-                if ((j & 7) == 7 || j == m - 1) {
-                    CB_CHECK_LAUNCH();
-                    CB_CUDA(cudaMemcpyAsync(lw.hostScal, S, sizeof(Scal), cudaMemcpyDeviceToHost, st));
-                    CB_CUDA(cudaStreamSynchronize(st));
-                    if (static_cast<Scal*>(lw.hostScal)->done) break;
-                }
-            }
-            fg_solve_kernel<<<1, 32, 0, st>>>(F);
-            fg_combine_kernel<<<nb, LB, 0, st>>>(N, lw.fgZ + L.H, PS, F, lw.e);
-            CB_CHECK_LAUNCH();
-            outer_update_kernel<<<G, 256, 0, st>>>(N, x, lw.e, S);
-            int zero = 0;
-            CB_CUDA(cudaMemcpyAsync(&S->done, &zero, sizeof(int), cudaMemcpyHostToDevice, st));
-            continue;
-        }
-        if (symmetric) {
-            inner_start_kernel<<<nb, LB, 0, st>>>(N, lw.r, lw.invD, status, lw.e, lw.p[0], lw.q[0], lw.part, S);
-            inner_start_finish_kernel<<<1, LB, 0, st>>>(lw.part, nb, S, etaK);
-        } else {
-            bs_start_kernel<<<nb, LB, 0, st>>>(N, lw.r, lw.rh, lw.e, lw.p[0], lw.q[0], lw.part, S);
-            bs_start_finish<<<1, LB, 0, st>>>(lw.part, nb, S, etaK, lw.mean + 1);
-        }
-        bool innerDone = false;
-        while (!innerDone) {
-            for (int it = 0; it < chunk; ++it) {
-                if (symmetric) {
-                    if (apply_levels(lw, lw.r, status, mode, S, st)) return 1;
-                    precond_z_kernel<<<nb, LB, 0, st>>>(N, fd, cd, lw.r, lw.invD, status, w1, lw.z, lw.q[cur], lw.part, S);
-                    beta_kernel<<<1, LB, 0, st>>>(lw.part, nb, S);
-                    direction_kernel<<<nb, LB, 0, st>>>(Af, N, lw.z, lw.p[cur], lw.p[cur ^ 1], lw.q[cur ^ 1], lw.r, lw.part, S);
-                    alpha_kernel<<<1, LB, 0, st>>>(lw.part, nb, S);
-                    step_kernel<<<nb, LB, 0, st>>>(N, lw.e, lw.r, lw.p[cur ^ 1], lw.q[cur ^ 1], lw.invD, status, lw.part, S);
-                    step_finish_kernel<<<1, LB, 0, st>>>(lw.part, nb, S, maxit);
-                    cur ^= 1;
-                } else {
-                    // p = p[0], v = q[0], ph = p[1], sh = q[1], s = z, t = t
-                    bs_dir_kernel<<<nb, LB, 0, st>>>(N, lw.r, lw.q[0], lw.invD, status, lw.p[0], lw.part, S);
-                    scale_finish<<<1, LB, 0, st>>>(lw.part, nb, S);
-                    if (apply_levels(lw, lw.p[0], status, mode, S, st)) return 1;
-                    bs_z_kernel<<<nb, LB, 0, st>>>(N, fd, cd, lw.p[0], lw.invD, status, w1, lw.p[1], S);
-                    bs_spmv_kernel<<<nb, LB, 0, st>>>(Af, N, lw.p[1], lw.q[0], lw.rh, nullptr, lw.part, S);
-                    bs_alpha_finish<<<1, LB, 0, st>>>(lw.part, nb, S);
-                    bs_s_kernel<<<nb, LB, 0, st>>>(N, lw.r, lw.q[0], lw.invD, status, lw.z, lw.part, S);
-                    scale_finish<<<1, LB, 0, st>>>(lw.part, nb, S);
-                    if (apply_levels(lw, lw.z, status, mode, S, st)) return 1;
-                    bs_z_kernel<<<nb, LB, 0, st>>>(N, fd, cd, lw.z, lw.invD, status, w1, lw.q[1], S);
-                    bs_spmv_kernel<<<nb, LB, 0, st>>>(Af, N, lw.q[1], lw.t, nullptr, lw.z, lw.part, S);
-                    bs_omega_finish<<<1, LB, 0, st>>>(lw.part, nb, S);
-                    bs_update_kernel<<<nb, LB, 0, st>>>(N, lw.e, lw.r, lw.p[1], lw.q[1], lw.z, lw.t, lw.rh, lw.part, S);
-                    bs_update_finish<<<1, LB, 0, st>>>(lw.part, nb, S, maxit);
-                }
-            }
-            CB_CHECK_LAUNCH();
+    // One stage of the solve: FP64 refinement passes around the inner method `smethod` with the
+    // preconditioner form `smode`, from the current x; inner iterations are capped at iterCap
+    // (counted over the whole solve).
+    auto stage = [&](int smode, int smethod, int iterCap) -> int {
+        const int maxit = iterCap;
+        const int mode = smode;
+        const float* w1 = level_w1(lw, mode);
+        const bool symmetric = smethod == LEARN_INNER_FCG;
+        const bool fgmres = smethod == LEARN_INNER_FGMRES;
+        // FGMRES: one restart cycle per refinement pass, as many cycles as the iteration budget
+        // allows, at most 100
+        const int max_outer = fgmres ? std::min(100, std::max(12, maxit / m + 1)) : 12;
+        const int chunk = 8;
+        for (int outer = 0; outer <= max_outer; ++outer) {
+            outer_residual_kernel<<<nb, LB, 0, st>>>(A, N, b, x, lw.r, lw.part, S);
+            outer_check_kernel<<<1, LB, 0, st>>>(lw.part, nb, S, max_outer);
             CB_CUDA(cudaMemcpyAsync(lw.hostScal, S, sizeof(Scal), cudaMemcpyDeviceToHost, st));
             CB_CUDA(cudaStreamSynchronize(st));
-            Scal* h2 = static_cast<Scal*>(lw.hostScal);
-            innerDone = h2->done != 0;
-            if (h2->iters >= maxit) break;
+            Scal* hs = static_cast<Scal*>(lw.hostScal);
+            if (outer == 0) {
+                // the tolerance needs ||b||^2: the first outer residual (x = 0) is b itself
+                double tol2 = std::max(rtol * rtol * hs->bb, atol * atol);
+                bool fin = hs->rr64 <= tol2 || !(hs->bb > 0.);
+                CB_CUDA(cudaMemcpyAsync(&S->tol2, &tol2, sizeof(double), cudaMemcpyHostToDevice, st));
+                if (fin) {
+                    int one = 1;
+                    CB_CUDA(cudaMemcpyAsync(&S->odone, &one, sizeof(int), cudaMemcpyHostToDevice, st));
+                    break;
+                }
+            } else if (hs->odone) {
+                break;
+            }
+            // inner target: deep first, then only the factor still missing
+            double etaK = eta;
+            if (hs->bb > 0. && hs->rr64 > 0.) {
+                double need = 0.25 * sqrt(std::max(rtol * rtol * hs->bb, atol * atol) / hs->rr64);
+                if (need > etaK) etaK = need;
+            }
+            if (etaK > 0.5) etaK = 0.5;
+            int cur = 0;
+            if (fgmres) {
+                fg_init_kernel<<<G, 256, 0, st>>>(N, lw.r, lw.fgV + L.H, lw.e, S, F);
+                fg_start_finish<<<1, 32, 0, st>>>(S, etaK, lw.mean + 1);
+                CB_CHECK_LAUNCH();
+                for (int j = 0; j < m; ++j) {
+                    float* vj = lw.fgV + j * PS + L.H;
+                    float* zj = lw.fgZ + j * PS + L.H;
+                    scale_partial_kernel<<<nb, LB, 0, st>>>(N, vj, lw.invD, status, lw.part, S);
+                    scale_finish<<<1, LB, 0, st>>>(lw.part, nb, S);
+                    if (apply_levels(lw, vj, status, mode, S, st)) return 1;
+                    bs_z_kernel<<<nb, LB, 0, st>>>(N, fd, cd, vj, lw.invD, status, w1, zj, S);
+                    fg_spmv_kernel<<<nb, LB, 0, st>>>(Af, N, zj, lw.t, S);
+                    // classical Gram-Schmidt with one re-orthogonalisation (CGS2): FP32 vectors lose
+                    // orthogonality in a single pass once the preconditioner is strong
+                    for (int pass = 0; pass < 2; ++pass) {
+                        double* hc = pass == 0 ? F->h1 : F->h2;
+                        fg_dots_kernel<<<dim3(j + 1, FG_DOT_BLOCKS), LB, 0, st>>>(N, lw.t, lw.fgV + L.H, PS, lw.fgPart, S);
+                        fg_dots_finish<<<j + 1, LB, 0, st>>>(lw.fgPart, FG_DOT_BLOCKS, hc, S);
+                        fg_orth_kernel<<<nb, LB, 0, st>>>(N, lw.t, lw.fgV + L.H, PS, j, hc, lw.part, S);
+                    }
+                    fg_step_finish<<<1, LB, 0, st>>>(lw.part, nb, j, m, maxit, F, S);
+                    fg_scale_kernel<<<G, 256, 0, st>>>(N, lw.t, lw.fgV + (j + 1) * PS + L.H, S);
+                    if ((j & 7) == 7 || j == m - 1) {
+                        CB_CHECK_LAUNCH();
+                        CB_CUDA(cudaMemcpyAsync(lw.hostScal, S, sizeof(Scal), cudaMemcpyDeviceToHost, st));
+                        CB_CUDA(cudaStreamSynchronize(st));
+                        if (static_cast<Scal*>(lw.hostScal)->done) break;
+                    }
+                }
+                fg_solve_kernel<<<1, 32, 0, st>>>(F);
+                fg_combine_kernel<<<nb, LB, 0, st>>>(N, lw.fgZ + L.H, PS, F, lw.e);
+                CB_CHECK_LAUNCH();
+                outer_update_kernel<<<G, 256, 0, st>>>(N, x, lw.e, S);
+                int zero = 0;
+                CB_CUDA(cudaMemcpyAsync(&S->done, &zero, sizeof(int), cudaMemcpyHostToDevice, st));
+                continue;
+            }
+            if (symmetric) {
+                inner_start_kernel<<<nb, LB, 0, st>>>(N, lw.r, lw.invD, status, lw.e, lw.p[0], lw.q[0], lw.part, S);
+                inner_start_finish_kernel<<<1, LB, 0, st>>>(lw.part, nb, S, etaK);
+            } else {
+                bs_start_kernel<<<nb, LB, 0, st>>>(N, lw.r, lw.rh, lw.e, lw.p[0], lw.q[0], lw.part, S);
+                bs_start_finish<<<1, LB, 0, st>>>(lw.part, nb, S, etaK, lw.mean + 1);
+            }
+            bool innerDone = false;
+            while (!innerDone) {
+                for (int it = 0; it < chunk; ++it) {
+                    if (symmetric) {
+                        if (apply_levels(lw, lw.r, status, mode, S, st)) return 1;
+                        precond_z_kernel<<<nb, LB, 0, st>>>(N, fd, cd, lw.r, lw.invD, status, w1, lw.z, lw.q[cur], lw.part, S);
+                        beta_kernel<<<1, LB, 0, st>>>(lw.part, nb, S);
+                        direction_kernel<<<nb, LB, 0, st>>>(Af, N, lw.z, lw.p[cur], lw.p[cur ^ 1], lw.q[cur ^ 1], lw.r, lw.part, S);
+                        alpha_kernel<<<1, LB, 0, st>>>(lw.part, nb, S);
+                        step_kernel<<<nb, LB, 0, st>>>(N, lw.e, lw.r, lw.p[cur ^ 1], lw.q[cur ^ 1], lw.invD, status, lw.part, S);
+                        step_finish_kernel<<<1, LB, 0, st>>>(lw.part, nb, S, maxit);
+                        cur ^= 1;
+                    } else {
+                        // p = p[0], v = q[0], ph = p[1], sh = q[1], s = z, t = t
+                        bs_dir_kernel<<<nb, LB, 0, st>>>(N, lw.r, lw.q[0], lw.invD, status, lw.p[0], lw.part, S);
+                        scale_finish<<<1, LB, 0, st>>>(lw.part, nb, S);
+                        if (apply_levels(lw, lw.p[0], status, mode, S, st)) return 1;
+                        bs_z_kernel<<<nb, LB, 0, st>>>(N, fd, cd, lw.p[0], lw.invD, status, w1, lw.p[1], S);
+                        bs_spmv_kernel<<<nb, LB, 0, st>>>(Af, N, lw.p[1], lw.q[0], lw.rh, nullptr, lw.part, S);
+                        bs_alpha_finish<<<1, LB, 0, st>>>(lw.part, nb, S);
+                        bs_s_kernel<<<nb, LB, 0, st>>>(N, lw.r, lw.q[0], lw.invD, status, lw.z, lw.part, S);
+                        scale_finish<<<1, LB, 0, st>>>(lw.part, nb, S);
+                        if (apply_levels(lw, lw.z, status, mode, S, st)) return 1;
+                        bs_z_kernel<<<nb, LB, 0, st>>>(N, fd, cd, lw.z, lw.invD, status, w1, lw.q[1], S);
+                        bs_spmv_kernel<<<nb, LB, 0, st>>>(Af, N, lw.q[1], lw.t, nullptr, lw.z, lw.part, S);
+                        bs_omega_finish<<<1, LB, 0, st>>>(lw.part, nb, S);
+                        bs_update_kernel<<<nb, LB, 0, st>>>(N, lw.e, lw.r, lw.p[1], lw.q[1], lw.z, lw.t, lw.rh, lw.part, S);
+                        bs_update_finish<<<1, LB, 0, st>>>(lw.part, nb, S, maxit);
+                    }
+                }
+                CB_CHECK_LAUNCH();
+                CB_CUDA(cudaMemcpyAsync(lw.hostScal, S, sizeof(Scal), cudaMemcpyDeviceToHost, st));
+                CB_CUDA(cudaStreamSynchronize(st));
+                Scal* h2 = static_cast<Scal*>(lw.hostScal);
+                innerDone = h2->done != 0;
+                if (h2->iters >= maxit) break;
+            }
+            outer_update_kernel<<<G, 256, 0, st>>>(N, x, lw.e, S);
+            // the next outer pass re-opens the inner solve
+            int zero = 0;
+            CB_CUDA(cudaMemcpyAsync(&S->done, &zero, sizeof(int), cudaMemcpyHostToDevice, st));
         }
-        outer_update_kernel<<<G, 256, 0, st>>>(N, x, lw.e, S);
-        // the next outer pass re-opens the inner solve
-        int zero = 0;
-        CB_CUDA(cudaMemcpyAsync(&S->done, &zero, sizeof(int), cudaMemcpyHostToDevice, st));
+        return 0;
+    };
+    if (stage(mode, method, maxit)) return 1;
+    // Cascade: a solve whose network stage stalled (three refinement passes in a row that each
+    // leave more than 90% of the true residual) or ran out of passes continues, from the iterate
+    // it reached, with the same pyramid and an identity in place of the network (a fixed linear
+    // preconditioner, so BiCGStab or flexible CG apply); only a solve that misses the tolerance
+    // there too leaves status != 0 for the plain FP64 re-solve.
+    int cascades = 0;
+    {
+        Scal* hs = static_cast<Scal*>(lw.hostScal);
+        if (mode == NET_MODE_NETWORK && (hs->status == 1 || hs->status == 2)) {
+            const int itersSoFar = hs->iters;
+            reopen_kernel<<<1, 32, 0, st>>>(S);
+            CB_CHECK_LAUNCH();
+            cascades = 1;
+            if (stage(NET_MODE_LEVELS, nonsym ? LEARN_INNER_BICGSTAB : LEARN_INNER_FCG, itersSoFar + maxit)) return 1;
+        }
     }
+    CB_CUDA(cudaMemcpyAsync(&out->cascades, &cascades, sizeof(int), cudaMemcpyHostToDevice, st));
     publish_kernel<<<1, 32, 0, st>>>(S, out);
     CB_CHECK_LAUNCH();
     CB_CUDA(cudaMemcpyAsync(lw.hostScal, S, sizeof(Scal), cudaMemcpyDeviceToHost, st));

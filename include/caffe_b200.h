@@ -76,6 +76,8 @@ typedef struct caffe_step_stats {
     int n_ghost;            /* immersed-boundary ghost cells */
     int n_rows;             /* unknowns per system (active + ghost cells) */
     double p_ms, mom_ms, step_ms;   /* device time of the step's phases (CUDA events) */
+    int cascades;           /* learned p' solves whose network stage stalled and that finished with
+                             * the pyramid alone (an identity in place of the network) */
 } caffe_step_stats;
 
 typedef struct caffe_dev caffe_dev;
