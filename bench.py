@@ -300,8 +300,8 @@ def fgmres_bytes_per_cell(m: int) -> float:
     again for the update and writing w (12 (j+1) + 8) + v_(j+1) = w / h 8."""
     return 79.5 + 12.0 * (m + 1)
 # DRAM bytes per cell and inner BiCGStab iteration of the fine-lattice kernels, from one ncu
-# capture (dram__bytes_read.sum + dram__bytes_write.sum, 240x160x160 case, per cell;
-# profiles/c5_ibsphere_learned_traffic.md); traffic grows with the cell count
+# capture (dram__bytes_read.sum + dram__bytes_write.sum of the 240x160x160 case, per cell);
+# traffic grows with the cell count
 LEARNED_TRAFFIC_PER_CELL = {"bicgstab": 154.0}
 
 

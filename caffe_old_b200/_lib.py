@@ -66,7 +66,7 @@ class StepStats(ctypes.Structure):
 EXPORTS = (
     "caffe_last_error", "caffe_dev_create", "caffe_dev_destroy", "caffe_dev_solve", "caffe_dev_phase",
     "caffe_dev_array", "caffe_dev_stats", "caffe_dev_stream", "caffe_dev_synchronize",
-    "caffe_ksp7_solve", "caffe_ksp7_solve_device", "caffe_ksp7_solve_device_noalloc",
+    "caffe_ksp7_solve", "caffe_ksp7_solve_device", "caffe_ksp7_solve_device_noalloc", "caffe_csr_solve", "caffe_csr_matvec",
     "caffe_precond_param_count", "caffe_precond_net_apply", "caffe_precond_net_grad",
     "caffe_dev_set_precond", "caffe_dev_get_precond", "caffe_dev_set_precond_mode", "caffe_dev_set_precond_options",
     "caffe_dev_record_pairs", "caffe_dev_pair_count", "caffe_dev_add_pairs", "caffe_dev_add_random_pairs", "caffe_dev_copy_pairs", "caffe_dev_train_precond",
@@ -98,6 +98,8 @@ def lib():
     L.caffe_ksp7_solve_device.argtypes = [ci, ci, ci, vp, vp, vp, ci, cd, ci, vp, ctypes.POINTER(ci), ctypes.POINTER(cd)]
     L.caffe_ksp7_solve_device_noalloc.argtypes = [ci, ci, ci, vp, vp, vp, ci, cd, ci, vp, ctypes.POINTER(ci),
                                                   ctypes.POINTER(cd)]
+    L.caffe_csr_solve.argtypes = [ci, vp, vp, vp, vp, vp, ci, cd, cd, ci, ctypes.POINTER(ci), ctypes.POINTER(cd)]
+    L.caffe_csr_matvec.argtypes = [ci, ci, vp, vp, vp, vp, vp]
     L.caffe_precond_param_count.restype = ci
     L.caffe_precond_net_apply.argtypes = [ci, ci, ci, vp, vp, vp]
     L.caffe_precond_net_grad.argtypes = [ci, ci, ci, vp, vp, vp, vp, vp]
@@ -168,4 +170,21 @@ def ksp7_solve(shape, coef7: np.ndarray, b: np.ndarray, method: str = "bicgstab_
                                 ctypes.byref(it), ctypes.byref(rr))
     if st == 1:
         raise CaffeError("caffe_ksp7_solve: " + last_error())
+    return x, it.value, rr.value, st
+
+
+def csr_solve(row_ptr, col, val, b, method: str = "bicgstab_jacobi", rtol: float = 1e-8, atol: float = 0.0,
+              maxit: int = 20000):
+    """SparseMatrix::solve for a general compressed-row system on the device; returns (x, iters,
+    relative residual, status)."""
+    row_ptr = np.ascontiguousarray(row_ptr, dtype=np.int32)
+    col = np.ascontiguousarray(col, dtype=np.int32)
+    val = np.ascontiguousarray(val, dtype=np.float64)
+    b = np.ascontiguousarray(b, dtype=np.float64)
+    x = np.zeros_like(b)
+    it, rr = ctypes.c_int(0), ctypes.c_double(0.0)
+    st = lib().caffe_csr_solve(int(b.size), _ptr(row_ptr), _ptr(col), _ptr(val), _ptr(b), _ptr(x), C.KSP_METHODS[method],
+                               float(rtol), float(atol), int(maxit), ctypes.byref(it), ctypes.byref(rr))
+    if st == 1:
+        raise CaffeError("caffe_csr_solve: " + last_error())
     return x, it.value, rr.value, st

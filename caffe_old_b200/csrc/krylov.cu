@@ -24,6 +24,7 @@
 // p = r + beta (p_old - omega v) and s = r - alpha v are recomputed at the stencil
 // neighbours instead of costing an extra pass and barrier.
 #include <cooperative_groups.h>
+#include <cstring>
 #include "krylov.cuh"
 
 #define CAFFE_KSP_CG_JACOBI_INT 2   // caffe_ksp value of Jacobi-CG (include/caffe_b200.h)
@@ -160,7 +161,24 @@ __device__ __forceinline__ void apply(const OpSym& A, long long c, X&& x, double
     if (A.gh.n > 0) ghost_fix<NR>(A.gh, c, x, y);
 }
 
+template <int NR, class X>
+__device__ __forceinline__ void apply(const OpCSR& A, long long c, X&& x, double (&y)[NR]) {
+    const int p0 = __ldg(A.ptr + c), p1 = __ldg(A.ptr + c + 1);
+#pragma unroll
+    for (int q = 0; q < NR; ++q) y[q] = 0.;
+    for (int p = p0; p < p1; ++p) {
+        const double v = __ldg(A.val + p);
+        const long long e = __ldg(A.col + p);
+#pragma unroll
+        for (int q = 0; q < NR; ++q) y[q] += v * x(q, e);
+    }
+}
+
 __device__ __forceinline__ double diag_of(const Op7& A, long long c) { return A.a[0][c]; }
+__device__ __forceinline__ double diag_of(const OpCSR& A, long long c) {
+    const int d = A.diag[c];
+    return d >= 0 ? A.val[d] : 0.;
+}
 __device__ __forceinline__ double diag_of(const OpSym& A, long long c) { return A.aP[c]; }
 
 template <class Op>
@@ -847,12 +865,32 @@ int ksp_cg7(const Op7& A, const double* b, double* x, const Lat& L, const KspWor
     return launch_coop(cg1_kernel<Op7>, G, a, &A, st);
 }
 
+int ksp_csr(const OpCSR& A, int method, long long n, const double* b, double* x, const KspWork& w, double rtol, int maxit,
+            cudaStream_t st, double atol) {
+    inv_diag_kernel<OpCSR><<<grid_for(n, 256), 256, 0, st>>>(A, n, w.invD);
+    CB_CHECK_LAUNCH();
+    Lat L;
+    std::memset(&L, 0, sizeof(L));
+    L.nI = (int)n; L.nJ = 1; L.nK = 1; L.N = n; L.nIJ = n; L.H = 0; L.PS = n;   // unpadded vectors
+    KArgs a = make_args(L, w, b, x, rtol, maxit, atol);
+    if (method == CAFFE_KSP_CG_JACOBI_INT) {
+        static int G = 0;
+        if (!G) G = coop_grid(cg1_kernel<OpCSR>);
+        return launch_coop(cg1_kernel<OpCSR>, G, a, &A, st);
+    }
+    static int G = 0;
+    if (!G) G = coop_grid(bicgstab_kernel<1, OpCSR>);
+    return launch_coop(bicgstab_kernel<1, OpCSR>, G, a, &A, st);
+}
+
 int krylov_grid_size(int which) {
     switch (which) {
         case 0: return coop_grid(bicgstab_kernel<3, Op7>);
         case 1: return coop_grid(bicgstab_kernel<1, OpSym>);
         case 2: return coop_grid(cg1_kernel<OpSym>);
         case 4: return coop_grid(cg1_kernel<Op7>);
+        case 5: return coop_grid(bicgstab_kernel<1, OpCSR>);
+        case 6: return coop_grid(cg1_kernel<OpCSR>);
         default: return coop_grid(bicgstab_kernel<1, Op7>);
     }
 }

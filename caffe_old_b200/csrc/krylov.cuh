@@ -34,6 +34,16 @@ struct OpSym {
     GhostRows gh;
 };
 
+// General sparse operator in compressed rows: the AIJ matrix SparseMatrix assembles row by row
+// (src/Math/SparseMatrix.cpp:49-83).  diag[r] is the position of row r's diagonal entry in
+// col / val, -1 when the row has none.
+struct OpCSR {
+    const int* ptr;
+    const int* col;
+    const double* val;
+    const int* diag;
+};
+
 struct KspOut {
     int iters[3];
     double relres[3];
@@ -85,8 +95,12 @@ int ksp_mixed_sym(const OpSym& A, int method, const double* b, double* x, const 
 // learned solve), decided on the device without a host round trip.
 int ksp_fallback_sym(const OpSym& A, int method, const double* b, double* x, const Lat& L, const KspWork& w, double rtol, int maxit,
                      cudaStream_t st, int project, const int* status, int* fallbacks, double atol = 0.);
+// Krylov solve of an n-row compressed-row system (vectors of n doubles, no halo): BiCGStab or CG
+// with Jacobi preconditioning, the same persistent kernels as the lattice solves.
+int ksp_csr(const OpCSR& A, int method, long long n, const double* b, double* x, const KspWork& w, double rtol, int maxit,
+            cudaStream_t st, double atol = 0.);
 // Blocks of the cooperative grid a solve launches: 0 BiCGStab on 3 right-hand sides (Op7),
-// 1 BiCGStab (OpSym), 2 CG (OpSym), 3 BiCGStab (Op7), 4 CG (Op7).  The block partials of a
+// 1 BiCGStab (OpSym), 2 CG (OpSym), 3 BiCGStab (Op7), 4 CG (Op7), 5 BiCGStab (OpCSR), 6 CG (OpCSR).  The block partials of a
 // solve take 2 x grid x 8 doubles.
 int krylov_grid_size(int which);
 

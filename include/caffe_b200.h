@@ -143,6 +143,19 @@ int caffe_ksp7_solve(int nI, int nJ, int nK, const double* coef7, const double* 
 int caffe_ksp7_solve_device(int nI, int nJ, int nK, const double* d_coef7, const double* d_b, double* d_x,
                             int method, double rtol, int maxit, void* stream, int* iters, double* rel_res);
 
+/* Krylov solve of a general sparse system of n rows in compressed-row form (host arrays: row_ptr
+ * n + 1 entries from 0, col / val row_ptr[n] entries, every column in [0, n)), b and x n doubles, x
+ * from zero.  Replaces SparseMatrix::solve over PETSc's AIJ matrix (src/Math/SparseMatrix.cpp:86-106)
+ * for any row structure; the host layer's SparseMatrix class calls it.  Stops once
+ * ||b - A x|| <= max(rtol ||b||, atol) (PETSc's rtol / atol test, on the true residual).
+ * Returns 0 when converged, 1 on invalid input or a device error, 2 at maxit, 3 on a breakdown,
+ * 4 on a non-finite residual (iters, rel_res and x filled for 0, 2, 3 and 4). */
+int caffe_csr_solve(int n, const int* row_ptr, const int* col, const double* val, const double* b, double* x,
+                    int method, double rtol, double atol, int maxit, int* iters, double* rel_res);
+/* y = A x for an m x n compressed-row matrix (host arrays): MatMult behind the reference's
+ * multiply(const SparseMatrix&, const SparseVector&, SparseVector&) (src/Math/SparseMatrix.cpp:132-135). */
+int caffe_csr_matvec(int m, int n, const int* row_ptr, const int* col, const double* val, const double* x, double* y);
+
 /* Learned preconditioner network (an extension; the reference has no learned component):
  * a 4-layer 3-D convolutional network with 3x3x3 kernels and 16 channels, BF16 weights and
  * activations, FP32 accumulation on the tensor cores.  Parameters are FP32, layer by layer:
