@@ -250,7 +250,7 @@ __global__ void __launch_bounds__(256) restrict_kernel(Dims3 fd, Dims3 cd, const
                                                        float scale, float* out, float* out2, float mul2, __nv_bfloat16* act0,
                                                        __nv_bfloat16* act0n, const float* maskc, float chan, const Scal* S) {
     if (S && S->done) return;
-    __shared__ float s0[RFK][RFJ][RFI];
+    __shared__ __align__(16) float s0[RFK][RFJ][RFI];
     __shared__ float t1[RFK][RFJ][RCI];
     __shared__ float t2[RFK][RCJ][RCI];
     __shared__ float wI[RCI][4], wJ[RCJ][4], wK[RCK][4];   // clamped trilinear weights of this tile
@@ -267,37 +267,55 @@ __global__ void __launch_bounds__(256) restrict_kernel(Dims3 fd, Dims3 cd, const
         int u = threadIdx.x - 4 * RCI - 4 * RCJ, ck = u >> 2, m = u & 3, K = K0 + ck;
         wK[ck][m] = rweight_in(2 * K - 1 + m, fd.n2, K, cd.n2);
     }
-    // stage the fine tile: one warp per (j, k) row of RFI cells, lanes along i; the three loads
-    // of an element are independent
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarp = blockDim.x >> 5;
+    // stage the fine tile: one warp per (j, k) row of RFI cells, lanes along i; all loads of a row's
+    // three 32-cell chunks are issued before any is stored
     for (int row = warp; row < RFJ * RFK; row += nwarp) {
         const int lj = row % RFJ, lk = row / RFJ;
         const int fj = fj0 + lj, fk = fk0 + lk;
         const bool rowIn = fj >= 0 && fj < fd.n1 && fk >= 0 && fk < fd.n2;
         const unsigned rowBase = rowIn ? (unsigned)fk * fsK + (unsigned)fj * fsJ : 0u;
+        constexpr int CH = (RFI + 31) / 32;
+        float fv[CH], dv[CH];
+        uint8_t sv[CH];
+        bool in[CH];
 #pragma unroll
-        for (int li = lane; li < RFI + 31; li += 32) {
-            if (li >= RFI) break;
-            const int fi = fi0 + li;
-            const bool in = rowIn && fi >= 0 && fi < fd.n0;
-            const unsigned f = in ? rowBase + (unsigned)fi : 0u;
-            const float fv = (in && fin) ? __ldg(fin + f) : 1.f;
-            const float dv = (in && invD) ? __ldg(invD + f) : 1.f;
-            const uint8_t sv = (in && st) ? __ldg(st + f) : (uint8_t)ST_ACTIVE;
-            s0[lk][lj][li] = (in && sv == ST_ACTIVE) ? fv * dv : 0.f;
+        for (int u = 0; u < CH; ++u) {
+            const int li = lane + 32 * u, fi = fi0 + li;
+            in[u] = rowIn && li < RFI && fi >= 0 && fi < fd.n0;
+            const unsigned f = in[u] ? rowBase + (unsigned)fi : 0u;
+            fv[u] = (in[u] && fin) ? __ldg(fin + f) : 1.f;
+            dv[u] = (in[u] && invD) ? __ldg(invD + f) : 1.f;
+            sv[u] = (in[u] && st) ? __ldg(st + f) : (uint8_t)ST_ACTIVE;
+        }
+#pragma unroll
+        for (int u = 0; u < CH; ++u) {
+            const int li = lane + 32 * u;
+            if (li < RFI) s0[lk][lj][li] = (in[u] && sv[u] == ST_ACTIVE) ? fv[u] * dv[u] : 0.f;
         }
     }
     __syncthreads();
-    for (int u = threadIdx.x; u < RFK * RFJ * RCI; u += blockDim.x) {
-        const int ci = u & (RCI - 1), rest = u / RCI, lj = rest % RFJ, lk = rest / RFJ;
-        const float* src = &s0[lk][lj][2 * ci];
-        t1[lk][lj][ci] = wI[ci][0] * src[0] + wI[ci][1] * src[1] + wI[ci][2] * src[2] + wI[ci][3] * src[3];
+    // blockDim.x is a multiple of RCI * RCJ, so a thread keeps one coarse column ci (pass 1) and one
+    // (ci, cj) pair (pass 2) for all its outputs: their weights stay in registers, and pass 1 reads
+    // its four fine values as two 8-byte pairs (2 ci is even)
+    {
+        const int ci = threadIdx.x & (RCI - 1);
+        const float w0 = wI[ci][0], w1 = wI[ci][1], w2 = wI[ci][2], w3 = wI[ci][3];
+        for (int u = threadIdx.x; u < RFK * RFJ * RCI; u += blockDim.x) {
+            const int rest = u / RCI, lj = rest % RFJ, lk = rest / RFJ;
+            const float2 a01 = *reinterpret_cast<const float2*>(&s0[lk][lj][2 * ci]);
+            const float2 a23 = *reinterpret_cast<const float2*>(&s0[lk][lj][2 * ci + 2]);
+            t1[lk][lj][ci] = w0 * a01.x + w1 * a01.y + w2 * a23.x + w3 * a23.y;
+        }
     }
     __syncthreads();
-    for (int u = threadIdx.x; u < RFK * RCJ * RCI; u += blockDim.x) {
-        const int ci = u & (RCI - 1), cj = (u / RCI) & (RCJ - 1), lk = u / (RCI * RCJ);
-        t2[lk][cj][ci] = wJ[cj][0] * t1[lk][2 * cj][ci] + wJ[cj][1] * t1[lk][2 * cj + 1][ci] + wJ[cj][2] * t1[lk][2 * cj + 2][ci] +
-                         wJ[cj][3] * t1[lk][2 * cj + 3][ci];
+    {
+        const int ci = threadIdx.x & (RCI - 1), cj = (threadIdx.x / RCI) & (RCJ - 1);
+        const float w0 = wJ[cj][0], w1 = wJ[cj][1], w2 = wJ[cj][2], w3 = wJ[cj][3];
+        for (int u = threadIdx.x; u < RFK * RCJ * RCI; u += blockDim.x) {
+            const int lk = u / (RCI * RCJ);
+            t2[lk][cj][ci] = w0 * t1[lk][2 * cj][ci] + w1 * t1[lk][2 * cj + 1][ci] + w2 * t1[lk][2 * cj + 2][ci] + w3 * t1[lk][2 * cj + 3][ci];
+        }
     }
     __syncthreads();
     for (int u = threadIdx.x; u < RCK * RCJ * RCI; u += blockDim.x) {
@@ -374,6 +392,29 @@ __device__ __forceinline__ void prolong4(const Dims3& fd, const Dims3& cd, const
     const float* r01 = wc + (unsigned)K0 * sK + (unsigned)J1 * sJ;
     const float* r10 = wc + (unsigned)K1 * sK + (unsigned)J0 * sJ;
     const float* r11 = wc + (unsigned)K1 * sK + (unsigned)J1 * sJ;
+    if ((fi & 1) == 0) {
+        // the four fine cells fi .. fi+3 draw on coarse columns F-1 .. F+2 (F = fi / 2, clamped):
+        // each of the four coarse rows is loaded once, 16 loads in all, and every fine value is
+        // blended in the same order as prolong_at's
+        const int F = fi >> 1;
+        const int col[4] = {pclamp(F - 1, cd.n0), F, pclamp(F + 1, cd.n0), pclamp(F + 2, cd.n0)};
+        float v00[4], v01[4], v10[4], v11[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            v00[u] = __ldg(r00 + col[u]); v01[u] = __ldg(r01 + col[u]);
+            v10[u] = __ldg(r10 + col[u]); v11[u] = __ldg(r11 + col[u]);
+        }
+        // (I0, I1) slots of fine cells fi, fi+1, fi+2, fi+3: (F, F-1), (F, F+1), (F+1, F), (F+1, F+2)
+        const int s0[4] = {1, 1, 2, 2}, s1[4] = {0, 2, 1, 3};
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+            auto row = [&](const float (&v)[4]) { return 0.75f * v[s0[m]] + 0.25f * v[s1[m]]; };
+            float k0 = 0.75f * row(v00) + 0.25f * row(v01);
+            float k1 = 0.75f * row(v10) + 0.25f * row(v11);
+            out[m] = 0.75f * k0 + 0.25f * k1;
+        }
+        return;
+    }
     // the four fine cells draw on coarse columns I-1 .. I+2 around I = fi / 2
 #pragma unroll
     for (int m = 0; m < 4; ++m) {
@@ -629,12 +670,60 @@ __global__ void __launch_bounds__(LB) bs_z_kernel(long long N, Dims3 fd, Dims3 c
         y[c] = zv;
     }
 }
+// A x for the 4 consecutive cells 4q .. 4q+3 (nI and nI*nJ multiples of 4, so every neighbouring
+// group of 4 is 16-byte aligned): 14 loads for the 4 rows instead of 14 per row.  The west /
+// south / bottom coefficients of a cell are the east / north / top ones of that neighbour.
+__device__ __forceinline__ void spmv4(const OpSymF32& A, const float* x, long long q, float (&Y)[4]) {
+    const long long c = 4 * q;
+    float P[4], E[4], Nn[4], T[4], Sn[4], B[4], X[4], XN[4], XS[4], XT[4], XB[4];
+    un4(ld4(A.aP, q), P); un4(ld4(A.aE, q), E); un4(ld4(A.aN, q), Nn); un4(ld4(A.aT, q), T);
+    un4(ld4(A.aN, q - A.nI / 4), Sn); un4(ld4(A.aT, q - A.nIJ / 4), B);
+    un4(ld4(x, q), X); un4(ld4(x, q + A.nI / 4), XN); un4(ld4(x, q - A.nI / 4), XS);
+    un4(ld4(x, q + A.nIJ / 4), XT); un4(ld4(x, q - A.nIJ / 4), XB);
+    const float eW = __ldg(A.aE + c - 1), xW = x[c - 1], xE = x[c + 4];
+    const float W[4] = {eW, E[0], E[1], E[2]};
+    const float xl[4] = {xW, X[0], X[1], X[2]};
+    const float xr[4] = {X[1], X[2], X[3], xE};
+#pragma unroll
+    for (int m = 0; m < 4; ++m)
+        Y[m] = P[m] * X[m] + E[m] * xr[m] + W[m] * xl[m] + Nn[m] * XN[m] + Sn[m] * XS[m] + T[m] * XT[m] + B[m] * XB[m];
+    if (A.gh.n > 0) {
+        const uint32_t bits = (__ldg(A.gh.bits + (c >> 5)) >> (c & 31)) & 0xFu;
+        if (bits)
+#pragma unroll
+            for (int m = 0; m < 4; ++m)
+                if ((bits >> m) & 1u) Y[m] = applyF(A, c + m, [&](long long e_) { return x[e_]; });
+    }
+}
+
 // out = A x; partial (a1, out), or with b2: (b2, out) and (out, out)
+template <bool V4>
 __global__ void __launch_bounds__(LB) bs_spmv_kernel(OpSymF32 A, long long N, const float* x, float* out, const float* a1, const float* b2,
                                                      double* part, const Scal* S) {
     if (S->done) return;
     double a[2] = {0., 0.};
-    for (long long c = blockIdx.x * (long long)LB + threadIdx.x; c < N; c += (long long)gridDim.x * LB) {
+    long long c0 = 0;
+    if (V4) {
+        const long long NQ = N >> 2;
+        for (long long q = blockIdx.x * (long long)LB + threadIdx.x; q < NQ; q += (long long)gridDim.x * LB) {
+            float Y[4];
+            spmv4(A, x, q, Y);
+            st4(out, q, Y);
+            if (b2) {
+                float Bv[4];
+                un4(ld4(b2, q), Bv);
+#pragma unroll
+                for (int m = 0; m < 4; ++m) { a[0] += (double)Bv[m] * Y[m]; a[1] += (double)Y[m] * Y[m]; }
+            } else {
+                float Av[4];
+                un4(ld4(a1, q), Av);
+#pragma unroll
+                for (int m = 0; m < 4; ++m) a[0] += (double)Av[m] * Y[m];
+            }
+        }
+        c0 = 4 * NQ;
+    }
+    for (long long c = c0 + blockIdx.x * (long long)LB + threadIdx.x; c < N; c += (long long)gridDim.x * LB) {
         float y = applyF(A, c, [&](long long e_) { return x[e_]; });
         out[c] = y;
         if (b2) { a[0] += (double)b2[c] * y; a[1] += (double)y * y; }
@@ -823,9 +912,20 @@ __global__ void __launch_bounds__(LB) scale_partial_kernel(long long N, const fl
     block_sums(a, 1, part);
 }
 // w = A z (FP32, with the ghost rows)
+template <bool V4>
 __global__ void __launch_bounds__(LB) fg_spmv_kernel(OpSymF32 A, long long N, const float* z, float* w, const Scal* S) {
     if (S->done) return;
-    for (long long c = blockIdx.x * (long long)LB + threadIdx.x; c < N; c += (long long)gridDim.x * LB)
+    long long c0 = 0;
+    if (V4) {
+        const long long NQ = N >> 2;
+        for (long long q = blockIdx.x * (long long)LB + threadIdx.x; q < NQ; q += (long long)gridDim.x * LB) {
+            float Y[4];
+            spmv4(A, z, q, Y);
+            st4(w, q, Y);
+        }
+        c0 = 4 * NQ;
+    }
+    for (long long c = c0 + blockIdx.x * (long long)LB + threadIdx.x; c < N; c += (long long)gridDim.x * LB)
         w[c] = applyF(A, c, [&](long long e_) { return z[e_]; });
 }
 // part[i * FG_DOT_BLOCKS + chunk] = sum over the chunk of w . v_i, i = blockIdx.x
@@ -1089,6 +1189,8 @@ int learned_solve(LearnedWork& lw, const OpSym& A, const uint8_t* status, const 
     CB_CHECK_LAUNCH();
     const Dims3 fd = dims_of(lw.lev[0]), cd = level1_dims(lw);
     const bool nonsym = A.gh.n > 0;
+    // 4-cell vector rows: neighbouring groups of 4 cells stay 16-byte aligned
+    const bool v4 = (L.nI % 4) == 0 && (L.nIJ % 4) == 0;
     int method = lw.inner;
     if (method == LEARN_INNER_AUTO)
         method = !nonsym ? LEARN_INNER_FCG : (mode == NET_MODE_NETWORK ? LEARN_INNER_FGMRES : LEARN_INNER_BICGSTAB);
@@ -1151,7 +1253,8 @@ int learned_solve(LearnedWork& lw, const OpSym& A, const uint8_t* status, const 
                     scale_finish<<<1, LB, 0, st>>>(lw.part, nb, S);
                     if (apply_levels(lw, vj, status, mode, S, st)) return 1;
                     bs_z_kernel<<<nb, LB, 0, st>>>(N, fd, cd, vj, lw.invD, status, w1, zj, S);
-                    fg_spmv_kernel<<<nb, LB, 0, st>>>(Af, N, zj, lw.t, S);
+                    if (v4) fg_spmv_kernel<true><<<nb, LB, 0, st>>>(Af, N, zj, lw.t, S);
+                    else fg_spmv_kernel<false><<<nb, LB, 0, st>>>(Af, N, zj, lw.t, S);
                     // classical Gram-Schmidt with one re-orthogonalisation (CGS2): FP32 vectors lose
                     // orthogonality in a single pass once the preconditioner is strong
                     for (int pass = 0; pass < 2; ++pass) {
@@ -1202,13 +1305,15 @@ int learned_solve(LearnedWork& lw, const OpSym& A, const uint8_t* status, const 
                         scale_finish<<<1, LB, 0, st>>>(lw.part, nb, S);
                         if (apply_levels(lw, lw.p[0], status, mode, S, st)) return 1;
                         bs_z_kernel<<<nb, LB, 0, st>>>(N, fd, cd, lw.p[0], lw.invD, status, w1, lw.p[1], S);
-                        bs_spmv_kernel<<<nb, LB, 0, st>>>(Af, N, lw.p[1], lw.q[0], lw.rh, nullptr, lw.part, S);
+                        if (v4) bs_spmv_kernel<true><<<nb, LB, 0, st>>>(Af, N, lw.p[1], lw.q[0], lw.rh, nullptr, lw.part, S);
+                        else bs_spmv_kernel<false><<<nb, LB, 0, st>>>(Af, N, lw.p[1], lw.q[0], lw.rh, nullptr, lw.part, S);
                         bs_alpha_finish<<<1, LB, 0, st>>>(lw.part, nb, S);
                         bs_s_kernel<<<nb, LB, 0, st>>>(N, lw.r, lw.q[0], lw.invD, status, lw.z, lw.part, S);
                         scale_finish<<<1, LB, 0, st>>>(lw.part, nb, S);
                         if (apply_levels(lw, lw.z, status, mode, S, st)) return 1;
                         bs_z_kernel<<<nb, LB, 0, st>>>(N, fd, cd, lw.z, lw.invD, status, w1, lw.q[1], S);
-                        bs_spmv_kernel<<<nb, LB, 0, st>>>(Af, N, lw.q[1], lw.t, nullptr, lw.z, lw.part, S);
+                        if (v4) bs_spmv_kernel<true><<<nb, LB, 0, st>>>(Af, N, lw.q[1], lw.t, nullptr, lw.z, lw.part, S);
+                        else bs_spmv_kernel<false><<<nb, LB, 0, st>>>(Af, N, lw.q[1], lw.t, nullptr, lw.z, lw.part, S);
                         bs_omega_finish<<<1, LB, 0, st>>>(lw.part, nb, S);
                         bs_update_kernel<<<nb, LB, 0, st>>>(N, lw.e, lw.r, lw.p[1], lw.q[1], lw.z, lw.t, lw.rh, lw.part, S);
                         bs_update_finish<<<1, LB, 0, st>>>(lw.part, nb, S, maxit);
