@@ -22,6 +22,7 @@
 // Every wait on the MMA-completion mbarrier is bounded; a CTA that times out records an
 // error, waits once more (bounded) and frees its tensor memory before leaving.
 #include <cuda_bf16.h>
+#include <algorithm>
 #include <cstdint>
 
 #include "common.cuh"
@@ -265,6 +266,183 @@ __global__ void __launch_bounds__(128) conv3d_tc_kernel(Lat L, const __nv_bfloat
 }
 
 size_t conv_smem_bytes() { return 1024 + W_BYTES + NBUF * BUF_BYTES; }
+
+// ------------------------------------------------------------------ weight gradient
+// dW[t][o][i] = sum_c x[c + off(t)][i] dz[c][o] (db[o] = sum_c dz[c][o]) as an implicit GEMM on the
+// tensor cores: D[(t, i)][o] = sum_c A[(t, i)][c] B[o][c] with M = 128 rows = 8 taps x 16 input
+// channels (four M tiles cover the 27 taps; rows of taps 27..31 are zero), N = 16 output channels
+// and K = the cells, 16 per tcgen05.mma.  A CTA (128 threads) takes chunks of 16 consecutive cells
+// along i, builds for each chunk the im2col tile A (taps x channels x cells) and the tile B
+// (dz, channels x cells) in shared memory in the canonical no-swizzle K-major layout, and one
+// thread issues the chunk's four MMAs into four 128 x 16 FP32 accumulators in tensor memory that
+// stay there for all the CTA's chunks.  Two staging buffers alternate, so the next chunk is built
+// while the MMAs of the previous one run.  At the end every thread reads its accumulator row
+// (tcgen05.ld) and adds it to the FP32 gradient.
+namespace {
+constexpr int WG_CH = 16;                          // cells per chunk (the MMA's K)
+constexpr int WG_TILE_BYTES = 16 * 256;            // 16 row groups of 8 rows x 2 K groups x 16 bytes
+constexpr int WG_A_BYTES = 4 * WG_TILE_BYTES;      // four M tiles
+constexpr int WG_B_BYTES = 512;                    // 16 x 16 bf16
+constexpr int WG_STAGE_BYTES = WG_A_BYTES + WG_B_BYTES;
+constexpr uint32_t WG_TMEM_COLS = 64;              // four 16-column accumulators
+
+// byte offset of element (row m, K column k) in a canonical no-swizzle K-major tile
+__device__ __forceinline__ int kmajor_off(int m, int k) { return (m >> 3) * 256 + (k >> 3) * 128 + (m & 7) * 16 + (k & 7) * 2; }
+}  // namespace
+
+__global__ void __launch_bounds__(128) weight_grad_tc_kernel(Lat L, const __nv_bfloat16* __restrict__ x, const __nv_bfloat16* __restrict__ dz,
+                                                             float* dW, float* db, int* err) {
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    __shared__ __align__(8) uint64_t mbar[2];
+    __shared__ uint32_t tmem_base_sh;
+    const int warp = threadIdx.x >> 5;
+    const int chunksI = (L.nI + WG_CH - 1) / WG_CH;
+    const long long nChunks = (long long)chunksI * L.nJ * L.nK;
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[0])));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[1])));
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base_sh)),
+                     "r"(WG_TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    const uint32_t tmem = tmem_base_sh;
+    const uint32_t bar[2] = {smem_u32(&mbar[0]), smem_u32(&mbar[1])};
+    uint32_t phase[2] = {0u, 0u};
+    bool pending[2] = {false, false};
+    bool failed = false;
+    float dbs[16];
+#pragma unroll
+    for (int o = 0; o < 16; ++o) dbs[o] = 0.f;
+    int n = 0;
+    for (long long u = blockIdx.x; u < nChunks; u += gridDim.x, ++n) {
+        const int s = n & 1;
+        // the MMAs that read this staging buffer two chunks ago must have finished
+        if (pending[s]) {
+            bool ok = mbar_wait_bounded(bar[s], phase[s]);
+            // a wait that ran out keeps its phase and stays pending: the drain below waits for
+            // those MMAs once more (bounded) before the tensor memory is freed
+            if (ok) { phase[s] ^= 1u; pending[s] = false; }
+            if (__syncthreads_or(ok ? 0 : 1)) { failed = true; break; }
+        }
+        unsigned char* A = smem + s * WG_STAGE_BYTES;
+        unsigned char* B = A + WG_A_BYTES;
+        const int ci = (int)(u % chunksI);
+        const long long rest = u / chunksI;
+        const int j = (int)(rest % L.nJ), k = (int)(rest / L.nJ);
+        const int i0 = ci * WG_CH;
+        // A: 32 taps x 16 cells, one (tap, cell) pair = 16 channels per step
+        for (int p = threadIdx.x; p < 32 * WG_CH; p += blockDim.x) {
+            const int cell = p & (WG_CH - 1), t = p / WG_CH;
+            uint4 lo = make_uint4(0u, 0u, 0u, 0u), hi = lo;
+            if (t < 27) {
+                const int ii = i0 + cell + t % 3 - 1, jj = j + (t / 3) % 3 - 1, kk = k + t / 9 - 1;
+                if (ii >= 0 && ii < L.nI && jj >= 0 && jj < L.nJ && kk >= 0 && kk < L.nK) {
+                    const uint4* src = reinterpret_cast<const uint4*>(x + (((long long)kk * L.nJ + jj) * L.nI + ii) * 16);
+                    lo = src[0];
+                    hi = src[1];
+                }
+            }
+            const __nv_bfloat16* vl = reinterpret_cast<const __nv_bfloat16*>(&lo);
+            const __nv_bfloat16* vh = reinterpret_cast<const __nv_bfloat16*>(&hi);
+            unsigned char* tile = A + (t >> 3) * WG_TILE_BYTES;
+            const int m0 = (t & 7) * 16;
+#pragma unroll
+            for (int ch = 0; ch < 8; ++ch) {
+                *reinterpret_cast<__nv_bfloat16*>(tile + kmajor_off(m0 + ch, cell)) = vl[ch];
+                *reinterpret_cast<__nv_bfloat16*>(tile + kmajor_off(m0 + 8 + ch, cell)) = vh[ch];
+            }
+        }
+        // B: dz of the chunk's cells (zero beyond the row), and the bias gradient
+        if (threadIdx.x < WG_CH) {
+            const int cell = threadIdx.x, ii = i0 + cell;
+            uint4 lo = make_uint4(0u, 0u, 0u, 0u), hi = lo;
+            if (ii < L.nI) {
+                const uint4* src = reinterpret_cast<const uint4*>(dz + (((long long)k * L.nJ + j) * L.nI + ii) * 16);
+                lo = src[0];
+                hi = src[1];
+            }
+            const __nv_bfloat16* vl = reinterpret_cast<const __nv_bfloat16*>(&lo);
+            const __nv_bfloat16* vh = reinterpret_cast<const __nv_bfloat16*>(&hi);
+#pragma unroll
+            for (int o = 0; o < 8; ++o) {
+                *reinterpret_cast<__nv_bfloat16*>(B + kmajor_off(o, cell)) = vl[o];
+                *reinterpret_cast<__nv_bfloat16*>(B + kmajor_off(8 + o, cell)) = vh[o];
+                dbs[o] += __bfloat162float(vl[o]);
+                dbs[8 + o] += __bfloat162float(vh[o]);
+            }
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        asm volatile("tcgen05.fence::before_thread_sync;");
+        __syncthreads();
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        if (threadIdx.x == 0) {
+            const uint64_t bd = sdesc(smem_u32(B), 128, 256);
+#pragma unroll 1
+            for (int T = 0; T < 4; ++T) {
+                const uint64_t ad = sdesc(smem_u32(A + T * WG_TILE_BYTES), 128, 256);
+                mma_bf16(tmem + (uint32_t)(16 * T), ad, bd, n > 0 ? 1u : 0u);
+            }
+            mma_commit(bar[s]);
+        }
+        pending[s] = true;
+    }
+    // drain: every committed group completes before the accumulators are read or freed
+    for (int q = 0; q < 2; ++q) {
+        if (!pending[q]) continue;
+        bool ok = mbar_wait_bounded(bar[q], phase[q]);
+        phase[q] ^= 1u;
+        if (!ok) failed = true;
+    }
+    const bool anyFail = __syncthreads_or(failed ? 1 : 0);
+    if (anyFail) {
+        if (threadIdx.x == 0) atomicExch(err, 1);
+    } else if (n > 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        // thread = accumulator row m = (tap, input channel) of each M tile
+        const int m = threadIdx.x, tl = m >> 4, ch = m & 15;
+#pragma unroll 1
+        for (int T = 0; T < 4; ++T) {
+            float v[16];
+            tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(16 * T), v);
+            const int t = 8 * T + tl;
+            if (t < 27)
+#pragma unroll
+                for (int o = 0; o < 16; ++o) atomicAdd(dW + (t * 16 + o) * 16 + ch, v[o]);
+        }
+        if (threadIdx.x < WG_CH)
+#pragma unroll
+            for (int o = 0; o < 16; ++o) atomicAdd(db + o, dbs[o]);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(WG_TMEM_COLS));
+}
+
+int launch_weight_grad(const Lat& L, const __nv_bfloat16* x, const __nv_bfloat16* dz, float* dW, float* db, int* err, cudaStream_t st) {
+    const size_t smem = 1024 + 2 * (size_t)WG_STAGE_BYTES;
+    static bool attr = false;
+    if (!attr) {
+        CB_CUDA(cudaFuncSetAttribute(weight_grad_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        attr = true;
+    }
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    const long long nChunks = (long long)((L.nI + WG_CH - 1) / WG_CH) * L.nJ * L.nK;
+    // a few CTAs per SM, each accumulating many chunks in tensor memory before its atomics
+    const long long g = std::min<long long>(nChunks, 4LL * nsm);
+    weight_grad_tc_kernel<<<(unsigned)(g > 0 ? g : 1), 128, smem, st>>>(L, x, dz, dW, db, err);
+    CB_CHECK_LAUNCH();
+    return 0;
+}
 
 int launch_conv3d(const Lat& L, int epi, const __nv_bfloat16* in, const __nv_bfloat16* wpack, const float* bias, __nv_bfloat16* out_bf,
                   float* out_f, const __nv_bfloat16* mask_act, int* err, cudaStream_t st, const int* skip) {

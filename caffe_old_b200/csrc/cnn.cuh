@@ -22,6 +22,10 @@ size_t conv_smem_bytes();
 int launch_conv3d(const Lat& L, int epi, const __nv_bfloat16* in, const __nv_bfloat16* wpack, const float* bias, __nv_bfloat16* out_bf,
                   float* out_f, const __nv_bfloat16* mask_act, int* err, cudaStream_t st, const int* skip = nullptr);
 
+// Weight gradient of one layer on the tensor cores: dW[t][o][i] += sum_c x[c + off(t)][i] dz[c][o],
+// db[o] += sum_c dz[c][o] (FP32, accumulated into dW / db).
+int launch_weight_grad(const Lat& L, const __nv_bfloat16* x, const __nv_bfloat16* dz, float* dW, float* db, int* err, cudaStream_t st);
+
 // Device buffers of one network applied on one lattice.
 struct NetBuffers {
     Lat L;

@@ -56,55 +56,6 @@ __global__ void pack_dy_kernel(long long N, const float* __restrict__ dy, __nv_b
     dst[1] = reinterpret_cast<uint4*>(v)[1];
 }
 
-// Weight gradient of one layer on the CUDA cores (FP32):
-//   dW[t][o][i] += sum_c x[c + off(t)][i] * dz[c][o],   db[o] += sum_c dz[c][o].
-// A block owns an 8 x 16 tile of cells and marches through DK k-planes; thread (o, i) keeps
-// the 27 tap sums of its (o, i) pair and adds them to the global gradient at the end.
-constexpr int GW_TI = 8, GW_TJ = 16, GW_DK = 16;
-__global__ void __launch_bounds__(256) weight_grad_kernel(Lat L, const __nv_bfloat16* __restrict__ x, const __nv_bfloat16* __restrict__ dz,
-                                                          float* dW, float* db) {
-    __shared__ float xs[3][GW_TJ + 2][GW_TI + 2][16];   // planes k-1, k, k+1 with halo
-    __shared__ float zs[GW_TJ][GW_TI][16];
-    const int o = threadIdx.x >> 4, ii = threadIdx.x & 15;
-    const int i0 = blockIdx.x * GW_TI, j0 = blockIdx.y * GW_TJ, k0 = blockIdx.z * GW_DK;
-    const int k1 = min(k0 + GW_DK, L.nK);
-    float acc[27];
-#pragma unroll
-    for (int t = 0; t < 27; ++t) acc[t] = 0.f;
-    float bacc = 0.f;
-    for (int k = k0; k < k1; ++k) {
-        __syncthreads();
-        for (int u = threadIdx.x; u < 3 * (GW_TJ + 2) * (GW_TI + 2); u += blockDim.x) {
-            int il = u % (GW_TI + 2), jl = (u / (GW_TI + 2)) % (GW_TJ + 2), s = u / ((GW_TI + 2) * (GW_TJ + 2));
-            int i = i0 + il - 1, j = j0 + jl - 1, kk = k + s - 1;
-            bool in = i >= 0 && i < L.nI && j >= 0 && j < L.nJ && kk >= 0 && kk < L.nK;
-            long long c = in ? ((long long)kk * L.nJ + j) * L.nI + i : 0;
-            for (int q = 0; q < 16; ++q) xs[s][jl][il][q] = in ? __bfloat162float(x[c * 16 + q]) : 0.f;
-        }
-        for (int u = threadIdx.x; u < GW_TJ * GW_TI; u += blockDim.x) {
-            int il = u % GW_TI, jl = u / GW_TI;
-            int i = i0 + il, j = j0 + jl;
-            bool in = i < L.nI && j < L.nJ;
-            long long c = in ? ((long long)k * L.nJ + j) * L.nI + i : 0;
-            for (int q = 0; q < 16; ++q) zs[jl][il][q] = in ? __bfloat162float(dz[c * 16 + q]) : 0.f;
-        }
-        __syncthreads();
-        for (int jl = 0; jl < GW_TJ; ++jl)
-            for (int il = 0; il < GW_TI; ++il) {
-                float zv = zs[jl][il][o];
-                if (ii == 0) bacc += zv;
-#pragma unroll
-                for (int t = 0; t < 27; ++t) {
-                    int dk = t / 9, dj = (t / 3) % 3, di = t % 3;
-                    acc[t] += xs[dk][jl + dj][il + di][ii] * zv;
-                }
-            }
-    }
-#pragma unroll
-    for (int t = 0; t < 27; ++t) atomicAdd(dW + (t * 16 + o) * 16 + ii, acc[t]);
-    if (ii == 0) atomicAdd(db + o, bacc);
-}
-
 }  // namespace
 
 int net_alloc(NetBuffers& nb, const Lat& L, void* (*alloc)(size_t, void*), void* ctx) {
@@ -162,12 +113,8 @@ int net_forward_if(NetBuffers& nb, const int* skip, cudaStream_t st) {
 int net_forward(NetBuffers& nb, cudaStream_t st) { return net_forward_if(nb, nullptr, st); }
 
 static int weight_grad(NetBuffers& nb, int l, const __nv_bfloat16* x, const __nv_bfloat16* dz, cudaStream_t st) {
-    const Lat& L = nb.L;
-    dim3 grid((L.nI + GW_TI - 1) / GW_TI, (L.nJ + GW_TJ - 1) / GW_TJ, (L.nK + GW_DK - 1) / GW_DK);
     float* g = nb.grad + (size_t)l * NET_LAYER_PARAMS;
-    weight_grad_kernel<<<grid, 256, 0, st>>>(L, x, dz, g, g + 27 * 256);
-    CB_CHECK_LAUNCH();
-    return 0;
+    return launch_weight_grad(nb.L, x, dz, g, g + 27 * 256, nb.err, st);
 }
 
 int net_backward(NetBuffers& nb, const float* dy, cudaStream_t st) {

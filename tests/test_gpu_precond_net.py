@@ -1,4 +1,4 @@
-"""Tensor-core network kernels (forward and backward) against the CPU FP64 restatement with
+"""Tensor-core network kernels (forward, backward data and weight gradient) against the CPU FP64 restatement with
 bf16 rounding at the same points.  Tolerances: 2e-2 relative L2 on the output and on each
 layer's gradient block (bf16 has an 8-bit mantissa; FP32 vs FP64 accumulation can flip a
 rounding)."""
@@ -39,8 +39,10 @@ def test_forward_matches_fp64_reference(shape):
     assert err < TOL, err
 
 
-def test_gradients_match_fp64_reference():
-    shape = (20, 18, 12)
+@pytest.mark.parametrize("shape", [(20, 18, 12), (37, 5, 21)])
+def test_gradients_match_fp64_reference(shape):
+    """Backward data (tcgen05) and the weight gradient (tcgen05 implicit GEMM over the cells,
+    including rows whose last 16-cell chunk is partly outside the lattice)."""
     n = int(np.prod(shape))
     rng = np.random.default_rng(4)
     params = R.random_params(2)
