@@ -10,20 +10,31 @@
 // stages plane k+2.  For each output plane the tile is one UMMA problem
 // M = 128 cells, N = 16 output channels, accumulated over the 27 taps with one
 // tcgen05.mma.kind::f16 of K = 16 input channels per tap into a 128 x 16 FP32 accumulator
-// in tensor memory.  Operands are in shared memory in the canonical no-swizzle K-major
-// layout (core matrices of 8 rows x 16 bytes): the A operand of tap (dk, dj, di) is input
-// plane k+dk shifted by di along i (three i-shifted copies of each plane are staged) and
-// by dj rows of the tile (a whole-core-matrix offset in the descriptor); B is the tap's
-// 16 x 16 weight block.  Input planes rotate through the staging slots as the CTA moves along k, so each input
-// plane is read from global memory once per tile.  The epilogue reads the accumulator with
+// in tensor memory.  The input planes arrive by TMA (cp.async.bulk.tensor, one thread issuing,
+// completion on a per-slot mbarrier): a box of 8 (i) x 18 (j, one halo row each side) cells x 16
+// channels lands as rows of 32 bytes (one cell's channels) with the 32-byte swizzle, which is the
+// K-major SWIZZLE_32B operand layout of the MMA, so the A operand of tap (dk, dj, di) is input
+// plane k+dk loaded at i offset di (three boxes per plane) and advanced by dj rows of 8 cells
+// (256 bytes) in the descriptor; cells outside the lattice arrive as zeros.  B is the tap's
+// 16 x 16 weight block (no-swizzle canonical layout).  Input planes rotate through the staging
+// slots as the CTA moves along k, so each input plane is read from global memory once per tile.
+// The tensor map covers this GPU's own activation buffer only (no cluster multicast).  The epilogue reads the accumulator with
 // tcgen05.ld (one TMEM lane per thread = one cell), applies bias / ReLU, or the ReLU mask
 // of the backward pass, and writes bf16 (or FP32 for the network output).
 //
 // Every wait on the MMA-completion mbarrier is bounded; a CTA that times out records an
 // error, waits once more (bounded) and frees its tensor memory before leaving.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_bf16.h>
 #include <algorithm>
+#include <array>
 #include <cstdint>
+#include <mutex>
+#include <utility>
+#include <vector>
+#include <cstring>
+#include <string>
 
 #include "common.cuh"
 #include "cnn.cuh"
@@ -100,26 +111,30 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
     for (int q = 0; q < 16; ++q) v[q] = __uint_as_float(r[q]);
 }
 
-// Stage input plane kk into the three i-shifted canonical buffers of rotation slot `slot`.
-__device__ __forceinline__ void stage_plane(unsigned char* bufs, int slot, const __nv_bfloat16* __restrict__ in, const Lat& L,
-                                            int i0, int j0, int kk) {
-    // units of 16 bytes: 3 shifts x ROWS rows x 8 cells x 2 chunks
-    const int total = 3 * ROWS * TI * 2;
-    for (int u = threadIdx.x; u < total; u += blockDim.x) {
-        int h = u & 1;
-        int il = (u >> 1) & 7;
-        int rest = u >> 4;
-        int jr = rest % ROWS;
-        int s = rest / ROWS;        // 0,1,2 -> di = -1,0,1
-        int i = i0 + il + s - 1, j = j0 + jr - 1;
-        uint4 val = make_uint4(0u, 0u, 0u, 0u);
-        if (kk >= 0 && kk < L.nK && i >= 0 && i < L.nI && j >= 0 && j < L.nJ) {
-            long long c = ((long long)kk * L.nJ + j) * L.nI + i;
-            val = *reinterpret_cast<const uint4*>(in + c * 16 + h * 8);
-        }
-        unsigned char* dst = bufs + (size_t)(slot * 3 + s) * BUF_BYTES + jr * GROUP_BYTES + h * 128 + il * 16;
-        *reinterpret_cast<uint4*>(dst) = val;
-    }
+// shared-memory matrix descriptor of a K-major SWIZZLE_32B operand: rows of 32 bytes (16 bf16 of
+// K), 8-row groups SBO bytes apart; the start address must be 256-byte aligned (base offset 0)
+__device__ __forceinline__ uint64_t sdesc_sw32(uint32_t saddr, uint32_t sbo) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
+    d |= (uint64_t)1 << 16;                                  // leading byte offset: 16 bytes (unused within the swizzle span)
+    d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+    d |= (uint64_t)1 << 46;
+    d |= (uint64_t)6 << 61;                                  // layout type SWIZZLE_32B
+    return d;
+}
+
+// TMA: one box of the activation tensor (channels, i, j, k) at coordinates (0, ci, cj, ck) into
+// shared memory, completion counted on mbarrier `bar`
+__device__ __forceinline__ void tma_load_box(uint32_t dst, const CUtensorMap* map, int ci, int cj, int ck, uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], [%6];"
+        :
+        : "r"(dst), "l"((uint64_t)map), "r"(0), "r"(ci), "r"(cj), "r"(ck), "r"(bar)
+        : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
 }
 
 }  // namespace
@@ -127,7 +142,7 @@ __device__ __forceinline__ void stage_plane(unsigned char* bufs, int slot, const
 // EPI: 0 bias + ReLU -> bf16; 1 bias -> FP32 channel 0 (network output); 2 backward data:
 // multiply by (mask_act > 0) -> bf16.  Weights: packed canonical blocks, 27 x 512 bytes.
 template <int EPI>
-__global__ void __launch_bounds__(128) conv3d_tc_kernel(Lat L, const __nv_bfloat16* __restrict__ in,
+__global__ void __launch_bounds__(128) conv3d_tc_kernel(Lat L, const __grid_constant__ CUtensorMap in_map,
                                                         const __nv_bfloat16* __restrict__ wpack, const float* __restrict__ bias,
                                                         __nv_bfloat16* out_bf, float* out_f, long long out_stride,
                                                         const __nv_bfloat16* __restrict__ mask_act, int KC, int* err,
@@ -140,8 +155,10 @@ __global__ void __launch_bounds__(128) conv3d_tc_kernel(Lat L, const __nv_bfloat
     unsigned char* wsm = smem;                                // W_BYTES
     unsigned char* bufs = smem + W_BYTES;                     // NBUF x BUF_BYTES
     __shared__ __align__(8) uint64_t mbar[2];
+    __shared__ __align__(8) uint64_t lbar[NPL];   // TMA completion, one per staging slot
     __shared__ uint32_t tmem_base_sh;
     __shared__ float bias_sh[16];
+    __shared__ int tma_fail_sh;
 
     const int i0 = blockIdx.x * TI, j0 = blockIdx.y * TJ;
     const int k0 = blockIdx.z * KC;
@@ -155,17 +172,36 @@ __global__ void __launch_bounds__(128) conv3d_tc_kernel(Lat L, const __nv_bfloat
     if (threadIdx.x == 0) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[0])));
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[1])));
+        for (int q = 0; q < NPL; ++q) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&lbar[q])));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        tma_fail_sh = 0;
     }
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base_sh)),
                      "r"(TMEM_COLS));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
-    // plane p lives in rotation slot (p - k0 + 1) mod 4; planes k0-1, k0, k0+1 first
+    // plane p lives in rotation slot (p - k0 + 1) mod 4; planes k0-1, k0, k0+1 first.  Thread 0
+    // issues every load and keeps, per slot, how many loads it has issued (the parity of the
+    // latest one is the phase to wait for).
     auto slot_of = [&](int plane) { return (plane - k0 + 1) & (NPL - 1); };
-    stage_plane(bufs, slot_of(k0 - 1), in, L, i0, j0, k0 - 1);
-    stage_plane(bufs, slot_of(k0), in, L, i0, j0, k0);
-    stage_plane(bufs, slot_of(k0 + 1), in, L, i0, j0, k0 + 1);
+    int loads[NPL] = {0, 0, 0, 0};
+    auto load_plane = [&](int plane) {
+        if (threadIdx.x != 0) return;
+        const int slot = slot_of(plane);
+        const uint32_t lb = smem_u32(&lbar[slot]);
+        mbar_expect_tx(lb, 3 * BUF_BYTES);
+        for (int sh = 0; sh < 3; ++sh)
+            tma_load_box(smem_u32(bufs + (size_t)(slot * 3 + sh) * BUF_BYTES), &in_map, i0 + sh - 1, j0 - 1, plane, lb);
+        ++loads[slot];
+    };
+    auto wait_plane = [&](int plane) -> bool {   // thread 0 only
+        const int slot = slot_of(plane);
+        return loads[slot] == 0 || mbar_wait_bounded(smem_u32(&lbar[slot]), (uint32_t)((loads[slot] - 1) & 1));
+    };
+    load_plane(k0 - 1);
+    load_plane(k0);
+    load_plane(k0 + 1);
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
@@ -181,6 +217,9 @@ __global__ void __launch_bounds__(128) conv3d_tc_kernel(Lat L, const __nv_bfloat
     // issued by one thread, completion signalled on bar[acc]
     auto issue = [&](int k, int acc) {
         if (threadIdx.x != 0) return;
+        // the three input planes must have landed; a load that never completes marks the CTA failed
+        // (its MMAs still run, on whatever the buffers hold, so that every wait below is satisfied)
+        if (!(wait_plane(k - 1) && wait_plane(k) && wait_plane(k + 1))) tma_fail_sh = 1;
         const uint32_t wbase = smem_u32(wsm);
         const uint32_t bbase = smem_u32(bufs);
         const int slots[3] = {slot_of(k - 1), slot_of(k), slot_of(k + 1)};
@@ -192,7 +231,7 @@ __global__ void __launch_bounds__(128) conv3d_tc_kernel(Lat L, const __nv_bfloat
 #pragma unroll 1
                 for (int di = 0; di < 3; ++di, ++t) {
                     uint32_t a_addr = bbase + (uint32_t)((slots[dk] * 3 + di) * BUF_BYTES + dj * GROUP_BYTES);
-                    uint64_t ad = sdesc(a_addr, 128, 256);
+                    uint64_t ad = sdesc_sw32(a_addr, 256);
                     uint64_t bd = sdesc(wbase + (uint32_t)(t * 512), 128, 256);
                     mma_bf16(tmem + (uint32_t)(16 * acc), ad, bd, t > 0 ? 1u : 0u);
                 }
@@ -205,8 +244,7 @@ __global__ void __launch_bounds__(128) conv3d_tc_kernel(Lat L, const __nv_bfloat
     if (k0 < k1) issue(k0, 0);
     for (int k = k0; k < k1; ++k) {
         const int acc = (k - k0) & 1;
-        if (k + 2 <= k1) stage_plane(bufs, slot_of(k + 2), in, L, i0, j0, k + 2);
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        if (k + 2 <= k1) load_plane(k + 2);
         asm volatile("tcgen05.fence::before_thread_sync;");
         __syncthreads();
         asm volatile("tcgen05.fence::after_thread_sync;");
@@ -214,7 +252,7 @@ __global__ void __launch_bounds__(128) conv3d_tc_kernel(Lat L, const __nv_bfloat
         bool ok = mbar_wait_bounded(bar[acc], phase[acc]);
         phase[acc] ^= 1u;
         // the decision to stop must be the same in every thread (barriers follow)
-        if (__syncthreads_or(ok ? 0 : 1)) {
+        if (__syncthreads_or((ok && !tma_fail_sh) ? 0 : 1)) {
             failed = true;
             accFail = acc;
             otherPending = k + 1 < k1;
@@ -258,6 +296,10 @@ __global__ void __launch_bounds__(128) conv3d_tc_kernel(Lat L, const __nv_bfloat
         // the tensor memory is freed
         mbar_wait_bounded(bar[accFail], phase[accFail] ^ 1u);        // the plane whose wait ran out
         if (otherPending) mbar_wait_bounded(bar[accFail ^ 1], phase[accFail ^ 1]);
+        // and the TMA loads still in flight before the shared memory goes away
+        if (threadIdx.x == 0)
+            for (int q = 0; q < NPL; ++q)
+                if (loads[q] > 0) mbar_wait_bounded(smem_u32(&lbar[q]), (uint32_t)((loads[q] - 1) & 1));
     }
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
@@ -444,8 +486,56 @@ int launch_weight_grad(const Lat& L, const __nv_bfloat16* x, const __nv_bfloat16
     return 0;
 }
 
+namespace {
+// cuTensorMapEncodeTiled from the driver, looked up once (no link-time dependency on libcuda)
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    return fn;
+}
+}  // namespace
+
+// Tensor map of a channel-last bf16 activation buffer (16 channels per cell) of lattice L: dims
+// (channel, i, j, k), box 16 x 8 x 18 x 1 (one staged plane of the convolution tile with its j
+// halo), 32-byte swizzle, zero fill outside the lattice.
+int make_act_tensor_map(CUtensorMap* map, const __nv_bfloat16* base, const Lat& L) {
+    PFN_cuTensorMapEncodeTiled_v12000 fn = encode_fn();
+    if (!fn) { set_error("cuTensorMapEncodeTiled is not available from the driver"); return 1; }
+    if (((uintptr_t)base & 15u) != 0) { set_error("activation buffer is not 16-byte aligned"); return 1; }
+    cuuint64_t dims[4] = {16, (cuuint64_t)L.nI, (cuuint64_t)L.nJ, (cuuint64_t)L.nK};
+    cuuint64_t strides[3] = {32, (cuuint64_t)32 * L.nI, (cuuint64_t)32 * L.nI * L.nJ};   // bytes, dims 1..3
+    cuuint32_t box[4] = {16, (cuuint32_t)TI, (cuuint32_t)ROWS, 1};
+    cuuint32_t estr[4] = {1, 1, 1, 1};
+    CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<__nv_bfloat16*>(base), dims, strides, box, estr,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_32B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) { set_error("cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")"); return 1; }
+    return 0;
+}
+
 int launch_conv3d(const Lat& L, int epi, const __nv_bfloat16* in, const __nv_bfloat16* wpack, const float* bias, __nv_bfloat16* out_bf,
                   float* out_f, const __nv_bfloat16* mask_act, int* err, cudaStream_t st, const int* skip) {
+    // encoded maps are kept per (buffer, lattice): the solve reuses the same few activation buffers
+    static std::vector<std::pair<std::array<long long, 4>, CUtensorMap>> cache;
+    static std::mutex cacheLock;
+    std::lock_guard<std::mutex> guard(cacheLock);
+    const std::array<long long, 4> key = {(long long)(uintptr_t)in, L.nI, L.nJ, L.nK};
+    const CUtensorMap* mp = nullptr;
+    for (auto& e : cache)
+        if (e.first == key) { mp = &e.second; break; }
+    if (!mp) {
+        CUtensorMap m;
+        if (make_act_tensor_map(&m, in, L)) return 1;
+        cache.emplace_back(key, m);
+        mp = &cache.back().second;
+    }
+    const CUtensorMap in_map = *mp;
     // k-planes per CTA: up to 16 (one staged plane serves three output planes), fewer on small
     // lattices so that the grid still covers the SMs twice
     const long long gxy = (long long)((L.nI + TI - 1) / TI) * ((L.nJ + TJ - 1) / TJ);
@@ -460,9 +550,9 @@ int launch_conv3d(const Lat& L, int epi, const __nv_bfloat16* in, const __nv_bfl
         CB_CUDA(cudaFuncSetAttribute(conv3d_tc_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         attr = true;
     }
-    if (epi == 0) conv3d_tc_kernel<0><<<grid, 128, smem, st>>>(L, in, wpack, bias, out_bf, out_f, 16, mask_act, KC, err, skip);
-    else if (epi == 1) conv3d_tc_kernel<1><<<grid, 128, smem, st>>>(L, in, wpack, bias, out_bf, out_f, 16, mask_act, KC, err, skip);
-    else conv3d_tc_kernel<2><<<grid, 128, smem, st>>>(L, in, wpack, bias, out_bf, out_f, 16, mask_act, KC, err, skip);
+    if (epi == 0) conv3d_tc_kernel<0><<<grid, 128, smem, st>>>(L, in_map, wpack, bias, out_bf, out_f, 16, mask_act, KC, err, skip);
+    else if (epi == 1) conv3d_tc_kernel<1><<<grid, 128, smem, st>>>(L, in_map, wpack, bias, out_bf, out_f, 16, mask_act, KC, err, skip);
+    else conv3d_tc_kernel<2><<<grid, 128, smem, st>>>(L, in_map, wpack, bias, out_bf, out_f, 16, mask_act, KC, err, skip);
     CB_CHECK_LAUNCH();
     return 0;
 }
