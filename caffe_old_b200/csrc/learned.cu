@@ -928,25 +928,6 @@ __global__ void __launch_bounds__(LB) fg_spmv_kernel(OpSymF32 A, long long N, co
     for (long long c = c0 + blockIdx.x * (long long)LB + threadIdx.x; c < N; c += (long long)gridDim.x * LB)
         w[c] = applyF(A, c, [&](long long e_) { return z[e_]; });
 }
-// part[i * FG_DOT_BLOCKS + chunk] = sum over the chunk of w . v_i, i = blockIdx.x
-__global__ void __launch_bounds__(LB) fg_dots_kernel(long long N, const float* w, const float* V, long long PS, double* part, const Scal* S) {
-    if (S->done) return;
-    const int i = blockIdx.x;
-    const long long chunk = (N + gridDim.y - 1) / gridDim.y;
-    const long long c0 = blockIdx.y * chunk, c1 = min(N, c0 + chunk);
-    const float* v = V + i * PS;
-    double a = 0.;
-    for (long long c = c0 + threadIdx.x; c < c1; c += LB) a += (double)w[c] * v[c];
-    __shared__ double sm[LB / 32];
-    for (int off = 16; off > 0; off >>= 1) a += __shfl_xor_sync(0xffffffffu, a, off);
-    if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = a;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double t = 0.;
-        for (int u = 0; u < LB / 32; ++u) t += sm[u];
-        part[(size_t)i * gridDim.y + blockIdx.y] = t;
-    }
-}
 // h[0..j] from the partials (block q sums entry q)
 __global__ void fg_dots_finish(const double* part, int nchunk, double* h, const Scal* S) {
     if (S->done) return;
@@ -962,6 +943,64 @@ __global__ void fg_dots_finish(const double* part, int nchunk, double* h, const 
     }
     if (threadIdx.x == 0) h[i] = sm[0];
 }
+// Dot products of w with v_0 .. v_j in one sweep that reads w and every v_i once: each thread
+// accumulates its cells' products per i in shared memory (FP32), then each block reduces them
+// (FP64) into part[i * gridDim.x + block], the layout fg_dots_finish reads.
+__global__ void __launch_bounds__(LB) fg_multidot_kernel(long long N, const float* w, const float* V, long long PS, int j, double* part,
+                                                         const Scal* S) {
+    if (S->done) return;
+    extern __shared__ float fg_sm[];
+    float* acc = fg_sm;   // [j + 1][LB]
+    const int t = threadIdx.x;
+    for (int i = 0; i <= j; ++i) acc[i * LB + t] = 0.f;
+    for (long long c = blockIdx.x * (long long)LB + t; c < N; c += (long long)gridDim.x * LB) {
+        const float wv = w[c];
+        for (int i = 0; i <= j; ++i) acc[i * LB + t] += wv * V[i * PS + c];
+    }
+    __syncthreads();
+    const int warp = t >> 5, lane = t & 31;
+    for (int i = warp; i <= j; i += LB / 32) {
+        double sacc = 0.;
+        for (int u = lane; u < LB; u += 32) sacc += (double)acc[i * LB + u];
+        for (int off = 16; off > 0; off >>= 1) sacc += __shfl_xor_sync(0xffffffffu, sacc, off);
+        if (lane == 0) part[(size_t)i * gridDim.x + blockIdx.x] = sacc;
+    }
+}
+
+// First Gram-Schmidt update fused with the second pass's dot products: w <- w - sum_i h1[i] v_i and
+// the dots (w, v_i) of the updated w, reading every v_i once (each thread keeps its cell's v_i in
+// shared memory between the update and the dots).  Partials as fg_multidot_kernel's.
+__global__ void __launch_bounds__(LB) fg_orth_dots_kernel(long long N, float* w, const float* V, long long PS, int j, const double* h1,
+                                                          double* part, const Scal* S) {
+    if (S->done) return;
+    extern __shared__ float fg_sm[];
+    float* acc = fg_sm;                  // [j + 1][LB]
+    float* vs = fg_sm + (j + 1) * LB;    // [j + 1][LB]
+    __shared__ float h[FGM + 1];
+    const int t = threadIdx.x;
+    for (int i = t; i <= j; i += blockDim.x) h[i] = (float)h1[i];
+    for (int i = 0; i <= j; ++i) acc[i * LB + t] = 0.f;
+    __syncthreads();
+    for (long long c = blockIdx.x * (long long)LB + t; c < N; c += (long long)gridDim.x * LB) {
+        float x = w[c];
+        for (int i = 0; i <= j; ++i) {
+            const float v = V[i * PS + c];
+            vs[i * LB + t] = v;
+            x -= h[i] * v;
+        }
+        w[c] = x;
+        for (int i = 0; i <= j; ++i) acc[i * LB + t] += x * vs[i * LB + t];
+    }
+    __syncthreads();
+    const int warp = t >> 5, lane = t & 31;
+    for (int i = warp; i <= j; i += LB / 32) {
+        double sacc = 0.;
+        for (int u = lane; u < LB; u += 32) sacc += (double)acc[i * LB + u];
+        for (int off = 16; off > 0; off >>= 1) sacc += __shfl_xor_sync(0xffffffffu, sacc, off);
+        if (lane == 0) part[(size_t)i * gridDim.x + blockIdx.x] = sacc;
+    }
+}
+
 // w -= sum_i h[i] v_i; partial ||w||^2
 __global__ void __launch_bounds__(LB) fg_orth_kernel(long long N, float* w, const float* V, long long PS, int j, const double* hc, double* part,
                                                      const Scal* S) {
@@ -1163,6 +1202,13 @@ int fg_alloc(LearnedWork& lw, int m) {
     lw.fgPart = static_cast<double*>(lw.alloc(sizeof(double) * (size_t)(FGM + 1) * FG_DOT_BLOCKS, lw.allocCtx));
     if (!lw.fgV || !lw.fgZ || !lw.fgScal || !lw.fgPart) { set_error("FGMRES workspace allocation failed"); return 1; }
     lw.fgCap = m;
+    // the fused Gram-Schmidt kernels keep (m + 1) x LB floats (twice, for the update + dots one)
+    const int smMax = (int)(2 * sizeof(float) * (size_t)(FGM + 1) * LB);
+    if (cudaFuncSetAttribute(fg_multidot_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smMax) != cudaSuccess ||
+        cudaFuncSetAttribute(fg_orth_dots_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smMax) != cudaSuccess) {
+        set_error("FGMRES kernels: shared-memory attribute refused");
+        return 1;
+    }
     return 0;
 }
 }  // namespace
@@ -1256,12 +1302,16 @@ int learned_solve(LearnedWork& lw, const OpSym& A, const uint8_t* status, const 
                     if (v4) fg_spmv_kernel<true><<<nb, LB, 0, st>>>(Af, N, zj, lw.t, S);
                     else fg_spmv_kernel<false><<<nb, LB, 0, st>>>(Af, N, zj, lw.t, S);
                     // classical Gram-Schmidt with one re-orthogonalisation (CGS2): FP32 vectors lose
-                    // orthogonality in a single pass once the preconditioner is strong
-                    for (int pass = 0; pass < 2; ++pass) {
-                        double* hc = pass == 0 ? F->h1 : F->h2;
-                        fg_dots_kernel<<<dim3(j + 1, FG_DOT_BLOCKS), LB, 0, st>>>(N, lw.t, lw.fgV + L.H, PS, lw.fgPart, S);
-                        fg_dots_finish<<<j + 1, LB, 0, st>>>(lw.fgPart, FG_DOT_BLOCKS, hc, S);
-                        fg_orth_kernel<<<nb, LB, 0, st>>>(N, lw.t, lw.fgV + L.H, PS, j, hc, lw.part, S);
+                    // orthogonality in a single pass once the preconditioner is strong.  Three sweeps over
+                    // the basis: the first pass's dots, its update fused with the second pass's dots, and
+                    // the second pass's update (with ||w||^2).
+                    {
+                        const size_t sm1 = sizeof(float) * (size_t)(j + 1) * LB;
+                        fg_multidot_kernel<<<FG_DOT_BLOCKS, LB, sm1, st>>>(N, lw.t, lw.fgV + L.H, PS, j, lw.fgPart, S);
+                        fg_dots_finish<<<j + 1, LB, 0, st>>>(lw.fgPart, FG_DOT_BLOCKS, F->h1, S);
+                        fg_orth_dots_kernel<<<FG_DOT_BLOCKS, LB, 2 * sm1, st>>>(N, lw.t, lw.fgV + L.H, PS, j, F->h1, lw.fgPart, S);
+                        fg_dots_finish<<<j + 1, LB, 0, st>>>(lw.fgPart, FG_DOT_BLOCKS, F->h2, S);
+                        fg_orth_kernel<<<nb, LB, 0, st>>>(N, lw.t, lw.fgV + L.H, PS, j, F->h2, lw.part, S);
                     }
                     fg_step_finish<<<1, LB, 0, st>>>(lw.part, nb, j, m, maxit, F, S);
                     fg_scale_kernel<<<G, 256, 0, st>>>(N, lw.t, lw.fgV + (j + 1) * PS + L.H, S);
