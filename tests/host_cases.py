@@ -12,7 +12,8 @@ def _vec(v):
     return "(" + ",".join(repr(float(x)) for x in v) + ")"
 
 
-def write_case(root: str, spec: C.CaseSpec, lengths, nodes_ijk, steps: int, write_interval: int = 1000, extra: str = "") -> None:
+def write_case(root: str, spec: C.CaseSpec, lengths, nodes_ijk, steps: int, write_interval: int = 1000, extra: str = "",
+               run_control_extra: str = "", initial_conditions: str | None = None) -> None:
     os.makedirs(os.path.join(root, "mesh"), exist_ok=True)
     os.makedirs(os.path.join(root, "case"), exist_ok=True)
     lx, ly, lz = lengths
@@ -25,7 +26,7 @@ def write_case(root: str, spec: C.CaseSpec, lengths, nodes_ijk, steps: int, writ
     with open(os.path.join(root, "case", "case.info"), "w") as f:
         f.write("; generated case\n\nRunControl\n{\n\tterminationCondition iterations\n"
                 f"\tmaxNumberOfIterations {steps + 1}\n\tfileWriteInterval {write_interval}\n\ttimeStep {spec.dt!r}\n"
-                "\tmaxSimTime 48\n\tmaxRealTimeHours 48\n}\n\n")
+                "\tmaxSimTime 48\n\tmaxRealTimeHours 48\n" + run_control_extra + "}\n\n")
         f.write("Solver\n{\n\ttimeAccurate " + ("ON" if spec.time_accurate else "OFF") + "\n"
                 f"\trelaxationFactorMomentum {spec.omega_u!r}\n\trelaxationFactorPCorr {spec.omega_p!r}\n"
                 f"\trho {spec.rho!r}\n\tmu {spec.mu!r}\n\tnumberOfPressureCorrections {spec.n_pcorr}\n"
@@ -42,22 +43,31 @@ def write_case(root: str, spec: C.CaseSpec, lengths, nodes_ijk, steps: int, writ
             f.write(f"\t{face}\n\t{{\n\t\ttype {typ}\n\t\trefVector {_vec(rv)}\n\t\trefValue {float(rval)!r}\n\t}}\n")
         f.write("}\n" + extra)
     with open(os.path.join(root, "case", "initialConditions.info"), "w") as f:
-        f.write(f"u\n{{\n\ttype uniform\n\tvalue {_vec(spec.u_init)}\n}}\n\np\n{{\n\ttype uniform\n\tvalue {float(spec.p_init)!r}\n}}\n")
+        if initial_conditions is not None:
+            f.write(initial_conditions)
+        else:
+            f.write(f"u\n{{\n\ttype uniform\n\tvalue {_vec(spec.u_init)}\n}}\n\np\n{{\n\ttype uniform\n\tvalue {float(spec.p_init)!r}\n}}\n")
+
+
+def read_tec360_fields(path: str, n_cells: int) -> dict:
+    """Cell fields of the last zone of a solution file written by HexaFvmMesh::writeTec360, by the
+    names of its VARIABLES line ("p", "massFlow", "u_x", ...)."""
+    import re
+    with open(path) as f:
+        text = f.read()
+    names = re.findall(r'"([^"]+)"', text.split("\n", 2)[1])
+    last = text.split("ZONE")[-1]
+    header, body = last.split("\n", 1)
+    vals = [float(x) for x in body.split()]
+    ni, nj, nk = (int(re.search(rf"{a} = (\d+)", header).group(1)) for a in "IJK")
+    off = 3 * ni * nj * nk
+    out = {}
+    for q, nm in enumerate(names[3:]):
+        out[nm] = vals[off + q * n_cells:off + (q + 1) * n_cells]
+    return out
 
 
 def read_tec360_last_zone(path: str, n_cells: int):
     """(p, u planes) of the last zone of a solution file written by HexaFvmMesh::writeTec360."""
-    with open(path) as f:
-        text = f.read()
-    zones = text.split("ZONE")
-    last = zones[-1]
-    body = last.split("\n", 1)[1]
-    vals = [float(x) for x in body.split()]
-    header = last.split("\n", 1)[0]
-    import re
-    ni, nj, nk = (int(re.search(rf"{a} = (\d+)", header).group(1)) for a in "IJK")
-    nn = ni * nj * nk
-    off = 3 * nn
-    p = vals[off:off + n_cells]
-    u = vals[off + n_cells:off + 4 * n_cells]
-    return p, u
+    f = read_tec360_fields(path, n_cells)
+    return f["p"], f["u_x"] + f["u_y"] + f["u_z"]

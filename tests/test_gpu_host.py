@@ -12,7 +12,7 @@ from caffe_old_b200 import build as B, cases as C
 from oracle.oracle import OracleSolver
 
 from helpers import KSP_RTOL, KSP_RTOL_IB, demean, rel_l2
-from host_cases import read_tec360_last_zone, write_case
+from host_cases import read_tec360_fields, read_tec360_last_zone, write_case
 
 pytestmark = pytest.mark.gpu
 BIN = os.path.join(os.path.dirname(B.__file__), "_build", "bin")
@@ -60,3 +60,47 @@ def test_module_run_matches_oracle(tmp_path, module, kind):
     ep = rel_l2(demean(p, vol, mask), demean(o.get("p"), vol, mask))
     print(module, "u", eu, "p", ep)
     assert eu < FIELD_RTOL and ep < FIELD_RTOL
+    mf = np.array(read_tec360_fields(str(tmp_path / "solution" / "testMesh.dat"), len(p))["massFlow"])
+    assert rel_l2(mf, o.get("massFlow")) < FIELD_RTOL or np.linalg.norm(mf - o.get("massFlow")) < 1e-14
+
+
+def test_piso_module_continued_from_restart_files(tmp_path):
+    """caffePiso writes uRestart.rst / pRestart.rst (RunControl.writeRestart ON) after 3 steps; a
+    second run of the module starts from them (initial conditions of type restart, the reader the
+    reference declares in InitialConditions.h:69) and takes 2 more steps.  The oracle does the same:
+    3 steps, then a fresh solver given those cell values, 2 steps.  The restart files hold the
+    first run's fields exactly (17 digits), and the continued run matches the oracle at 1e-10."""
+    from caffe_old_b200 import restart as RS
+    spec = C.config2_cavity3d(n=10)[1].replace(mom_rtol=KSP_RTOL, p_rtol=KSP_RTOL)
+    lengths, res = (1.0, 1.0, 1.0), (11, 9, 8)
+    first, second = tmp_path / "first", tmp_path / "second"
+    first.mkdir()
+    second.mkdir()
+    write_case(str(first), spec, lengths, res, steps=3, run_control_extra="\twriteRestart ON\n")
+    subprocess.run([os.path.join(BIN, "hexaMesh")], cwd=first, check=True, capture_output=True)
+    r = subprocess.run([os.path.join(BIN, "caffePiso")], cwd=first, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    nodes = _nodes_from_dat(first / "mesh" / "structuredMesh.dat")
+    nI, nJ, nK = (int(d) - 1 for d in nodes.shape[2::-1])
+    n = nI * nJ * nK
+    o = OracleSolver(nodes, spec)
+    for _ in range(3):
+        o.solve(spec.dt)
+    u_rst = RS.read_restart(str(first / "uRestart.rst"), (nI, nJ, nK), 3)     # N x 3
+    p_rst = RS.read_restart(str(first / "pRestart.rst"), (nI, nJ, nK))
+    assert np.array_equal(u_rst.ravel(), o.get("u").ravel()) or rel_l2(u_rst.ravel(), o.get("u")) < FIELD_RTOL
+    ics = (f"u\n{{\n\ttype restart\n\tfile {first / 'uRestart.rst'}\n}}\n\n"
+           f"p\n{{\n\ttype restart\n\tfile {first / 'pRestart.rst'}\n}}\n")
+    write_case(str(second), spec, lengths, res, steps=2, initial_conditions=ics)
+    subprocess.run([os.path.join(BIN, "hexaMesh")], cwd=second, check=True, capture_output=True)
+    r = subprocess.run([os.path.join(BIN, "caffePiso")], cwd=second, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    p2, u2 = read_tec360_last_zone(str(second / "solution" / "testMesh.dat"), n)
+    o2 = OracleSolver(nodes, spec)
+    o2.set("u", u_rst.ravel())
+    o2.set("p", p_rst)
+    for _ in range(2):
+        o2.solve(spec.dt)
+    vol = o2.get("vol")
+    assert rel_l2(np.array(u2).reshape(3, -1).T.ravel(), o2.get("u")) < FIELD_RTOL
+    assert rel_l2(demean(np.array(p2), vol), demean(o2.get("p"), vol)) < FIELD_RTOL
