@@ -67,6 +67,7 @@ EXPORTS = (
     "caffe_last_error", "caffe_dev_create", "caffe_dev_destroy", "caffe_dev_solve", "caffe_dev_phase",
     "caffe_dev_array", "caffe_dev_stats", "caffe_dev_stream", "caffe_dev_synchronize",
     "caffe_ksp7_solve", "caffe_ksp7_solve_device", "caffe_ksp7_solve_device_noalloc", "caffe_csr_solve", "caffe_csr_matvec",
+    "caffe_diffusion_create", "caffe_diffusion_destroy", "caffe_diffusion_solve", "caffe_diffusion_phase", "caffe_diffusion_array",
     "caffe_precond_param_count", "caffe_precond_net_apply", "caffe_precond_net_grad",
     "caffe_dev_set_precond", "caffe_dev_get_precond", "caffe_dev_set_precond_mode", "caffe_dev_set_precond_options",
     "caffe_dev_record_pairs", "caffe_dev_pair_count", "caffe_dev_add_pairs", "caffe_dev_add_random_pairs", "caffe_dev_copy_pairs", "caffe_dev_train_precond",
@@ -100,6 +101,12 @@ def lib():
                                                   ctypes.POINTER(cd)]
     L.caffe_csr_solve.argtypes = [ci, vp, vp, vp, vp, vp, ci, cd, cd, ci, ctypes.POINTER(ci), ctypes.POINTER(cd)]
     L.caffe_csr_matvec.argtypes = [ci, ci, vp, vp, vp, vp, vp]
+    L.caffe_diffusion_create.argtypes = [vp, ci, ci, ci, vp, vp, ci, cd, ci, cd, ci, ci, ctypes.POINTER(vp)]
+    L.caffe_diffusion_destroy.argtypes = [vp]
+    L.caffe_diffusion_solve.argtypes = [vp, cd, ctypes.POINTER(cd), ctypes.POINTER(ci), ctypes.POINTER(cd)]
+    L.caffe_diffusion_phase.argtypes = [vp, ctypes.c_char_p, cd]
+    L.caffe_diffusion_array.restype = ctypes.c_long
+    L.caffe_diffusion_array.argtypes = [vp, ctypes.c_char_p, vp, ctypes.c_long, ci]
     L.caffe_precond_param_count.restype = ci
     L.caffe_precond_net_apply.argtypes = [ci, ci, ci, vp, vp, vp]
     L.caffe_precond_net_grad.argtypes = [ci, ci, ci, vp, vp, vp, vp, vp]

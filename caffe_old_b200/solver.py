@@ -158,3 +158,76 @@ class IbPiso(DeviceSolver):
 
 def make_solver(nodes: np.ndarray, spec: C.CaseSpec, device: int = 0) -> DeviceSolver:
     return {"simple": Simple, "piso": Piso, "ibpiso": IbPiso}[spec.kind](nodes, spec, device)
+
+
+DIFFUSION_BC = {"fixed": 0, "zeroGradient": 1, "empty": 2}
+
+
+class Diffusion:
+    """The reference's Diffusion solver (src/Solvers/Diffusion.cpp) on the device: unit
+    diffusivity, boundary types fixed / zeroGradient / empty per face (east, west, north, south,
+    top, bottom) with their reference values, a uniform initial phi.  ``solve(dt)`` assembles and
+    solves one linear system and returns ||A x - b||_inf, as Diffusion::solve does."""
+
+    def __init__(self, nodes: np.ndarray, bc_types, bc_values, time_accurate: bool = False, phi0: float = 0.0,
+                 method: str = "bicgstab_jacobi", rtol: float = 1e-8, maxit: int = 10000, device: int = 0):
+        from . import _lib
+        L = _lib.lib()
+        nodes = np.ascontiguousarray(nodes, dtype=np.float64)
+        nK1, nJ1, nI1, _ = nodes.shape
+        self.shape = (nI1 - 1, nJ1 - 1, nK1 - 1)
+        self.ncells = int(np.prod(self.shape))
+        types = np.array([DIFFUSION_BC[t] for t in bc_types], dtype=np.int32)
+        refs = np.ascontiguousarray(bc_values, dtype=np.float64)
+        if types.size != 6 or refs.size != 6:
+            raise ValueError("six boundary types and values (east, west, north, south, top, bottom)")
+        h = ctypes.c_void_p()
+        rc = L.caffe_diffusion_create(nodes.ctypes.data_as(ctypes.c_void_p), nI1, nJ1, nK1, types.ctypes.data_as(ctypes.c_void_p),
+                                      refs.ctypes.data_as(ctypes.c_void_p), 1 if time_accurate else 0, float(phi0),
+                                      C.KSP_METHODS[method], float(rtol), int(maxit), int(device), ctypes.byref(h))
+        if rc != 0:
+            raise _lib.CaffeError("caffe_diffusion_create: " + _lib.last_error())
+        self._h = h.value
+        self.iters, self.rel_res = 0, 0.0
+
+    def close(self):
+        from . import _lib
+        if getattr(self, "_h", None):
+            _lib.lib().caffe_diffusion_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def solve(self, dt: float = 1.0) -> float:
+        from . import _lib
+        r, it, rr = ctypes.c_double(0.0), ctypes.c_int(0), ctypes.c_double(0.0)
+        if _lib.lib().caffe_diffusion_solve(self._h, float(dt), ctypes.byref(r), ctypes.byref(it), ctypes.byref(rr)) != 0:
+            raise _lib.CaffeError("caffe_diffusion_solve: " + _lib.last_error())
+        self.iters, self.rel_res = it.value, rr.value
+        return r.value
+
+    def phase(self, name: str, dt: float = 1.0) -> None:
+        from . import _lib
+        if _lib.lib().caffe_diffusion_phase(self._h, name.encode(), float(dt)) != 0:
+            raise _lib.CaffeError(f"caffe_diffusion_phase {name}: " + _lib.last_error())
+
+    def get(self, name: str) -> np.ndarray:
+        from . import _lib
+        L = _lib.lib()
+        n = L.caffe_diffusion_array(self._h, name.encode(), None, 0, 0)
+        if n < 0:
+            raise KeyError(name)
+        out = np.zeros(n, dtype=np.float64)
+        if L.caffe_diffusion_array(self._h, name.encode(), out.ctypes.data_as(ctypes.c_void_p), n, 0) < 0:
+            raise _lib.CaffeError(_lib.last_error())
+        return out
+
+    def set(self, name: str, values: np.ndarray) -> None:
+        from . import _lib
+        v = np.ascontiguousarray(values, dtype=np.float64).ravel()
+        if _lib.lib().caffe_diffusion_array(self._h, name.encode(), v.ctypes.data_as(ctypes.c_void_p), v.size, 1) < 0:
+            raise _lib.CaffeError(_lib.last_error())

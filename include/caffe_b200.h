@@ -156,6 +156,24 @@ int caffe_csr_solve(int n, const int* row_ptr, const int* col, const double* val
  * multiply(const SparseMatrix&, const SparseVector&, SparseVector&) (src/Math/SparseMatrix.cpp:132-135). */
 int caffe_csr_matvec(int m, int n, const int* row_ptr, const int* col, const double* val, const double* x, double* y);
 
+/* Scalar diffusion with unit diffusivity on one block: the reference's Diffusion solver
+ * (src/Solvers/Diffusion.cpp:35-131), its coefficients as written there (a_nb = +D_f,
+ * a_P = -sum D_f + V/dt, b = (V/dt) phi0).  bc_type per face (east, west, north, south, top,
+ * bottom): 0 fixed, 1 zeroGradient, 2 empty (PrimitiveBoundaryCondition::Type), ref_val the
+ * faces' reference values; phi starts at phi0.  caffe_diffusion_solve is Diffusion::solve: assemble,
+ * Krylov solve (method / rtol / maxit as for caffe_ksp7_solve), phi and its faces and gradient,
+ * and ||A x - b||_inf (its return value in the reference).  caffe_diffusion_phase runs one part:
+ * "assemble", "solve" (the linear solve into x) or "post" (everything after it).
+ * caffe_diffusion_array: "phi", "x" (writable), "b", "A" (N x 7: aP aE aW aN aS aT aB), "phiFaceI/J/K",
+ * "phiPatch0".."phiPatch5", "gradPhi" (N x 3); same conventions as caffe_dev_array. */
+typedef struct caffe_diffusion caffe_diffusion;
+int caffe_diffusion_create(const double* nodes, int nNodesI, int nNodesJ, int nNodesK, const int* bc_type, const double* ref_val,
+                           int time_accurate, double phi0, int method, double rtol, int maxit, int device, caffe_diffusion** out);
+int caffe_diffusion_destroy(caffe_diffusion* h);
+int caffe_diffusion_solve(caffe_diffusion* h, double dt, double* residual_inf, int* iters, double* rel_res);
+int caffe_diffusion_phase(caffe_diffusion* h, const char* name, double dt);
+long caffe_diffusion_array(caffe_diffusion* h, const char* name, double* host, long count, int dir);
+
 /* Learned preconditioner network (an extension; the reference has no learned component):
  * a 4-layer 3-D convolutional network with 3x3x3 kernels and 16 channels, BF16 weights and
  * activations, FP32 accumulation on the tensor cores.  Parameters are FP32, layer by layer:
