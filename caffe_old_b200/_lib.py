@@ -68,6 +68,8 @@ EXPORTS = (
     "caffe_dev_array", "caffe_dev_stats", "caffe_dev_stream", "caffe_dev_synchronize",
     "caffe_ksp7_solve", "caffe_ksp7_solve_device", "caffe_ksp7_solve_device_noalloc", "caffe_csr_solve", "caffe_csr_matvec",
     "caffe_diffusion_create", "caffe_diffusion_destroy", "caffe_diffusion_solve", "caffe_diffusion_phase", "caffe_diffusion_array",
+    "caffe_coupled_create", "caffe_coupled_destroy", "caffe_coupled_solve", "caffe_coupled_phase", "caffe_coupled_stats",
+    "caffe_coupled_system", "caffe_coupled_array",
     "caffe_precond_param_count", "caffe_precond_net_apply", "caffe_precond_net_grad",
     "caffe_dev_set_precond", "caffe_dev_get_precond", "caffe_dev_set_precond_mode", "caffe_dev_set_precond_options",
     "caffe_dev_record_pairs", "caffe_dev_pair_count", "caffe_dev_add_pairs", "caffe_dev_add_random_pairs", "caffe_dev_copy_pairs", "caffe_dev_train_precond",
@@ -107,6 +109,15 @@ def lib():
     L.caffe_diffusion_phase.argtypes = [vp, ctypes.c_char_p, cd]
     L.caffe_diffusion_array.restype = ctypes.c_long
     L.caffe_diffusion_array.argtypes = [vp, ctypes.c_char_p, vp, ctypes.c_long, ci]
+    L.caffe_coupled_create.argtypes = [vp, ci, ci, ci, ctypes.POINTER(CaffeCase), ci, ctypes.POINTER(vp)]
+    L.caffe_coupled_destroy.argtypes = [vp]
+    L.caffe_coupled_solve.argtypes = [vp, cd, ctypes.POINTER(cd)]
+    L.caffe_coupled_phase.argtypes = [vp, ctypes.c_char_p, cd]
+    L.caffe_coupled_stats.argtypes = [vp, ctypes.POINTER(ci), ctypes.POINTER(cd), ctypes.POINTER(ci)]
+    L.caffe_coupled_system.restype = ctypes.c_longlong
+    L.caffe_coupled_system.argtypes = [vp, vp, vp, vp]
+    L.caffe_coupled_array.restype = ctypes.c_long
+    L.caffe_coupled_array.argtypes = [vp, ctypes.c_char_p, vp, ctypes.c_long, ci]
     L.caffe_precond_param_count.restype = ci
     L.caffe_precond_net_apply.argtypes = [ci, ci, ci, vp, vp, vp]
     L.caffe_precond_net_grad.argtypes = [ci, ci, ci, vp, vp, vp, vp, vp]

@@ -231,3 +231,86 @@ class Diffusion:
         v = np.ascontiguousarray(values, dtype=np.float64).ravel()
         if _lib.lib().caffe_diffusion_array(self._h, name.encode(), v.ctypes.data_as(ctypes.c_void_p), v.size, 1) < 0:
             raise _lib.CaffeError(_lib.last_error())
+
+
+class Coupled:
+    """The reference's Coupled solver (src/Solvers/Coupled.cpp) on the device: momentum and
+    continuity assembled into one block system of 4 N unknowns (u_x, u_y, u_z, p) and solved
+    together, then the Rhie-Chow face fluxes.  The case is a CaseSpec (boundary conditions, rho,
+    mu, omega_u, time_accurate / n_inner, mom_method / mom_rtol / mom_atol / maxit).
+    ``solve(dt)`` is Coupled::solve and returns the continuity error."""
+
+    def __init__(self, nodes: np.ndarray, spec: C.CaseSpec, device: int = 0):
+        from . import _lib
+        L = _lib.lib()
+        nodes = np.ascontiguousarray(nodes, dtype=np.float64)
+        nK1, nJ1, nI1, _ = nodes.shape
+        self.shape = (nI1 - 1, nJ1 - 1, nK1 - 1)
+        self.ncells = int(np.prod(self.shape))
+        self.spec = spec
+        self._case = _lib.make_case(spec)
+        h = ctypes.c_void_p()
+        if L.caffe_coupled_create(nodes.ctypes.data_as(ctypes.c_void_p), nI1, nJ1, nK1, ctypes.byref(self._case), int(device),
+                                  ctypes.byref(h)) != 0:
+            raise _lib.CaffeError("caffe_coupled_create: " + _lib.last_error())
+        self._h = h.value
+
+    def close(self):
+        from . import _lib
+        if getattr(self, "_h", None):
+            _lib.lib().caffe_coupled_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def solve(self, dt: float | None = None) -> float:
+        from . import _lib
+        r = ctypes.c_double(0.0)
+        if _lib.lib().caffe_coupled_solve(self._h, float(self.spec.dt if dt is None else dt), ctypes.byref(r)) != 0:
+            raise _lib.CaffeError("caffe_coupled_solve: " + _lib.last_error())
+        return r.value
+
+    def phase(self, name: str, dt: float | None = None) -> None:
+        from . import _lib
+        if _lib.lib().caffe_coupled_phase(self._h, name.encode(), float(self.spec.dt if dt is None else dt)) != 0:
+            raise _lib.CaffeError(f"caffe_coupled_phase {name}: " + _lib.last_error())
+
+    def stats(self) -> dict:
+        from . import _lib
+        it, rr, st = ctypes.c_int(0), ctypes.c_double(0.0), ctypes.c_int(0)
+        _lib.lib().caffe_coupled_stats(self._h, ctypes.byref(it), ctypes.byref(rr), ctypes.byref(st))
+        return {"iters": it.value, "rel_res": rr.value, "status": st.value}
+
+    def system(self):
+        """The block matrix in compressed rows: (row_ptr, col, val)."""
+        from . import _lib
+        L = _lib.lib()
+        nnz = L.caffe_coupled_system(self._h, None, None, None)
+        ptr = np.zeros(4 * self.ncells + 1, dtype=np.int32)
+        col = np.zeros(nnz, dtype=np.int32)
+        val = np.zeros(nnz, dtype=np.float64)
+        if L.caffe_coupled_system(self._h, ptr.ctypes.data_as(ctypes.c_void_p), col.ctypes.data_as(ctypes.c_void_p),
+                                  val.ctypes.data_as(ctypes.c_void_p)) < 0:
+            raise _lib.CaffeError(_lib.last_error())
+        return ptr, col, val
+
+    def get(self, name: str) -> np.ndarray:
+        from . import _lib
+        L = _lib.lib()
+        n = L.caffe_coupled_array(self._h, name.encode(), None, 0, 0)
+        if n < 0:
+            raise KeyError(name)
+        out = np.zeros(n, dtype=np.float64)
+        if L.caffe_coupled_array(self._h, name.encode(), out.ctypes.data_as(ctypes.c_void_p), n, 0) < 0:
+            raise _lib.CaffeError(_lib.last_error())
+        return out
+
+    def set(self, name: str, values: np.ndarray) -> None:
+        from . import _lib
+        v = np.ascontiguousarray(values, dtype=np.float64).ravel()
+        if _lib.lib().caffe_coupled_array(self._h, name.encode(), v.ctypes.data_as(ctypes.c_void_p), v.size, 1) < 0:
+            raise _lib.CaffeError(_lib.last_error())

@@ -174,6 +174,31 @@ int caffe_diffusion_solve(caffe_diffusion* h, double dt, double* residual_inf, i
 int caffe_diffusion_phase(caffe_diffusion* h, const char* name, double dt);
 long caffe_diffusion_array(caffe_diffusion* h, const char* name, double* host, long count, int dir);
 
+/* Momentum and continuity solved as one block system: the reference's Coupled solver
+ * (src/Solvers/Coupled.cpp:5-339).  Unknowns u_x, u_y, u_z, p, each numbered like the cells
+ * (4 N rows); momentum rows hold 14 entries, continuity rows 28.  The case fields used are
+ * bc_type, ref_vec, ref_val, rho, mu, omega_u, time_accurate, n_inner, mom_method, mom_rtol,
+ * mom_atol and maxit; u and p start at zero, as in the reference.  caffe_coupled_solve is
+ * Coupled::solve (u0 = u, n_inner iterations of assembly, block solve and Rhie-Chow fluxes when
+ * time-accurate, one otherwise) and returns the continuity error max |net face flux| / V.
+ * caffe_coupled_phase runs one part: "save_u0", "assemble" ("assemble_momentum" then
+ * "assemble_continuity"), "solve" (the block solve into x), "post" (u, p, grad p, h, face fluxes)
+ * or "continuity".  caffe_coupled_stats gives the last block solve's iterations, true relative
+ * residual and status (0 converged, 1 maxit, 2 breakdown, 3 non-finite).
+ * caffe_coupled_system copies the block matrix out in compressed rows (row_ptr 4N + 1, col and
+ * val nnz; any may be NULL) and returns nnz; the entries of each row are in the reference's
+ * insertion order.  caffe_coupled_array: "u", "u0", "gradP", "h" (N x 3), "p", "d" (N),
+ * "massFlowI/J/K" (faces), "b", "x" (4N); u, u0, p, gradP, massFlow* and x are writable. */
+typedef struct caffe_coupled caffe_coupled;
+int caffe_coupled_create(const double* nodes, int nNodesI, int nNodesJ, int nNodesK, const caffe_case* cs, int device,
+                         caffe_coupled** out);
+int caffe_coupled_destroy(caffe_coupled* h);
+int caffe_coupled_solve(caffe_coupled* h, double dt, double* continuity);
+int caffe_coupled_phase(caffe_coupled* h, const char* name, double dt);
+int caffe_coupled_stats(caffe_coupled* h, int* iters, double* rel_res, int* status);
+long long caffe_coupled_system(caffe_coupled* h, int* row_ptr, int* col, double* val);
+long caffe_coupled_array(caffe_coupled* h, const char* name, double* host, long count, int dir);
+
 /* Learned preconditioner network (an extension; the reference has no learned component):
  * a 4-layer 3-D convolutional network with 3x3x3 kernels and 16 channels, BF16 weights and
  * activations, FP32 accumulation on the tensor cores.  Parameters are FP32, layer by layer:

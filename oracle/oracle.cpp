@@ -1394,8 +1394,16 @@ struct Coupled {
         return computeContinuityError();
     }
 
-    // Coupled::computeMomentumAndPressure (Coupled.cpp:54-280)
+    // Coupled::computeMomentumAndPressure (Coupled.cpp:54-280), in three parts: the assembly of
+    // the block system, its solve and what follows the solve
     void computeMomentumAndPressure(double dt) {
+        assemble(dt);
+        solveSystem();
+        post();
+    }
+
+    // Coupled.cpp:54-245: momentum rows, d and its faces, continuity rows
+    void assemble(double dt) {
         uStar.c = u.c;
         const int dI[7] = {0, 1, -1, 0, 0, 0, 0}, dJ[7] = {0, 0, 0, 1, -1, 0, 0}, dK[7] = {0, 0, 0, 0, 0, 1, -1};
         // momentum rows
@@ -1475,7 +1483,13 @@ struct Coupled {
                     A.setRow(rowNo, 7, cols, a);
                     b[rowNo] = bp;
                 }
-        st = kspSolve(cs.mom_method, A, b, x, cs.mom_rtol, cs.maxit);
+    }
+
+    // Coupled.cpp:247-249
+    void solveSystem() { st = kspSolve(cs.mom_method, A, b, x, cs.mom_rtol, cs.maxit, cs.mom_atol); }
+
+    // Coupled.cpp:251-278
+    void post() {
         for (int c = 0; c < N; ++c) {
             u.c[c] = v3(x[c], x[c + N], x[c + 2 * (size_t)N]);
             p.c[c] = x[c + 3 * (size_t)N];
@@ -1818,7 +1832,37 @@ long oracle_coupled_array(void* hh, const char* name, double* buf, long count, i
     if (n == "massFlowJ") return vecd(s->mf.fJ);
     if (n == "massFlowK") return vecd(s->mf.fK);
     if (n == "b") return vecd(s->b);
+    if (n == "x") return vecd(s->x);
+    if (n == "h") return vecv(s->h.c);
+    if (n == "u0") return vecv(s->u0.c);
     return -1;
+}
+
+// One part of Coupled::computeMomentumAndPressure: "save_u0" (the start of Coupled::solve),
+// "assemble", "solve" or "post".
+int oracle_coupled_phase(void* hh, const char* name, double dt) {
+    auto* s = static_cast<orc::Coupled*>(hh);
+    try {
+        std::string n(name);
+        if (n == "save_u0") s->u0.c = s->u.c;
+        else if (n == "assemble") s->assemble(dt);
+        else if (n == "solve") s->solveSystem();
+        else if (n == "post") s->post();
+        else { g_err = "unknown phase " + n; return 2; }
+        return 0;
+    } catch (const std::exception& e) { g_err = e.what(); return 1; }
+}
+
+// The assembled block system as its rows were set (the layout of oracle_system); returns the
+// row count (4 N).
+int oracle_coupled_system(void* hh, int* width, int* cnt, int* col, double* val) {
+    auto* s = static_cast<orc::Coupled*>(hh);
+    const orc::Rows& A = s->A;
+    if (width) *width = A.width;
+    if (cnt) std::memcpy(cnt, A.cnt.data(), sizeof(int) * A.cnt.size());
+    if (col) std::memcpy(col, A.col.data(), sizeof(int) * A.col.size());
+    if (val) std::memcpy(val, A.val.data(), sizeof(double) * A.val.size());
+    return A.n;
 }
 
 // Diffusion solver.  types: per face E W N S T B, 0 fixed, 1 zeroGradient, 2 empty; refs:

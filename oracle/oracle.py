@@ -77,6 +77,8 @@ def lib():
         L.oracle_coupled_stats.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
         L.oracle_coupled_array.restype = ctypes.c_long
         L.oracle_coupled_array.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_void_p, ctypes.c_long, ctypes.c_int]
+        L.oracle_coupled_phase.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_double]
+        L.oracle_coupled_system.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
         L.oracle_diffusion_create.restype = ctypes.c_void_p
         L.oracle_diffusion_create.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
                                               ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_double,
@@ -262,6 +264,31 @@ class OracleCoupled:
         out = np.zeros(n, dtype=np.float64)
         L.oracle_coupled_array(self._h, name.encode(), _ptr(out), n, 0)
         return out
+
+    def set(self, name: str, values: np.ndarray) -> None:
+        v = np.ascontiguousarray(values, dtype=np.float64).ravel()
+        n = lib().oracle_coupled_array(self._h, name.encode(), None, 0, 0)
+        if n != v.size:
+            raise ValueError(f"{name}: expected {n} values, got {v.size}")
+        lib().oracle_coupled_array(self._h, name.encode(), _ptr(v), n, 1)
+
+    def phase(self, name: str, dt: float | None = None) -> None:
+        """One part of Coupled::computeMomentumAndPressure: save_u0, assemble, solve, post."""
+        if lib().oracle_coupled_phase(self._h, name.encode(), float(self.spec.dt if dt is None else dt)) != 0:
+            raise RuntimeError("oracle_coupled_phase: " + lib().oracle_last_error().decode())
+
+    def system(self):
+        """The assembled block system: per row its entries in insertion order, as
+        (counts, columns, values) with columns -1 past each row's count, and the width."""
+        L = lib()
+        n = L.oracle_coupled_system(self._h, None, None, None, None)
+        w = ctypes.c_int(0)
+        L.oracle_coupled_system(self._h, ctypes.byref(w), None, None, None)
+        cnt = np.zeros(n, dtype=np.int32)
+        col = np.zeros(n * w.value, dtype=np.int32)
+        val = np.zeros(n * w.value, dtype=np.float64)
+        L.oracle_coupled_system(self._h, None, _ptr(cnt), _ptr(col), _ptr(val))
+        return cnt, col.reshape(n, w.value), val.reshape(n, w.value)
 
 
 DIFFUSION_BC = {"fixed": 0, "zeroGradient": 1, "empty": 2}
