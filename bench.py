@@ -348,7 +348,8 @@ def run_b200(args, world, rank, local, pg):
     def record(tag):
         st = dev.last_stats
         per_step.append({"phase": tag, "p_ms": round(st["p_ms"], 2), "p_iters": st["p_iters_total"], "p_solves": st["p_solves"],
-                         "fallbacks": st["fallbacks"], "cascades": st["cascades"], "step_ms": round(st["step_ms"], 2),
+                         "fallbacks": st["fallbacks"], "cascades": st["cascades"], "net_iters": st["net_iters"],
+                         "step_ms": round(st["step_ms"], 2),
                          "p_res_max": st["p_res_max"]})
 
     for _ in range(args.warmup):
@@ -362,7 +363,7 @@ def run_b200(args, world, rank, local, pg):
     t0 = torch.cuda.Event(enable_timing=True)
     t1 = torch.cuda.Event(enable_timing=True)
     p_ms, p_iters, p_solves, mom_ms, mom_iters, status, fallbacks, res_max = 0.0, 0, 0, 0.0, 0, 0, 0, 0.0
-    cascades = 0
+    cascades = net_iters = 0
     conts = []
     l0 = _lib.lib().caffe_launch_count()
     t0.record(stream)
@@ -373,6 +374,7 @@ def run_b200(args, world, rank, local, pg):
         p_ms += st["p_ms"]; p_iters += st["p_iters_total"]; p_solves += st["p_solves"]
         mom_ms += st["mom_ms"]; mom_iters += sum(st["mom_iters"]); status = max(status, st["status"])
         fallbacks += st["fallbacks"]; res_max = max(res_max, st["p_res_max"]); cascades += st["cascades"]
+        net_iters += st["net_iters"]
     t1.record(stream)
     t1.synchronize()
     launches = _lib.lib().caffe_launch_count() - l0
@@ -482,6 +484,7 @@ def run_b200(args, world, rank, local, pg):
             "p_solve_ms": p_ms / args.steps, "momentum_solve_ms": mom_ms / args.steps,
             "p_iters_per_step": p_iters / args.steps, "mom_iters_per_step": mom_iters / args.steps,
             "p_res_max": res_max, "fallbacks": fallbacks, "cascades": cascades,
+            "net_iters_per_step": net_iters / args.steps,
             "continuity_last": conts[-1], "solver_status": status,
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
             "gpu_launches": launches, "compare": compare, "per_step": per_step,

@@ -52,7 +52,7 @@ class StepStats(ctypes.Structure):
         ("p_res_max", ctypes.c_double), ("mom_res_max", ctypes.c_double),
         ("status", ctypes.c_int), ("fallbacks", ctypes.c_int), ("n_ghost", ctypes.c_int), ("n_rows", ctypes.c_int),
         ("p_ms", ctypes.c_double), ("mom_ms", ctypes.c_double), ("step_ms", ctypes.c_double),
-        ("cascades", ctypes.c_int),
+        ("cascades", ctypes.c_int), ("net_iters", ctypes.c_int),
     ]
 
     def as_dict(self) -> dict:

@@ -33,6 +33,7 @@ struct StepAcc {
     int status;
     int fallbacks;
     int cascades;
+    int net_iters;
     double p_res_max;
     double mom_res_max;
     double continuity;
@@ -85,7 +86,7 @@ __global__ void acc_kernel(const KspOut* o, StepAcc* acc, int kind, int nr) {
             acc->mom_iters[q] = o->iters[q];
             if (rr > acc->mom_res_max) acc->mom_res_max = rr;
         } else {
-            if (kind == 2) acc->cascades += o->cascades;
+            if (kind == 2) { acc->cascades += o->cascades; acc->net_iters += o->net_iters; }
             acc->p_iters_last = o->iters[q];
             acc->p_iters_total += o->iters[q];
             acc->p_solves += 1;
@@ -533,6 +534,7 @@ int read_stats(caffe_dev* h, caffe_step_stats* s) {
     o.status = a.status;
     o.fallbacks = a.fallbacks;
     o.cascades = a.cascades;
+    o.net_iters = a.net_iters;
     o.n_ghost = h->ib ? h->ibs.nGhostHost : 0;
     o.n_rows = (int)(h->L.N - (h->ib ? h->ibs.nInactiveHost : 0));
     float ms = 0.f;

@@ -4,10 +4,11 @@
 // Data: activations are channel-last bf16, 16 channels (32 bytes) per cell, cell index
 // (k*nJ + j)*nI + i; zero padding outside the lattice.
 //
-// One CTA (128 threads, 4 warps) owns an 8 (i) x 16 (j) tile of output cells and marches
-// through KC consecutive k-planes, software-pipelined: four staged input planes rotate and two
-// TMEM accumulators alternate, so the MMAs of plane k+1 run while the CTA stores plane k and
-// stages plane k+2.  For each output plane the tile is one UMMA problem
+// One CTA owns an 8 (i) x 16 (j) tile of output cells and marches through KC consecutive
+// k-planes.  Its warps specialise: one thread streams the input planes in by TMA up to three
+// planes ahead through six staging slots, one thread issues the MMAs, and four warps drain the
+// four TMEM accumulators (epilogue), each handing over to the next through mbarriers, so loads,
+// MMAs and stores of different planes overlap.  For each output plane the tile is one UMMA problem
 // M = 128 cells, N = 16 output channels, accumulated over the 27 taps with one
 // tcgen05.mma.kind::f16 of K = 16 input channels per tap into a 128 x 16 FP32 accumulator
 // in tensor memory.  The input planes arrive by TMA (cp.async.bulk.tensor, one thread issuing,
@@ -22,8 +23,9 @@
 // tcgen05.ld (one TMEM lane per thread = one cell), applies bias / ReLU, or the ReLU mask
 // of the backward pass, and writes bf16 (or FP32 for the network output).
 //
-// Every wait on the MMA-completion mbarrier is bounded; a CTA that times out records an
-// error, waits once more (bounded) and frees its tensor memory before leaving.
+// Every mbarrier wait is bounded; a role whose wait runs out marks the CTA failed, the other roles
+// stop at their next wait, the MMAs and TMA loads already issued are waited for (bounded), the
+// CTA records an error and frees its tensor memory before leaving.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 #include <cuda_bf16.h>
@@ -47,10 +49,14 @@ constexpr int TI = 8, TJ = 16;          // tile: 8 cells along i, 16 along j -> 
 constexpr int ROWS = TJ + 2;            // staged j-rows (one halo row each side)
 constexpr int GROUP_BYTES = 256;        // one j-row of 8 cells x 16 channels, canonical layout
 constexpr int BUF_BYTES = ROWS * GROUP_BYTES;          // 4608
-constexpr int NPL = 4;                  // rotating staged planes (3 in use by the MMAs, 1 being filled)
-constexpr int NBUF = 3 * NPL;           // planes x 3 i-shifts
+constexpr int NPL = 6;                  // staged input-plane slots (each 3 i-shifted boxes)
+constexpr int NACC = 4;                 // TMEM accumulators (16 columns each)
 constexpr int W_BYTES = 27 * 512;       // 27 taps x 16 x 16 bf16
-constexpr uint32_t TMEM_COLS = 32;
+constexpr uint32_t TMEM_COLS = 16 * NACC;
+constexpr int EPI_THREADS = 128;        // warps 0-3: epilogue
+constexpr int PRODUCER_THREAD = 128;    // warp 4, lane 0: TMA loads
+constexpr int MMA_THREAD = 160;         // warp 5, lane 0: MMA issue
+constexpr int CONV_THREADS = 192;
 constexpr long long WAIT_LIMIT = 1ll << 20;   // try_wait rounds (each may block briefly): about a second at most
 
 // instruction descriptor: kind::f16, D = F32, A = B = BF16, both K-major, N = 16, M = 128
@@ -141,28 +147,40 @@ __device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
 
 // EPI: 0 bias + ReLU -> bf16; 1 bias -> FP32 channel 0 (network output); 2 backward data:
 // multiply by (mask_act > 0) -> bf16.  Weights: packed canonical blocks, 27 x 512 bytes.
+//
+// Warp roles (192 threads): warps 0-3 run the epilogue (thread = TMEM lane = output cell), warp 4
+// lane 0 issues the TMA loads, warp 5 lane 0 issues the MMAs.  They hand work over through
+// mbarriers only:
+//   full[s]   plane slot s has landed (TMA transaction count)
+//   empty[s]  the last MMAs reading slot s have completed (tcgen05.commit after output plane o,
+//             the last reader of input plane o)
+//   accf[a]   accumulator a holds a finished output plane (tcgen05.commit)
+//   acce[a]   the epilogue has read accumulator a (128 arrivals)
+// Input plane q (= k0 - 1 + q) lives in slot q mod NPL; output plane o (= k0 + o) reads input
+// planes o, o+1, o+2 and accumulates in TMEM columns 16 (o mod NACC).  The producer runs up to
+// NPL - 3 planes ahead of the MMAs and the MMAs up to NACC - 1 planes ahead of the epilogue.
 template <int EPI>
-__global__ void __launch_bounds__(128) conv3d_tc_kernel(Lat L, const __grid_constant__ CUtensorMap in_map,
-                                                        const __nv_bfloat16* __restrict__ wpack, const float* __restrict__ bias,
-                                                        __nv_bfloat16* out_bf, float* out_f, long long out_stride,
-                                                        const __nv_bfloat16* __restrict__ mask_act, int KC, int* err,
-                                                        const int* __restrict__ skip) {
+__global__ void __launch_bounds__(CONV_THREADS) conv3d_tc_kernel(Lat L, const __grid_constant__ CUtensorMap in_map,
+                                                                 const __nv_bfloat16* __restrict__ wpack, const float* __restrict__ bias,
+                                                                 __nv_bfloat16* out_bf, float* out_f, long long out_stride,
+                                                                 const __nv_bfloat16* __restrict__ mask_act, int KC, int* err,
+                                                                 const int* __restrict__ skip) {
     // a solve that has already converged turns its remaining launches into no-ops (uniform)
     if (skip && *skip) return;
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     // 1 KiB-align the dynamic region
     unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     unsigned char* wsm = smem;                                // W_BYTES
-    unsigned char* bufs = smem + W_BYTES;                     // NBUF x BUF_BYTES
-    __shared__ __align__(8) uint64_t mbar[2];
-    __shared__ __align__(8) uint64_t lbar[NPL];   // TMA completion, one per staging slot
+    unsigned char* bufs = smem + W_BYTES;                     // NPL x 3 x BUF_BYTES
+    __shared__ __align__(8) uint64_t full[NPL], empty[NPL], accf[NACC], acce[NACC];
     __shared__ uint32_t tmem_base_sh;
     __shared__ float bias_sh[16];
-    __shared__ int tma_fail_sh;
+    __shared__ volatile int fail_sh;
 
     const int i0 = blockIdx.x * TI, j0 = blockIdx.y * TJ;
     const int k0 = blockIdx.z * KC;
-    const int k1 = min(k0 + KC, L.nK);
+    const int nO = min(k0 + KC, L.nK) - k0;   // output planes of this CTA
+    const int nP = nO + 2;                    // input planes k0-1 .. k0+nO
     const int warp = threadIdx.x >> 5;
 
     // weights and bias to shared memory
@@ -170,144 +188,143 @@ __global__ void __launch_bounds__(128) conv3d_tc_kernel(Lat L, const __grid_cons
         reinterpret_cast<uint4*>(wsm)[u] = reinterpret_cast<const uint4*>(wpack)[u];
     if (threadIdx.x < 16) bias_sh[threadIdx.x] = bias ? bias[threadIdx.x] : 0.f;
     if (threadIdx.x == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[0])));
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[1])));
-        for (int q = 0; q < NPL; ++q) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&lbar[q])));
+        for (int q = 0; q < NPL; ++q) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&full[q])));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&empty[q])));
+        }
+        for (int q = 0; q < NACC; ++q) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&accf[q])));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&acce[q])), "r"(EPI_THREADS));
+        }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-        tma_fail_sh = 0;
+        fail_sh = 0;
     }
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base_sh)),
                      "r"(TMEM_COLS));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
-    // plane p lives in rotation slot (p - k0 + 1) mod 4; planes k0-1, k0, k0+1 first.  Thread 0
-    // issues every load and keeps, per slot, how many loads it has issued (the parity of the
-    // latest one is the phase to wait for).
-    auto slot_of = [&](int plane) { return (plane - k0 + 1) & (NPL - 1); };
-    int loads[NPL] = {0, 0, 0, 0};
-    auto load_plane = [&](int plane) {
-        if (threadIdx.x != 0) return;
-        const int slot = slot_of(plane);
-        const uint32_t lb = smem_u32(&lbar[slot]);
-        mbar_expect_tx(lb, 3 * BUF_BYTES);
-        for (int sh = 0; sh < 3; ++sh)
-            tma_load_box(smem_u32(bufs + (size_t)(slot * 3 + sh) * BUF_BYTES), &in_map, i0 + sh - 1, j0 - 1, plane, lb);
-        ++loads[slot];
-    };
-    auto wait_plane = [&](int plane) -> bool {   // thread 0 only
-        const int slot = slot_of(plane);
-        return loads[slot] == 0 || mbar_wait_bounded(smem_u32(&lbar[slot]), (uint32_t)((loads[slot] - 1) & 1));
-    };
-    load_plane(k0 - 1);
-    load_plane(k0);
-    load_plane(k0 + 1);
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;");
     const uint32_t tmem = tmem_base_sh;
-    const uint32_t bar[2] = {smem_u32(&mbar[0]), smem_u32(&mbar[1])};
-    uint32_t phase[2] = {0u, 0u};
-    bool failed = false;
-    int accFail = 0;
-    bool otherPending = false;
 
-    // the 27 MMAs of output plane k into accumulator acc (TMEM columns 16 acc .. 16 acc + 15),
-    // issued by one thread, completion signalled on bar[acc]
-    auto issue = [&](int k, int acc) {
-        if (threadIdx.x != 0) return;
-        // the three input planes must have landed; a load that never completes marks the CTA failed
-        // (its MMAs still run, on whatever the buffers hold, so that every wait below is satisfied)
-        if (!(wait_plane(k - 1) && wait_plane(k) && wait_plane(k + 1))) tma_fail_sh = 1;
-        const uint32_t wbase = smem_u32(wsm);
-        const uint32_t bbase = smem_u32(bufs);
-        const int slots[3] = {slot_of(k - 1), slot_of(k), slot_of(k + 1)};
-        int t = 0;
-#pragma unroll 1
-        for (int dk = 0; dk < 3; ++dk)
-#pragma unroll 1
-            for (int dj = 0; dj < 3; ++dj)
-#pragma unroll 1
-                for (int di = 0; di < 3; ++di, ++t) {
-                    uint32_t a_addr = bbase + (uint32_t)((slots[dk] * 3 + di) * BUF_BYTES + dj * GROUP_BYTES);
-                    uint64_t ad = sdesc_sw32(a_addr, 256);
-                    uint64_t bd = sdesc(wbase + (uint32_t)(t * 512), 128, 256);
-                    mma_bf16(tmem + (uint32_t)(16 * acc), ad, bd, t > 0 ? 1u : 0u);
-                }
-        mma_commit(bar[acc]);
+    // bounded wait that also gives up once another role has failed
+    auto wait = [&](uint64_t* b, uint32_t parity) -> bool {
+        const uint32_t a = smem_u32(b);
+        for (long long t = 0; t < WAIT_LIMIT; ++t) {
+            if (mbar_try(a, parity)) return true;
+            if (fail_sh) return false;
+        }
+        fail_sh = 1;
+        return false;
     };
 
-    // Pipeline: while the MMAs of plane k+1 run, the CTA finishes plane k (wait, epilogue) and
-    // has already staged plane k+2; plane k+2 overwrites the slot of plane k-2, whose last
-    // reader (the MMAs of plane k-1) completed in the previous iteration.
-    if (k0 < k1) issue(k0, 0);
-    for (int k = k0; k < k1; ++k) {
-        const int acc = (k - k0) & 1;
-        if (k + 2 <= k1) load_plane(k + 2);
-        asm volatile("tcgen05.fence::before_thread_sync;");
-        __syncthreads();
-        asm volatile("tcgen05.fence::after_thread_sync;");
-        if (k + 1 < k1) issue(k + 1, acc ^ 1);
-        bool ok = mbar_wait_bounded(bar[acc], phase[acc]);
-        phase[acc] ^= 1u;
-        // the decision to stop must be the same in every thread (barriers follow)
-        if (__syncthreads_or((ok && !tma_fail_sh) ? 0 : 1)) {
-            failed = true;
-            accFail = acc;
-            otherPending = k + 1 < k1;
-            break;
+    if (threadIdx.x == PRODUCER_THREAD) {
+        // TMA producer: plane q into slot q mod NPL once the MMAs have released the slot
+        int issued[NPL] = {};
+        for (int q = 0; q < nP; ++q) {
+            const int sl = q % NPL;
+            if (q >= NPL && !wait(&empty[sl], (uint32_t)((q / NPL - 1) & 1))) break;
+            const uint32_t fb = smem_u32(&full[sl]);
+            mbar_expect_tx(fb, 3 * BUF_BYTES);
+            for (int sh = 0; sh < 3; ++sh)
+                tma_load_box(smem_u32(bufs + (size_t)(sl * 3 + sh) * BUF_BYTES), &in_map, i0 + sh - 1, j0 - 1, k0 - 1 + q, fb);
+            ++issued[sl];
         }
-        asm volatile("tcgen05.fence::after_thread_sync;");
-        // epilogue: thread = TMEM lane = output cell
-        float v[16];
-        tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(16 * acc), v);
-        int m = threadIdx.x;
-        int i = i0 + (m & 7), j = j0 + (m >> 3);
-        if (i < L.nI && j < L.nJ) {
-            long long c = ((long long)k * L.nJ + j) * L.nI + i;
-            if (EPI == 1) {
-                out_f[c] = v[0] + bias_sh[0];
-            } else {
-                float o[16];
-                if (EPI == 0) {
+        // every load in flight lands before the shared memory is released
+        for (int sl = 0; sl < NPL; ++sl)
+            if (issued[sl] > 0) mbar_wait_bounded(smem_u32(&full[sl]), (uint32_t)((issued[sl] - 1) & 1));
+    } else if (threadIdx.x == MMA_THREAD) {
+        // MMA issuer: the 27 taps of output plane o into accumulator o mod NACC
+        const uint32_t wbase = smem_u32(wsm);
+        const uint32_t bbase = smem_u32(bufs);
+        int ready = 0;
+        int committed[NACC] = {};
+        for (int o = 0; o < nO; ++o) {
+            const int a = o % NACC;
+            bool ok = true;
+            while (ok && ready < o + 3) {
+                ok = wait(&full[ready % NPL], (uint32_t)((ready / NPL) & 1));
+                ++ready;
+            }
+            if (ok && o >= NACC) ok = wait(&acce[a], (uint32_t)((o / NACC - 1) & 1));
+            if (!ok) break;
+            asm volatile("tcgen05.fence::after_thread_sync;");
+            int t = 0;
+#pragma unroll 1
+            for (int dk = 0; dk < 3; ++dk) {
+                const int sl = (o + dk) % NPL;
+#pragma unroll 1
+                for (int dj = 0; dj < 3; ++dj)
 #pragma unroll
-                    for (int q = 0; q < 16; ++q) o[q] = fmaxf(v[q] + bias_sh[q], 0.f);
+                    for (int di = 0; di < 3; ++di, ++t) {
+                        const uint32_t a_addr = bbase + (uint32_t)((sl * 3 + di) * BUF_BYTES + dj * GROUP_BYTES);
+                        mma_bf16(tmem + (uint32_t)(16 * a), sdesc_sw32(a_addr, 256), sdesc(wbase + (uint32_t)(t * 512), 128, 256),
+                                 t > 0 ? 1u : 0u);
+                    }
+            }
+            mma_commit(smem_u32(&accf[a]));
+            mma_commit(smem_u32(&empty[o % NPL]));
+            ++committed[a];
+        }
+        // every MMA issued completes before the tensor memory is released
+        for (int a = 0; a < NACC; ++a)
+            if (committed[a] > 0) mbar_wait_bounded(smem_u32(&accf[a]), (uint32_t)((committed[a] - 1) & 1));
+    } else if (threadIdx.x < EPI_THREADS) {
+        // epilogue: thread = TMEM lane = output cell (i0 + m mod 8, j0 + m / 8)
+        const int m = threadIdx.x;
+        const int i = i0 + (m & 7), j = j0 + (m >> 3);
+        const bool inside = i < L.nI && j < L.nJ;
+        for (int o = 0; o < nO; ++o) {
+            const int a = o % NACC;
+            // warp-uniform outcome: the tcgen05.ld below is a warp-wide instruction
+            if (!__all_sync(0xffffffffu, wait(&accf[a], (uint32_t)((o / NACC) & 1)) ? 1 : 0)) break;
+            asm volatile("tcgen05.fence::after_thread_sync;");
+            float v[16];
+            tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(16 * a), v);
+            asm volatile("tcgen05.fence::before_thread_sync;");
+            asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&acce[a])) : "memory");
+            if (inside) {
+                const long long c = ((long long)(k0 + o) * L.nJ + j) * L.nI + i;
+                if (EPI == 1) {
+                    out_f[c] = v[0] + bias_sh[0];
                 } else {
-                    const __nv_bfloat16* mp = mask_act + c * 16;
+                    float r[16];
+                    if (EPI == 0) {
 #pragma unroll
-                    for (int q = 0; q < 16; ++q) o[q] = __bfloat162float(mp[q]) > 0.f ? v[q] : 0.f;
+                        for (int q = 0; q < 16; ++q) r[q] = fmaxf(v[q] + bias_sh[q], 0.f);
+                    } else {
+                        const uint4* mp = reinterpret_cast<const uint4*>(mask_act + c * 16);
+                        const uint4 m0 = mp[0], m1 = mp[1];
+                        const __nv_bfloat16* mk0 = reinterpret_cast<const __nv_bfloat16*>(&m0);
+                        const __nv_bfloat16* mk1 = reinterpret_cast<const __nv_bfloat16*>(&m1);
+#pragma unroll
+                        for (int q = 0; q < 8; ++q) {
+                            r[q] = __bfloat162float(mk0[q]) > 0.f ? v[q] : 0.f;
+                            r[8 + q] = __bfloat162float(mk1[q]) > 0.f ? v[8 + q] : 0.f;
+                        }
+                    }
+                    __align__(16) __nv_bfloat16 ob[16];
+#pragma unroll
+                    for (int q = 0; q < 16; ++q) ob[q] = __float2bfloat16_rn(r[q]);
+                    uint4* dst = reinterpret_cast<uint4*>(out_bf + c * out_stride);
+                    dst[0] = reinterpret_cast<uint4*>(ob)[0];
+                    dst[1] = reinterpret_cast<uint4*>(ob)[1];
                 }
-                __align__(16) __nv_bfloat16 ob[16];
-#pragma unroll
-                for (int q = 0; q < 16; ++q) ob[q] = __float2bfloat16_rn(o[q]);
-                uint4* dst = reinterpret_cast<uint4*>(out_bf + c * out_stride);
-                dst[0] = reinterpret_cast<uint4*>(ob)[0];
-                dst[1] = reinterpret_cast<uint4*>(ob)[1];
             }
         }
-        // the accumulator just read is rewritten by the MMAs of plane k+2, issued in the next
-        // iteration after its barrier, i.e. after every thread has finished this epilogue
-        asm volatile("tcgen05.fence::before_thread_sync;");
     }
-    if (failed) {
-        if (threadIdx.x == 0) atomicExch(err, 1);
-        // let the MMAs still in flight (at most the other accumulator's plane) finish before
-        // the tensor memory is freed
-        mbar_wait_bounded(bar[accFail], phase[accFail] ^ 1u);        // the plane whose wait ran out
-        if (otherPending) mbar_wait_bounded(bar[accFail ^ 1], phase[accFail ^ 1]);
-        // and the TMA loads still in flight before the shared memory goes away
-        if (threadIdx.x == 0)
-            for (int q = 0; q < NPL; ++q)
-                if (loads[q] > 0) mbar_wait_bounded(smem_u32(&lbar[q]), (uint32_t)((loads[q] - 1) & 1));
-    }
+    __syncwarp();
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;");
+    if (threadIdx.x == 0 && fail_sh) atomicExch(err, 1);
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
 }
 
-size_t conv_smem_bytes() { return 1024 + W_BYTES + NBUF * BUF_BYTES; }
+size_t conv_smem_bytes() { return 1024 + W_BYTES + (size_t)NPL * 3 * BUF_BYTES; }
 
 // ------------------------------------------------------------------ weight gradient
 // dW[t][o][i] = sum_c x[c + off(t)][i] dz[c][o] (db[o] = sum_c dz[c][o]) as an implicit GEMM on the
@@ -550,9 +567,9 @@ int launch_conv3d(const Lat& L, int epi, const __nv_bfloat16* in, const __nv_bfl
         CB_CUDA(cudaFuncSetAttribute(conv3d_tc_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         attr = true;
     }
-    if (epi == 0) conv3d_tc_kernel<0><<<grid, 128, smem, st>>>(L, in_map, wpack, bias, out_bf, out_f, 16, mask_act, KC, err, skip);
-    else if (epi == 1) conv3d_tc_kernel<1><<<grid, 128, smem, st>>>(L, in_map, wpack, bias, out_bf, out_f, 16, mask_act, KC, err, skip);
-    else conv3d_tc_kernel<2><<<grid, 128, smem, st>>>(L, in_map, wpack, bias, out_bf, out_f, 16, mask_act, KC, err, skip);
+    if (epi == 0) conv3d_tc_kernel<0><<<grid, CONV_THREADS, smem, st>>>(L, in_map, wpack, bias, out_bf, out_f, 16, mask_act, KC, err, skip);
+    else if (epi == 1) conv3d_tc_kernel<1><<<grid, CONV_THREADS, smem, st>>>(L, in_map, wpack, bias, out_bf, out_f, 16, mask_act, KC, err, skip);
+    else conv3d_tc_kernel<2><<<grid, CONV_THREADS, smem, st>>>(L, in_map, wpack, bias, out_bf, out_f, 16, mask_act, KC, err, skip);
     CB_CHECK_LAUNCH();
     return 0;
 }

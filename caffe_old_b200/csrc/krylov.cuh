@@ -49,6 +49,7 @@ struct KspOut {
     double relres[3];
     int status[3];      // 0 converged, 1 maxit, 2 breakdown, 3 non-finite
     int cascades;       // learned solve only: 1 when its network stage handed over to the pyramid stage
+    int net_iters;      // learned solve only: inner iterations run with the network in the preconditioner
 };
 
 // Workspace for up to NR = 3 right-hand sides; every array is a halo-padded cell array of

@@ -1389,9 +1389,10 @@ int learned_solve(LearnedWork& lw, const OpSym& A, const uint8_t* status, const 
     // it reached, with the same pyramid and an identity in place of the network (a fixed linear
     // preconditioner, so BiCGStab or flexible CG apply); only a solve that misses the tolerance
     // there too leaves status != 0 for the plain FP64 re-solve.
-    int cascades = 0;
+    int cascades = 0, netIters = 0;
     {
         Scal* hs = static_cast<Scal*>(lw.hostScal);
+        if (mode == NET_MODE_NETWORK) netIters = hs->iters;
         if (mode == NET_MODE_NETWORK && (hs->status == 1 || hs->status == 2)) {
             const int itersSoFar = hs->iters;
             reopen_kernel<<<1, 32, 0, st>>>(S);
@@ -1401,6 +1402,7 @@ int learned_solve(LearnedWork& lw, const OpSym& A, const uint8_t* status, const 
         }
     }
     CB_CUDA(cudaMemcpyAsync(&out->cascades, &cascades, sizeof(int), cudaMemcpyHostToDevice, st));
+    CB_CUDA(cudaMemcpyAsync(&out->net_iters, &netIters, sizeof(int), cudaMemcpyHostToDevice, st));
     publish_kernel<<<1, 32, 0, st>>>(S, out);
     CB_CHECK_LAUNCH();
     CB_CUDA(cudaMemcpyAsync(lw.hostScal, S, sizeof(Scal), cudaMemcpyDeviceToHost, st));

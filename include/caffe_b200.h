@@ -78,6 +78,8 @@ typedef struct caffe_step_stats {
     double p_ms, mom_ms, step_ms;   /* device time of the step's phases (CUDA events) */
     int cascades;           /* learned p' solves whose network stage stalled and that finished with
                              * the pyramid alone (an identity in place of the network) */
+    int net_iters;          /* inner iterations of the step's learned p' solves run with the network
+                             * in the preconditioner (the rest ran with the pyramid alone) */
 } caffe_step_stats;
 
 typedef struct caffe_dev caffe_dev;
