@@ -57,6 +57,21 @@ constexpr int EPI_THREADS = 128;        // warps 0-3: epilogue
 constexpr int PRODUCER_THREAD = 128;    // warp 4, lane 0: TMA loads
 constexpr int MMA_THREAD = 160;         // warp 5, lane 0: MMA issue
 constexpr int CONV_THREADS = 192;
+
+// one lattice of a grouped convolution launch (kernel parameter space)
+struct ConvJob {
+    CUtensorMap map;                 // activations in (this GPU's own buffer)
+    Lat L;
+    __nv_bfloat16* out_bf;
+    float* out_f;
+    const __nv_bfloat16* mask;
+    int KC, gx, gy;
+};
+struct ConvGroup {
+    ConvJob job[CONV_MAX_JOBS];
+    int ctaEnd[CONV_MAX_JOBS];       // inclusive prefix sums of the jobs' CTA counts
+    int n;
+};
 constexpr long long WAIT_LIMIT = 1ll << 20;   // try_wait rounds (each may block briefly): about a second at most
 
 // instruction descriptor: kind::f16, D = F32, A = B = BF16, both K-major, N = 16, M = 128
@@ -159,14 +174,28 @@ __device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
 // Input plane q (= k0 - 1 + q) lives in slot q mod NPL; output plane o (= k0 + o) reads input
 // planes o, o+1, o+2 and accumulates in TMEM columns 16 (o mod NACC).  The producer runs up to
 // NPL - 3 planes ahead of the MMAs and the MMAs up to NACC - 1 planes ahead of the epilogue.
+//
+// One launch serves a group of up to CONV_MAX_JOBS lattices (the levels of a pyramid and both
+// signs of the odd network form): the CTAs of job p are blocks ctaEnd[p-1] .. ctaEnd[p]-1, each
+// job with its own tensor map, lattice, outputs and k-planes per CTA, and every job the same layer
+// weights.
 template <int EPI>
-__global__ void __launch_bounds__(CONV_THREADS) conv3d_tc_kernel(Lat L, const __grid_constant__ CUtensorMap in_map,
+__global__ void __launch_bounds__(CONV_THREADS) conv3d_tc_kernel(const __grid_constant__ ConvGroup g,
                                                                  const __nv_bfloat16* __restrict__ wpack, const float* __restrict__ bias,
-                                                                 __nv_bfloat16* out_bf, float* out_f, long long out_stride,
-                                                                 const __nv_bfloat16* __restrict__ mask_act, int KC, int* err,
-                                                                 const int* __restrict__ skip) {
+                                                                 int* err, const int* __restrict__ skip) {
     // a solve that has already converged turns its remaining launches into no-ops (uniform)
     if (skip && *skip) return;
+    int job = 0;
+    while (job + 1 < g.n && (int)blockIdx.x >= g.ctaEnd[job]) ++job;
+    const ConvJob& J = g.job[job];
+    const Lat L = J.L;
+    const CUtensorMap* in_map = &J.map;
+    __nv_bfloat16* out_bf = J.out_bf;
+    float* out_f = J.out_f;
+    const __nv_bfloat16* __restrict__ mask_act = J.mask;
+    const int KC = J.KC;
+    const int local = (int)blockIdx.x - (job > 0 ? g.ctaEnd[job - 1] : 0);
+    const int bx = local % J.gx, by = (local / J.gx) % J.gy, bz = local / (J.gx * J.gy);
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     // 1 KiB-align the dynamic region
     unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -177,8 +206,8 @@ __global__ void __launch_bounds__(CONV_THREADS) conv3d_tc_kernel(Lat L, const __
     __shared__ float bias_sh[16];
     __shared__ volatile int fail_sh;
 
-    const int i0 = blockIdx.x * TI, j0 = blockIdx.y * TJ;
-    const int k0 = blockIdx.z * KC;
+    const int i0 = bx * TI, j0 = by * TJ;
+    const int k0 = bz * KC;
     const int nO = min(k0 + KC, L.nK) - k0;   // output planes of this CTA
     const int nP = nO + 2;                    // input planes k0-1 .. k0+nO
     const int warp = threadIdx.x >> 5;
@@ -230,7 +259,7 @@ __global__ void __launch_bounds__(CONV_THREADS) conv3d_tc_kernel(Lat L, const __
             const uint32_t fb = smem_u32(&full[sl]);
             mbar_expect_tx(fb, 3 * BUF_BYTES);
             for (int sh = 0; sh < 3; ++sh)
-                tma_load_box(smem_u32(bufs + (size_t)(sl * 3 + sh) * BUF_BYTES), &in_map, i0 + sh - 1, j0 - 1, k0 - 1 + q, fb);
+                tma_load_box(smem_u32(bufs + (size_t)(sl * 3 + sh) * BUF_BYTES), in_map, i0 + sh - 1, j0 - 1, k0 - 1 + q, fb);
             ++issued[sl];
         }
         // every load in flight lands before the shared memory is released
@@ -309,7 +338,7 @@ __global__ void __launch_bounds__(CONV_THREADS) conv3d_tc_kernel(Lat L, const __
                     __align__(16) __nv_bfloat16 ob[16];
 #pragma unroll
                     for (int q = 0; q < 16; ++q) ob[q] = __float2bfloat16_rn(r[q]);
-                    uint4* dst = reinterpret_cast<uint4*>(out_bf + c * out_stride);
+                    uint4* dst = reinterpret_cast<uint4*>(out_bf + c * 16);
                     dst[0] = reinterpret_cast<uint4*>(ob)[0];
                     dst[1] = reinterpret_cast<uint4*>(ob)[1];
                 }
@@ -536,30 +565,25 @@ int make_act_tensor_map(CUtensorMap* map, const __nv_bfloat16* base, const Lat& 
     return 0;
 }
 
-int launch_conv3d(const Lat& L, int epi, const __nv_bfloat16* in, const __nv_bfloat16* wpack, const float* bias, __nv_bfloat16* out_bf,
-                  float* out_f, const __nv_bfloat16* mask_act, int* err, cudaStream_t st, const int* skip) {
-    // encoded maps are kept per (buffer, lattice): the solve reuses the same few activation buffers
+namespace {
+// encoded maps are kept per (buffer, lattice): the solves reuse the same few activation buffers
+const CUtensorMap* cached_map(const __nv_bfloat16* in, const Lat& L) {
     static std::vector<std::pair<std::array<long long, 4>, CUtensorMap>> cache;
     static std::mutex cacheLock;
     std::lock_guard<std::mutex> guard(cacheLock);
     const std::array<long long, 4> key = {(long long)(uintptr_t)in, L.nI, L.nJ, L.nK};
-    const CUtensorMap* mp = nullptr;
     for (auto& e : cache)
-        if (e.first == key) { mp = &e.second; break; }
-    if (!mp) {
-        CUtensorMap m;
-        if (make_act_tensor_map(&m, in, L)) return 1;
-        cache.emplace_back(key, m);
-        mp = &cache.back().second;
-    }
-    const CUtensorMap in_map = *mp;
-    // k-planes per CTA: up to 16 (one staged plane serves three output planes), fewer on small
-    // lattices so that the grid still covers the SMs twice
-    const long long gxy = (long long)((L.nI + TI - 1) / TI) * ((L.nJ + TJ - 1) / TJ);
-    const long long kc = gxy * L.nK / 296;
-    const int KC = (int)(kc < 1 ? 1 : (kc > 16 ? 16 : kc));
-    dim3 grid((L.nI + TI - 1) / TI, (L.nJ + TJ - 1) / TJ, (L.nK + KC - 1) / KC);
-    size_t smem = conv_smem_bytes();
+        if (e.first == key) return &e.second;
+    CUtensorMap m;
+    if (make_act_tensor_map(&m, in, L)) return nullptr;
+    cache.emplace_back(key, m);
+    return &cache.back().second;
+}
+}  // namespace
+
+int launch_conv3d_group(int epi, const ConvSpec* specs, int n, const __nv_bfloat16* wpack, const float* bias, int* err, cudaStream_t st,
+                        const int* skip) {
+    const size_t smem = conv_smem_bytes();
     static bool attr = false;
     if (!attr) {
         CB_CUDA(cudaFuncSetAttribute(conv3d_tc_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -567,11 +591,44 @@ int launch_conv3d(const Lat& L, int epi, const __nv_bfloat16* in, const __nv_bfl
         CB_CUDA(cudaFuncSetAttribute(conv3d_tc_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         attr = true;
     }
-    if (epi == 0) conv3d_tc_kernel<0><<<grid, CONV_THREADS, smem, st>>>(L, in_map, wpack, bias, out_bf, out_f, 16, mask_act, KC, err, skip);
-    else if (epi == 1) conv3d_tc_kernel<1><<<grid, CONV_THREADS, smem, st>>>(L, in_map, wpack, bias, out_bf, out_f, 16, mask_act, KC, err, skip);
-    else conv3d_tc_kernel<2><<<grid, CONV_THREADS, smem, st>>>(L, in_map, wpack, bias, out_bf, out_f, 16, mask_act, KC, err, skip);
-    CB_CHECK_LAUNCH();
+    for (int b = 0; b < n; b += CONV_MAX_JOBS) {
+        ConvGroup g;
+        std::memset(&g, 0, sizeof(g));
+        g.n = std::min(CONV_MAX_JOBS, n - b);
+        long long ctas = 0;
+        for (int p = 0; p < g.n; ++p) {
+            const ConvSpec& sp = specs[b + p];
+            const Lat& L = sp.L;
+            const CUtensorMap* mp = cached_map(sp.in, L);
+            if (!mp) return 1;
+            ConvJob& J = g.job[p];
+            J.map = *mp;
+            J.L = L;
+            J.out_bf = sp.out_bf; J.out_f = sp.out_f; J.mask = sp.mask;
+            J.gx = (L.nI + TI - 1) / TI;
+            J.gy = (L.nJ + TJ - 1) / TJ;
+            // k-planes per CTA: up to 16 (one staged plane serves three output planes), fewer on
+            // small lattices so that the job alone would still cover the SMs twice
+            const long long kc = (long long)J.gx * J.gy * L.nK / 296;
+            J.KC = (int)(kc < 1 ? 1 : (kc > 16 ? 16 : kc));
+            ctas += (long long)J.gx * J.gy * ((L.nK + J.KC - 1) / J.KC);
+            if (ctas > (1ll << 30)) { set_error("convolution group too large"); return 1; }
+            g.ctaEnd[p] = (int)ctas;
+        }
+        const unsigned grid = (unsigned)ctas;
+        if (epi == 0) conv3d_tc_kernel<0><<<grid, CONV_THREADS, smem, st>>>(g, wpack, bias, err, skip);
+        else if (epi == 1) conv3d_tc_kernel<1><<<grid, CONV_THREADS, smem, st>>>(g, wpack, bias, err, skip);
+        else conv3d_tc_kernel<2><<<grid, CONV_THREADS, smem, st>>>(g, wpack, bias, err, skip);
+        CB_CHECK_LAUNCH();
+    }
     return 0;
+}
+
+int launch_conv3d(const Lat& L, int epi, const __nv_bfloat16* in, const __nv_bfloat16* wpack, const float* bias, __nv_bfloat16* out_bf,
+                  float* out_f, const __nv_bfloat16* mask_act, int* err, cudaStream_t st, const int* skip) {
+    ConvSpec sp;
+    sp.L = L; sp.in = in; sp.out_bf = out_bf; sp.out_f = out_f; sp.mask = mask_act;
+    return launch_conv3d_group(epi, &sp, 1, wpack, bias, err, st, skip);
 }
 
 }  // namespace cb

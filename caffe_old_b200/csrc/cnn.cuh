@@ -22,6 +22,20 @@ size_t conv_smem_bytes();
 int launch_conv3d(const Lat& L, int epi, const __nv_bfloat16* in, const __nv_bfloat16* wpack, const float* bias, __nv_bfloat16* out_bf,
                   float* out_f, const __nv_bfloat16* mask_act, int* err, cudaStream_t st, const int* skip = nullptr);
 
+// One convolution layer over several lattices in one launch (the same weights and epilogue):
+// input activations in, bf16 activations out (epi 0 / 2) or FP32 channel 0 out (epi 1), the
+// ReLU mask of epi 2.
+constexpr int CONV_MAX_JOBS = 16;
+struct ConvSpec {
+    Lat L;
+    const __nv_bfloat16* in;
+    __nv_bfloat16* out_bf;
+    float* out_f;
+    const __nv_bfloat16* mask;
+};
+int launch_conv3d_group(int epi, const ConvSpec* specs, int n, const __nv_bfloat16* wpack, const float* bias, int* err, cudaStream_t st,
+                        const int* skip = nullptr);
+
 // Weight gradient of one layer on the tensor cores: dW[t][o][i] += sum_c x[c + off(t)][i] dz[c][o],
 // db[o] += sum_c dz[c][o] (FP32, accumulated into dW / db).
 int launch_weight_grad(const Lat& L, const __nv_bfloat16* x, const __nv_bfloat16* dz, float* dW, float* db, int* err, cudaStream_t st);
@@ -47,6 +61,9 @@ int net_pack_weights(NetBuffers& nb, cudaStream_t st);
 int net_forward(NetBuffers& nb, cudaStream_t st);
 // same, every launch a no-op while *skip is non-zero
 int net_forward_if(NetBuffers& nb, const int* skip, cudaStream_t st);
+// the forward passes of several networks that share one set of weights (nets[0]'s), one
+// launch per layer for all of them
+int net_forward_group_if(NetBuffers* const* nets, int n, const int* skip, cudaStream_t st);
 // backward for dL/dy (FP32, N): accumulates dL/dparams into nb.grad
 int net_backward(NetBuffers& nb, const float* dy, cudaStream_t st);
 // act[0] from a 2-channel FP32 input laid out [N][2]

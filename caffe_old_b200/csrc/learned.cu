@@ -1094,8 +1094,14 @@ int apply_levels(LearnedWork& lw, const float* rfine, const uint8_t* status, int
                                                                    c.mask, c.chan, S);
     }
     CB_CHECK_LAUNCH();
-    for (int l = 1; l < lw.nLev; ++l)
-        if (netAt(l) && (net_forward_if(lw.lev[l].net, &S->done, st) || net_forward_if(lw.lev[l].netNeg, &S->done, st))) return 1;
+    // every network level and both signs of the odd form: one grouped launch per layer
+    {
+        NetBuffers* nets[2 * LEARN_MAX_LEVELS];
+        int nn = 0;
+        for (int l = 1; l < lw.nLev; ++l)
+            if (netAt(l)) { nets[nn++] = &lw.lev[l].net; nets[nn++] = &lw.lev[l].netNeg; }
+        if (nn > 0 && net_forward_group_if(nets, nn, &S->done, st)) return 1;
+    }
     for (int l = lw.nLev - 1; l >= 1; --l) {
         Level& f = lw.lev[l];
         const bool top = l + 1 >= lw.nLev;

@@ -112,6 +112,25 @@ int net_forward_if(NetBuffers& nb, const int* skip, cudaStream_t st) {
 
 int net_forward(NetBuffers& nb, cudaStream_t st) { return net_forward_if(nb, nullptr, st); }
 
+int net_forward_group_if(NetBuffers* const* nets, int n, const int* skip, cudaStream_t st) {
+    if (n < 1) return 0;
+    std::vector<ConvSpec> sp((size_t)n);
+    for (int l = 0; l < NET_LAYERS; ++l) {
+        for (int q = 0; q < n; ++q) {
+            NetBuffers& nb = *nets[q];
+            if (nb.wfwd != nets[0]->wfwd) { set_error("grouped networks must share their weights"); return 1; }
+            sp[q].L = nb.L;
+            sp[q].in = nb.act[l];
+            sp[q].out_bf = l < NET_LAYERS - 1 ? nb.act[l + 1] : nullptr;
+            sp[q].out_f = l < NET_LAYERS - 1 ? nullptr : nb.y;
+            sp[q].mask = nullptr;
+        }
+        if (launch_conv3d_group(l < NET_LAYERS - 1 ? 0 : 1, sp.data(), n, wf_of(*nets[0], l), bias_of(*nets[0], l), nets[0]->err, st, skip))
+            return 1;
+    }
+    return 0;
+}
+
 static int weight_grad(NetBuffers& nb, int l, const __nv_bfloat16* x, const __nv_bfloat16* dz, cudaStream_t st) {
     float* g = nb.grad + (size_t)l * NET_LAYER_PARAMS;
     return launch_weight_grad(nb.L, x, dz, g, g + 27 * 256, nb.err, st);
