@@ -454,6 +454,7 @@ long caffe_diffusion_array(caffe_diffusion* h, const char* name, double* host, l
     else if (n == "phiFaceK") { base = h->face[2]; len = L.nFK; }
     else if (n.size() == 9 && n.compare(0, 8, "phiPatch") == 0 && n[8] >= '0' && n[8] <= '5') { base = h->patch[n[8] - '0']; len = h->patchN[n[8] - '0']; }
     else if (n == "gradPhi") { base = h->grad; len = L.N; planes = 3; stride = L.PS; }
+    else if (n == "cc") { base = h->cc; len = L.N; planes = 3; stride = L.PS; }
     else if (n == "A") { len = L.N; planes = 7; }
     else { set_error("unknown array " + n); return -1; }
     const long need = (long)(len * planes);

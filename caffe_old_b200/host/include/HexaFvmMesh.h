@@ -6,6 +6,7 @@
 #include <fstream>
 #include <memory>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "Vector3D.h"
@@ -41,4 +42,5 @@ protected:
     std::string name_ = "mesh";
     mutable const Solver* solver_ = nullptr;
     std::ofstream foutTec360_;
+    std::vector<std::pair<std::string, int>> tecVars_;   // the variables of the open Tecplot file
 };

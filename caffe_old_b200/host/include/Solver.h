@@ -4,6 +4,7 @@
 // iteration / time step on the GPU and returns the maximum continuity error.
 #pragma once
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "HexaFvmMesh.h"
@@ -24,8 +25,11 @@ public:
 
     // host copies of device fields, component planes of nCells each: "u" (3 planes), "p",
     // "pCorr", "massFlowI/J/K", ... (names of caffe_dev_array)
-    std::vector<double> field(const std::string& name) const;
-    void setField(const std::string& name, const std::vector<double>& values);
+    virtual std::vector<double> field(const std::string& name) const;
+    virtual void setField(const std::string& name, const std::vector<double>& values);
+    // the cell fields the solver registers for Tecplot output, in the order they are written,
+    // with their component counts (Simple.cpp:57-59: p, massFlow, then the vector u)
+    virtual std::vector<std::pair<std::string, int>> tecplotFields() const { return {{"p", 1}, {"massFlow", 1}, {"u", 3}}; }
     const caffe_step_stats& lastStats() const { return stats_; }
     const caffe_case& caseParameters() const { return case_; }
     caffe_dev* handle() const { return h_; }
@@ -36,6 +40,8 @@ public:
     static caffe_case caseFromInput(const Input& input, int kind);
 
 protected:
+    // a solver with its own device handle (Coupled, Diffusion): no flow-solver handle
+    Solver(const HexaFvmMesh& mesh, const char* name);
     double step(double timeStep);
     const HexaFvmMesh& mesh_;
     caffe_case case_;

@@ -88,15 +88,23 @@ void HexaFvmMesh::writeTec360(double time, const std::string& directory) {
         foutTec360_.open(directory + name_ + ".dat");
         if (!foutTec360_) Output::raiseException("HexaFvmMesh", "writeTec360", "cannot open \"" + directory + name_ + ".dat\"");
         foutTec360_ << std::setprecision(16);
-        foutTec360_ << "TITLE = \"" << name_ << "\"\n"
-                    << "VARIABLES = \"x\", \"y\", \"z\", \"p\", \"massFlow\", \"u_x\", \"u_y\", \"u_z\"\n";
     }
-    // the fields the reference's solvers register for output, scalars first (p, massFlow), then
-    // the vector u (Simple.cpp:57-59, HexaFvmMesh.cpp:479-611)
-    const std::vector<double> u = solver_->field("u"), p = solver_->field("p"), mf = solver_->field("massFlow");
+    // the fields the solver registers for output, scalars first, then vectors by component
+    // (HexaFvmMesh.cpp:479-611)
+    const auto vars = solver_->tecplotFields();
+    if (tecVars_.empty()) {
+        static const char* comp[3] = {"_x", "_y", "_z"};
+        foutTec360_ << "TITLE = \"" << name_ << "\"\n" << "VARIABLES = \"x\", \"y\", \"z\"";
+        for (const auto& v : vars)
+            for (int c = 0; c < v.second; ++c) foutTec360_ << ", \"" << v.first << (v.second > 1 ? comp[c] : "") << "\"";
+        foutTec360_ << "\n";
+        tecVars_ = vars;
+    }
+    int nVar = 0;
+    for (const auto& v : tecVars_) nVar += v.second;
     const size_t N = (size_t)nI_ * nJ_ * nK_;
     foutTec360_ << "ZONE T = \"" << time << "\", I = " << nI_ + 1 << ", J = " << nJ_ + 1 << ", K = " << nK_ + 1
-                << ", DATAPACKING = BLOCK, VARLOCATION = ([4-8] = CELLCENTERED), SOLUTIONTIME = " << time << "\n";
+                << ", DATAPACKING = BLOCK, VARLOCATION = ([4-" << 3 + nVar << "] = CELLCENTERED), SOLUTIONTIME = " << time << "\n";
     const size_t nn = nodes_.size() / 3;
     for (int l = 0; l < 3; ++l) {
         for (size_t q = 0; q < nn; ++q) foutTec360_ << nodes_[3 * q + l] << (q % 8 == 7 ? '\n' : ' ');
@@ -106,9 +114,10 @@ void HexaFvmMesh::writeTec360(double time, const std::string& directory) {
         for (size_t q = 0; q < N; ++q) foutTec360_ << a[q] << (q % 8 == 7 ? '\n' : ' ');
         foutTec360_ << '\n';
     };
-    block(p.data());
-    block(mf.data());
-    for (int c = 0; c < 3; ++c) block(u.data() + c * N);
+    for (const auto& v : tecVars_) {
+        const std::vector<double> a = solver_->field(v.first);
+        for (int c = 0; c < v.second; ++c) block(a.data() + c * N);
+    }
     foutTec360_.flush();
 }
 

@@ -21,6 +21,8 @@
 #include <fstream>
 #include <iostream>
 
+#include "Coupled.h"
+#include "Diffusion.h"
 #include "IbPiso.h"
 #include "MultiphasePiso.h"
 #include "InitialConditions.h"
@@ -165,6 +167,12 @@ Solver::Solver(const Input& input, const HexaFvmMesh& mesh, int kind) : mesh_(me
     mesh.attachSolver(this);
 }
 
+Solver::Solver(const HexaFvmMesh& mesh, const char* name) : mesh_(mesh) {
+    std::memset(&case_, 0, sizeof(case_));
+    name_ = name;
+    mesh.attachSolver(this);
+}
+
 Solver::~Solver() {
     mesh_.detachSolver(this);
     if (h_) caffe_dev_destroy(h_);
@@ -211,3 +219,152 @@ double IbPiso::solve(double timeStep) { return step(timeStep); }
 
 MultiphasePiso::MultiphasePiso(const Input& input, const HexaFvmMesh& mesh) : Piso(input, mesh, CAFFE_PISO) { name_ = "MultiphasePiso"; }
 double MultiphasePiso::solve(double timeStep) { return step(timeStep); }
+
+// ---------------------------------------------------------------------------- Coupled
+namespace {
+
+// an interleaved N x c host array from the device library as c planes of N
+std::vector<double> to_planes(const std::vector<double>& a, int comps) {
+    if (comps == 1) return a;
+    const size_t n = a.size() / comps;
+    std::vector<double> out(a.size());
+    for (size_t q = 0; q < n; ++q)
+        for (int c = 0; c < comps; ++c) out[c * n + q] = a[q * comps + c];
+    return out;
+}
+std::vector<double> to_interleaved(const std::vector<double>& a, int comps) {
+    if (comps == 1) return a;
+    const size_t n = a.size() / comps;
+    std::vector<double> out(a.size());
+    for (size_t q = 0; q < n; ++q)
+        for (int c = 0; c < comps; ++c) out[q * comps + c] = a[c * n + q];
+    return out;
+}
+int vector_components(const std::string& name) { return name == "u" || name == "u0" || name == "gradP" || name == "h" || name == "gradPhi" || name == "cc" ? 3 : 1; }
+
+}  // namespace
+
+Coupled::Coupled(const Input& input, const HexaFvmMesh& mesh) : Solver(mesh, "Coupled") {
+    const InfoTree& c = input.caseParameters;
+    static const char* faces[6] = {"east", "west", "north", "south", "top", "bottom"};
+    for (int f = 0; f < 6; ++f) {
+        std::string b = std::string("Boundaries.") + faces[f];
+        case_.bc_type[f] = face_type(c.get<std::string>(b + ".type"));
+        case_.ref_val[f] = c.get<double>(b + ".refValue");
+        Vector3D v = std::stov(c.get<std::string>(b + ".refVector"));
+        case_.ref_vec[f][0] = v.x; case_.ref_vec[f][1] = v.y; case_.ref_vec[f][2] = v.z;
+    }
+    case_.kind = CAFFE_SIMPLE;
+    case_.time_accurate = c.get<std::string>("Solver.timeAccurate") == "ON" ? 1 : 0;
+    case_.n_inner = case_.time_accurate ? c.get<int>("Solver.numberOfInnerIterations") : 1;
+    case_.omega_u = c.get<double>("Solver.relaxationFactorMomentum");
+    case_.omega_p = 1.;
+    case_.rho = c.get<double>("Solver.rho");
+    case_.mu = c.get<double>("Solver.mu");
+    case_.mom_method = ksp_method(c.get<std::string>("LinearSolvers.momentum", std::string("bicgstab_jacobi")));
+    case_.p_method = case_.mom_method;
+    case_.mom_rtol = case_.p_rtol = c.get<double>("LinearSolvers.tolerance", 1e-8);
+    case_.mom_atol = case_.p_atol = c.get<double>("LinearSolvers.absoluteTolerance", 0.);
+    case_.maxit = c.get<int>("LinearSolvers.maxIterations", 20000);
+    const int nI1 = mesh.nCellsI() + 1, nJ1 = mesh.nCellsJ() + 1, nK1 = mesh.nCellsK() + 1;
+    if (caffe_coupled_create(mesh.nodes().data(), nI1, nJ1, nK1, &case_, 0, &hc_) != 0)
+        Output::raiseException("Coupled", "Coupled", std::string("device set-up failed: ") + caffe_last_error());
+}
+
+Coupled::~Coupled() {
+    if (hc_) caffe_coupled_destroy(hc_);
+}
+
+double Coupled::solve(double timeStep) {
+    if (caffe_coupled_solve(hc_, timeStep, &continuity_) != 0)
+        Output::raiseException("Coupled", "solve", std::string("device step failed: ") + caffe_last_error());
+    return continuity_;
+}
+
+void Coupled::displayUpdateMessage() {
+    int iters = 0, status = 0;
+    double relres = 0.;
+    caffe_coupled_stats(hc_, &iters, &relres, &status);
+    Output::print("Coupled", "completed iteration.");
+    Output::print("Coupled", "Krylov iterations (block system) : " + std::to_string(iters));
+    Output::print("Coupled", "Max continuity error             : " + std::to_string(continuity_));
+    Output::printLine();
+}
+
+std::vector<double> Coupled::field(const std::string& name) const {
+    if (name == "massFlow") return std::vector<double>((size_t)mesh_.nCells(), 0.);
+    long n = caffe_coupled_array(hc_, name.c_str(), nullptr, 0, 0);
+    if (n < 0) Output::raiseException("Coupled", "field", "unknown field \"" + name + "\"");
+    std::vector<double> out((size_t)n);
+    if (caffe_coupled_array(hc_, name.c_str(), out.data(), n, 0) < 0)
+        Output::raiseException("Coupled", "field", std::string("read failed: ") + caffe_last_error());
+    return to_planes(out, vector_components(name));
+}
+
+void Coupled::setField(const std::string& name, const std::vector<double>& values) {
+    std::vector<double> v = to_interleaved(values, vector_components(name));
+    if (caffe_coupled_array(hc_, name.c_str(), v.data(), (long)v.size(), 1) < 0)
+        Output::raiseException("Coupled", "setField", std::string("write failed: ") + caffe_last_error());
+}
+
+// ---------------------------------------------------------------------------- Diffusion
+Diffusion::Diffusion(const Input& input, const HexaFvmMesh& mesh) : Solver(mesh, "Diffusion") {
+    const InfoTree& c = input.caseParameters;
+    static const char* faces[6] = {"east", "west", "north", "south", "top", "bottom"};
+    int types[6];
+    double refs[6];
+    for (int f = 0; f < 6; ++f) {
+        std::string b = std::string("Boundaries.") + faces[f];
+        const std::string t = c.get<std::string>(b + ".type");
+        if (t == "fixed") types[f] = 0;
+        else if (t == "zeroGradient") types[f] = 1;
+        else if (t == "empty") types[f] = 2;
+        else Output::raiseException("FlowBoundaryCondition", "FlowBoundaryCondition", "invalid boundary type \"" + t + "\".");
+        refs[f] = c.get<double>(b + ".refValue");
+    }
+    case_.time_accurate = c.get<std::string>("Solver.timeAccurate") == "ON" ? 1 : 0;
+    const int method = ksp_method(c.get<std::string>("LinearSolvers.diffusion", std::string("bicgstab_jacobi")));
+    const double rtol = c.get<double>("LinearSolvers.tolerance", 1e-8);
+    const int maxit = c.get<int>("LinearSolvers.maxIterations", 20000);
+    // a uniform phi goes in at creation; other initial conditions are evaluated at the centroids
+    InitialConditions ics(input);
+    double phi0 = 0.;
+    const bool uniform = !ics.has("phi") || input.initialConditions.get<std::string>("phi.type") == "uniform";
+    if (uniform && input.initialConditions.has("phi.value")) phi0 = input.initialConditions.get<double>("phi.value");
+    const int nI1 = mesh.nCellsI() + 1, nJ1 = mesh.nCellsJ() + 1, nK1 = mesh.nCellsK() + 1;
+    if (caffe_diffusion_create(mesh.nodes().data(), nI1, nJ1, nK1, types, refs, case_.time_accurate, phi0, method, rtol, maxit, 0, &hd_) != 0)
+        Output::raiseException("Diffusion", "Diffusion", std::string("device set-up failed: ") + caffe_last_error());
+    if (!uniform) setField("phi", ics.values("phi", 1, field("cc")));
+}
+
+Diffusion::~Diffusion() {
+    if (hd_) caffe_diffusion_destroy(hd_);
+}
+
+double Diffusion::solve(double timeStep) {
+    if (caffe_diffusion_solve(hd_, timeStep, &residual_, &iters_, &relres_) != 0)
+        Output::raiseException("Diffusion", "solve", std::string("device solve failed: ") + caffe_last_error());
+    return residual_;
+}
+
+void Diffusion::displayUpdateMessage() {
+    Output::print("Diffusion", "completed iteration.");
+    Output::print("Diffusion", "Krylov iterations : " + std::to_string(iters_));
+    Output::print("Diffusion", "||A x - b||_inf   : " + std::to_string(residual_));
+    Output::printLine();
+}
+
+std::vector<double> Diffusion::field(const std::string& name) const {
+    long n = caffe_diffusion_array(hd_, name.c_str(), nullptr, 0, 0);
+    if (n < 0) Output::raiseException("Diffusion", "field", "unknown field \"" + name + "\"");
+    std::vector<double> out((size_t)n);
+    if (caffe_diffusion_array(hd_, name.c_str(), out.data(), n, 0) < 0)
+        Output::raiseException("Diffusion", "field", std::string("read failed: ") + caffe_last_error());
+    return to_planes(out, vector_components(name));
+}
+
+void Diffusion::setField(const std::string& name, const std::vector<double>& values) {
+    std::vector<double> v = to_interleaved(values, vector_components(name));
+    if (caffe_diffusion_array(hd_, name.c_str(), v.data(), (long)v.size(), 1) < 0)
+        Output::raiseException("Diffusion", "setField", std::string("write failed: ") + caffe_last_error());
+}

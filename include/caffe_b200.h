@@ -167,7 +167,7 @@ int caffe_csr_matvec(int m, int n, const int* row_ptr, const int* col, const dou
  * and ||A x - b||_inf (its return value in the reference).  caffe_diffusion_phase runs one part:
  * "assemble", "solve" (the linear solve into x) or "post" (everything after it).
  * caffe_diffusion_array: "phi", "x" (writable), "b", "A" (N x 7: aP aE aW aN aS aT aB), "phiFaceI/J/K",
- * "phiPatch0".."phiPatch5", "gradPhi" (N x 3); same conventions as caffe_dev_array. */
+ * "phiPatch0".."phiPatch5", "gradPhi", "cc" (cell centroids) (N x 3); same conventions as caffe_dev_array. */
 typedef struct caffe_diffusion caffe_diffusion;
 int caffe_diffusion_create(const double* nodes, int nNodesI, int nNodesJ, int nNodesK, const int* bc_type, const double* ref_val,
                            int time_accurate, double phi0, int method, double rtol, int maxit, int device, caffe_diffusion** out);

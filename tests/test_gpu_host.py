@@ -104,3 +104,59 @@ def test_piso_module_continued_from_restart_files(tmp_path):
     vol = o2.get("vol")
     assert rel_l2(np.array(u2).reshape(3, -1).T.ravel(), o2.get("u")) < FIELD_RTOL
     assert rel_l2(demean(np.array(p2), vol), demean(o2.get("p"), vol)) < FIELD_RTOL
+
+
+def test_coupled_module_run_matches_oracle(tmp_path):
+    """caffeCoupled (the reference's Modules/caffeCoupled.cpp flow) runs a 2-D lid-driven cavity
+    case directory; u and p after the last iteration match the oracle's Coupled restatement on
+    the same nodes (1e-8: the block solves stop at a 1e-12 relative residual on each side)."""
+    from oracle.oracle import OracleCoupled
+    spec = C.config1_cavity2d(n=10)[1].replace(mom_method="bicgstab_jacobi", mom_rtol=1e-12, p_rtol=1e-12, maxit=20000)
+    steps = 6
+    nodes, p, u = _run(tmp_path, "caffeCoupled", spec, (1.0, 1.0, 0.1), (11, 11, 2), steps)
+    o = OracleCoupled(nodes, spec)
+    for _ in range(steps):
+        o.solve(spec.dt)
+    eu = rel_l2(u.reshape(3, -1).T.ravel(), o.get("u"))
+    po = o.get("p")
+    ep = rel_l2(p - p.mean(), po - po.mean())
+    print("caffeCoupled u", eu, "p", ep)
+    assert eu < 1e-8 and ep < 1e-8
+    o.close()
+
+
+def test_diffusion_module_run_matches_oracle(tmp_path):
+    """caffeDiffusion (the reference's Modules/caffeDiffusion.cpp flow) runs the layout of the
+    reference's FlatPlateDiffusion2D example (fixed west 1, other sides 0, empty top and bottom)
+    on a generated mesh; phi and its gradient after the last solve match the oracle's Diffusion
+    restatement (1e-9: the solves stop at a 1e-12 relative residual on each side)."""
+    from oracle.oracle import OracleDiffusion
+    root = tmp_path
+    spec = C.config1_cavity2d(n=4)[1]
+    write_case(str(root), spec, (1.0, 1.0, 0.05), (17, 13, 2), steps=2)
+    types = ("fixed", "fixed", "fixed", "fixed", "empty", "empty")
+    refs = (0.0, 1.0, 0.0, 0.0, 0.0, 0.0)
+    with open(root / "case" / "case.info", "w") as f:
+        f.write("RunControl\n{\n\tterminationCondition iterations\n\tmaxNumberOfIterations 3\n\tfileWriteInterval 1000\n"
+                "\ttimeStep 0.01\n\tmaxSimTime 48\n\tmaxRealTimeHours 48\n}\n\nSolver\n{\n\ttimeAccurate OFF\n}\n\n"
+                "LinearSolvers\n{\n\ttolerance 1e-12\n\tmaxIterations 20000\n}\n\nBoundaries\n{\n")
+        for face, t, v in zip(C.FACES, types, refs):
+            f.write(f"\t{face}\n\t{{\n\t\ttype {t}\n\t\trefValue {v!r}\n\t}}\n")
+        f.write("}\n")
+    with open(root / "case" / "initialConditions.info", "w") as f:
+        f.write("phi\n{\n\ttype uniform\n\tvalue 0\n}\n")
+    subprocess.run([os.path.join(BIN, "hexaMesh")], cwd=root, check=True, capture_output=True)
+    r = subprocess.run([os.path.join(BIN, "caffeDiffusion")], cwd=root, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    nodes = _nodes_from_dat(root / "mesh" / "structuredMesh.dat")
+    n = int(np.prod([d - 1 for d in nodes.shape[:3]]))
+    fields = read_tec360_fields(str(root / "solution" / "testMesh.dat"), n)
+    o = OracleDiffusion(nodes, types, refs, time_accurate=False, phi0=0.0, method="bicgstab_jacobi", rtol=1e-12, maxit=20000)
+    for _ in range(2):
+        o.solve(0.01)
+    ephi = rel_l2(np.array(fields["phi"]), o.get("phi"))
+    grad = np.stack([fields["gradPhi_x"], fields["gradPhi_y"], fields["gradPhi_z"]], axis=1).ravel()
+    eg = rel_l2(grad, o.get("gradPhi"))
+    print("caffeDiffusion phi", ephi, "gradPhi", eg)
+    assert ephi < 1e-9 and eg < 1e-9
+    o.close()

@@ -78,7 +78,8 @@ def test_info_parser_errors_are_reported(tmp_path, host_bins):
 
 
 @pytest.mark.skipif(not os.path.isdir(REF_MODULES), reason="reference sources not present")
-@pytest.mark.parametrize("module", ["caffeSimple.cpp", "caffePiso.cpp", "caffeIbPiso.cpp", "caffeMultiphasePiso.cpp", "hexaMesh.cpp"])
+@pytest.mark.parametrize("module", ["caffeSimple.cpp", "caffePiso.cpp", "caffeIbPiso.cpp", "caffeMultiphasePiso.cpp", "caffeCoupled.cpp",
+                                    "caffeDiffusion.cpp", "hexaMesh.cpp"])
 def test_reference_module_mains_compile_unchanged(tmp_path, host_bins, module):
     """The reference's module mains, read where they lie, compile and link against the host
     layer's headers with no change (the drop-in property of the host interface)."""
