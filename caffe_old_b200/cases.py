@@ -185,12 +185,13 @@ def config4_channel_sphere(dims=(256, 128, 128), seed: int = 0, steps: int = 50)
     return nodes, spec, steps
 
 
-def config5_sphere(dims=(384, 256, 256), steps: int = 500, p_form: str = "learned_mixed"):
-    """Flow over an immersed sphere R=0.25 at (2,2,2) in an 8x4x4 box, Re=300, PISO with
-    3 correctors, dt=2e-3; the same stabilising settings as the channel case."""
+def config5_sphere(dims=(384, 256, 256), steps: int = 500, p_form: str = "learned_mixed", re: float = 300.0):
+    """Flow over an immersed sphere R=0.25 at (2,2,2) in an 8x4x4 box, Re=300 (diameter-based;
+    `re` changes it), PISO with 3 correctors, dt=2e-3; the same stabilising settings as the
+    channel case."""
     nodes = cartesian_nodes(dims, (8.0, 4.0, 4.0))
     bc, ref = channel_bcs(1.0)
-    spec = CaseSpec(kind="ibpiso", bc=bc, ref_vec=ref, rho=1.0, mu=0.5 / 300.0, time_accurate=True,
+    spec = CaseSpec(kind="ibpiso", bc=bc, ref_vec=ref, rho=1.0, mu=0.5 / float(re), time_accurate=True,
                     omega_u=0.7, omega_p=0.3, n_inner=2, n_pcorr=3, convection="upwind",
                     mom_method="bicgstab_jacobi", p_method="bicgstab_jacobi", mom_rtol=1e-8, p_rtol=1e-8,
                     dt=2e-3, ib_radius=0.25, ib_center=(2.0, 2.0, 2.0), p_form=p_form, u_init=(1.0, 0.0, 0.0))

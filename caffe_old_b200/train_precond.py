@@ -1,18 +1,23 @@
 """Train the learned preconditioner on the GPU and write the parameters the package ships
 (caffe_old_b200/data/precond_params.npy).
 
-Training pairs come from the plain FP64 solver's first steps on several seeds of the IB
-channel case (Re ~ U[100, 300]):
+Training pairs come from the first steps on several seeds (Re ~ U[100, 300]) of the IB channel
+case (--case channel) or of the sphere-in-a-box case (--case sphere, the 8x4x4 box of the
+25.2M-cell configuration):
 * the (b, x*) of every pressure-correction solve;
 * residual/correction pairs (b - A x_k, x* - x_k) from plain re-solves truncated after 8, 32
   and 128 iterations;
 * multi-scale synthetic pairs (A e, e).
 
-All pairs live in HBM on one handle, and the network is trained there by the library's
-tensor-core forward and backward passes (Adam, energy-norm loss).
+The steps themselves run with the plain FP64 p' solve (--form fp64) or, where a plain step is
+too slow (a 25M-cell lattice), with the learned + mixed form in pyramid mode (--form levels);
+either way every solve reaches the same 1e-8 FP64 residual, and the truncated re-solves are the
+plain solver's.  All pairs live in HBM on one handle, and the network is trained there by the
+library's tensor-core forward and backward passes (Adam, energy-norm loss).
 
-  python -m caffe_old_b200.train_precond [--dims 256 128 128] [--seeds 1 2 3 4] [--steps-per-seed 4]
-                                         [--random 128] [--train-steps 1500] [--out path]
+  python -m caffe_old_b200.train_precond [--case channel|sphere] [--dims 256 128 128] [--seeds 1 2 3 4]
+                                         [--steps-per-seed 4] [--form fp64|levels] [--random 128]
+                                         [--train-steps 1500] [--out path]
 """
 from __future__ import annotations
 
@@ -30,6 +35,8 @@ from .solver import make_solver
 
 def main(argv=None) -> dict:
     ap = argparse.ArgumentParser()
+    ap.add_argument("--case", default="channel", choices=("channel", "sphere"))
+    ap.add_argument("--form", default="fp64", choices=("fp64", "levels"))
     ap.add_argument("--dims", type=int, nargs=3, default=(256, 128, 128))
     ap.add_argument("--seeds", type=int, nargs="+", default=(11, 12, 13, 14))
     ap.add_argument("--steps-per-seed", type=int, default=4)
@@ -47,8 +54,14 @@ def main(argv=None) -> dict:
     handles = []
     store = None
     for q, seed in enumerate(args.seeds):
-        nodes, spec, _ = C.config4_channel_sphere(dims, seed=seed)
-        s = make_solver(nodes, spec.replace(p_form="fp64"))
+        if args.case == "channel":
+            nodes, spec, _ = C.config4_channel_sphere(dims, seed=seed)
+        else:
+            re = float(np.random.default_rng(seed).uniform(100.0, 300.0))
+            nodes, spec, _ = C.config5_sphere(dims, re=re)
+        s = make_solver(nodes, spec.replace(p_form="fp64" if args.form == "fp64" else "learned_mixed"))
+        if args.form == "levels":
+            P.set_mode(s, "levels")
         cap = args.steps_per_seed * spec.n_inner * spec.n_pcorr * per_solve
         if store is None:
             # the first seed's handle holds every pair and trains; the others hand theirs over
@@ -76,7 +89,7 @@ def main(argv=None) -> dict:
     store.close()
     os.makedirs(os.path.dirname(os.path.abspath(args.out)), exist_ok=True)
     np.save(args.out, params.astype(np.float32))
-    info = {"net_from": args.net_from, "pairs": n, "seeds": list(args.seeds), "dims": list(dims),
+    info = {"case": args.case, "form": args.form, "net_from": args.net_from, "pairs": n, "seeds": list(args.seeds), "dims": list(dims),
             "train_steps": args.train_steps, "batch": args.batch, "lr": args.lr, "pair_generation_s": round(t1 - t0, 1),
             "training_s": round(t2 - t1, 1), "loss_jacobi": before["jacobi"], "loss_levels": before["levels"],
             "loss_network": after, "loss_first_steps": [float(v) for v in hist[:5]],
