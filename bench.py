@@ -322,6 +322,10 @@ def configure_precond(dev, args):
     net_from = args.net_from if args.net_from is not None else int(P.default_info().get("net_from", 1) if not args.params else 1)
     args.net_from = net_from
     P.set_options(dev, args.inner, net_from, args.restart)
+    # the network runs only on levels whose level channel it was trained on
+    net_to = args.net_to if args.net_to is not None else (P.trained_last_level() if not args.params else None)
+    P.set_net_levels(dev, net_from, net_to)
+    args.net_to = net_to
     return params
 
 
@@ -479,6 +483,8 @@ def run_b200(args, world, rank, local, pg):
             "data": "synthetic (seeded mesh and case, no dataset)",
             "config": {"workload": label, "cells": N, "p_form": args.p_form,
                        "precond": args.precond if learned else None, "inner": method,
+                       "net_levels": [args.net_from, args.net_to] if learned and args.precond == "network" else None,
+                       "restart": args.restart if method == "fgmres" else None,
                        "parallelism": f"replicas x{world}",
                        "l2": f"inputs larger than L2: working set ~{working_set / 2**30:.1f} GiB > 126 MB"},
             "p_solve_ms": p_ms / args.steps, "momentum_solve_ms": mom_ms / args.steps,
@@ -511,6 +517,8 @@ def main():
     ap.add_argument("--inner", default="auto", choices=("auto", "fcg", "bicgstab", "fgmres"))
     ap.add_argument("--net-from", type=int, default=None, help="first pyramid level that runs the network "
                     "(default: the one the shipped parameters were trained for)")
+    ap.add_argument("--net-to", type=int, default=None, help="last pyramid level that runs the network "
+                    "(default: the coarsest level the shipped parameters were trained on)")
     ap.add_argument("--restart", type=int, default=40)
     ap.add_argument("--params", default=None, help="network parameters (.npy); default: the shipped ones")
     ap.add_argument("--size", type=int, default=None)

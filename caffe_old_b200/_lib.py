@@ -72,6 +72,7 @@ EXPORTS = (
     "caffe_coupled_system", "caffe_coupled_array",
     "caffe_precond_param_count", "caffe_precond_net_apply", "caffe_precond_net_grad",
     "caffe_dev_set_precond", "caffe_dev_get_precond", "caffe_dev_set_precond_mode", "caffe_dev_set_precond_options",
+    "caffe_dev_set_precond_net_levels",
     "caffe_dev_record_pairs", "caffe_dev_pair_count", "caffe_dev_add_pairs", "caffe_dev_add_random_pairs", "caffe_dev_copy_pairs", "caffe_dev_train_precond",
     "caffe_dev_eval_precond", "caffe_launch_count",
 )
@@ -125,6 +126,7 @@ def lib():
     L.caffe_dev_get_precond.argtypes = [vp, vp]
     L.caffe_dev_set_precond_mode.argtypes = [vp, ci]
     L.caffe_dev_set_precond_options.argtypes = [vp, ci, ci, ci]
+    L.caffe_dev_set_precond_net_levels.argtypes = [vp, ci, ci]
     L.caffe_dev_record_pairs.argtypes = [vp, ci, ci]
     L.caffe_dev_pair_count.argtypes = [vp]
     L.caffe_dev_add_pairs.argtypes = [vp, vp, vp, ci]

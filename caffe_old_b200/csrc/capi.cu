@@ -904,6 +904,17 @@ int caffe_dev_set_precond_options(caffe_dev* h, int inner_method, int net_from_l
     return 0;
 }
 
+int caffe_dev_set_precond_net_levels(caffe_dev* h, int first_level, int last_level) {
+    g_err.clear();
+    if (!h) { set_error("handle is NULL"); return 1; }
+    if (first_level < 1 || (last_level >= 0 && last_level < first_level)) { set_error("invalid network levels"); return 1; }
+    CB_CUDA(cudaSetDevice(h->device));
+    if (h->ensure_learned()) return 1;
+    h->lw.netFrom = first_level;
+    h->lw.netTo = last_level < 0 ? (1 << 20) : last_level;
+    return 0;
+}
+
 int caffe_dev_record_pairs(caffe_dev* h, int capacity, int snapshots) {
     g_err.clear();
     if (!h || capacity < 0 || snapshots < 0 || snapshots > 8) { set_error("invalid arguments"); return 1; }

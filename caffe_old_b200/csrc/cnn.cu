@@ -114,6 +114,23 @@ __device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t phase) {
     return ok != 0;
 }
 
+// the same test, letting the hardware suspend the thread for up to `ns` nanoseconds while the
+// phase is incomplete (it resumes when the phase completes), so that waiting warps do not take
+// issue slots from the producer and MMA threads
+__device__ __forceinline__ bool mbar_try_sleep(uint32_t bar, uint32_t phase, uint32_t ns) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred P1;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2, %3;\n\t"
+        "selp.b32 %0, 1, 0, P1;\n\t}\n"
+        : "=r"(ok)
+        : "r"(bar), "r"(phase), "r"(ns)
+        : "memory");
+    return ok != 0;
+}
+constexpr long long SLEEP_WAIT_LIMIT = 1ll << 19;   // rounds of at most SLEEP_NS each: about a second at most
+constexpr uint32_t SLEEP_NS = 2000;
+
 __device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t phase) {
     for (long long t = 0; t < WAIT_LIMIT; ++t)
         if (mbar_try(bar, phase)) return true;
@@ -239,12 +256,12 @@ __global__ void __launch_bounds__(CONV_THREADS) conv3d_tc_kernel(const __grid_co
     asm volatile("tcgen05.fence::after_thread_sync;");
     const uint32_t tmem = tmem_base_sh;
 
-    // bounded wait that also gives up once another role has failed
+    // bounded wait that also gives up once another role has failed (checked every 16 rounds)
     auto wait = [&](uint64_t* b, uint32_t parity) -> bool {
         const uint32_t a = smem_u32(b);
-        for (long long t = 0; t < WAIT_LIMIT; ++t) {
-            if (mbar_try(a, parity)) return true;
-            if (fail_sh) return false;
+        for (long long t = 0; t < SLEEP_WAIT_LIMIT; ++t) {
+            if (mbar_try_sleep(a, parity, SLEEP_NS)) return true;
+            if ((t & 15) == 15 && fail_sh) return false;
         }
         fail_sh = 1;
         return false;
@@ -282,10 +299,10 @@ __global__ void __launch_bounds__(CONV_THREADS) conv3d_tc_kernel(const __grid_co
             if (!ok) break;
             asm volatile("tcgen05.fence::after_thread_sync;");
             int t = 0;
-#pragma unroll 1
+#pragma unroll
             for (int dk = 0; dk < 3; ++dk) {
                 const int sl = (o + dk) % NPL;
-#pragma unroll 1
+#pragma unroll
                 for (int dj = 0; dj < 3; ++dj)
 #pragma unroll
                     for (int di = 0; di < 3; ++di, ++t) {

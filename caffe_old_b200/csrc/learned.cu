@@ -17,7 +17,8 @@
 // (the second evaluation negates only the residual channel): a network with biases and
 // constant input channels has a part that does not depend on the residual, which would add
 // the same vector to every preconditioned direction; the odd form gives M(0) = 0 and
-// M(-r) = -M(r) exactly.  Levels finer than the first network level (netFrom) use the
+// M(-r) = -M(r) exactly.  Levels finer than the first network level (netFrom) or coarser than
+// the last one (netTo) use the
 // identity.  Two reference forms use the same code: JACOBI (no levels: M = D^-1, the method
 // without the network) and LEVELS (y_l = u_l / s, the pyramid with an identity in place of
 // the network).
@@ -1084,7 +1085,7 @@ Dims3 dims_of(const Level& l) { return Dims3{l.n[0], l.n[1], l.n[2]}; }
 // (result in lev[1].w).  Every kernel is a no-op while S->done is set.
 int apply_levels(LearnedWork& lw, const float* rfine, const uint8_t* status, int mode, Scal* S, cudaStream_t st) {
     if (mode == NET_MODE_JACOBI || lw.nLev < 2) return 0;
-    auto netAt = [&](int l) { return mode == NET_MODE_NETWORK && l >= lw.netFrom; };
+    auto netAt = [&](int l) { return mode == NET_MODE_NETWORK && l >= lw.netFrom && l <= lw.netTo; };
     for (int l = 1; l < lw.nLev; ++l) {
         Level& c = lw.lev[l];
         const Level& f = lw.lev[l - 1];
@@ -1696,7 +1697,7 @@ int learned_train(LearnedWork& lw, const OpSym& A, const uint8_t* status, const 
                 const Level& f = lw.lev[l - 1];
                 restrict_kernel<<<restrict_grid(dims_of(c)), 256, 0, st>>>(dims_of(f), dims_of(c), l == 1 ? lw.r : f.u, nullptr, nullptr, 1.f,
                                                                            c.u, c.w, c.gain, nullptr, nullptr, nullptr, 0.f, S);
-                if (l >= lw.netFrom) {
+                if (l >= lw.netFrom && l <= lw.netTo) {
                     // y = (net(x) - net(-x)) / 2: the two evaluations get dL/dy / 2 and -dL/dy / 2
                     half_split_kernel<<<grid_for(c.N, 256), 256, 0, st>>>(c.N, c.w, c.w2);
                     if (net_backward(c.net, c.w, st) || net_backward(c.netNeg, c.w2, st)) return 1;

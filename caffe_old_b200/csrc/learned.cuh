@@ -60,6 +60,7 @@ struct LearnedWork {
     bool masksReady = false;
     bool haveParams = false;
     int netFrom = 1;             // first level that runs the network (finer levels: identity)
+    int netTo = 1 << 20;         // last level that runs the network (coarser levels: identity)
     int inner = LEARN_INNER_AUTO;
     int restart = 40;            // FGMRES cycle length (one cycle per FP64 refinement pass)
     // FGMRES basis (restart + 1 planes) and preconditioned vectors (restart planes), one

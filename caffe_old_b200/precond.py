@@ -81,6 +81,30 @@ def default_info() -> dict:
     return {}
 
 
+def pyramid_dims(dims) -> list:
+    """The lattices of the learned preconditioner's level pyramid for a cell lattice `dims`
+    (the rule of the device's learned_alloc: halve every direction longer than one cell until
+    at most 64 cells remain, at most 12 levels)."""
+    out = [[int(v) for v in dims]]
+    while len(out) < 12:
+        f = out[-1]
+        if f[0] * f[1] * f[2] <= 64 or f == [1, 1, 1]:
+            break
+        out.append([(v + 1) // 2 if v > 1 else 1 for v in f])
+    return out
+
+
+def trained_last_level() -> int | None:
+    """The coarsest pyramid level the shipped parameters were trained on (the network has never
+    seen the level channel of a coarser one), or None when unknown."""
+    info = default_info()
+    if "net_to" in info:
+        return int(info["net_to"])
+    if "dims" in info:
+        return len(pyramid_dims(info["dims"])) - 1
+    return None
+
+
 def _check(rc: int, what: str) -> None:
     if rc != 0:
         raise CaffeError(f"{what}: " + last_error())
@@ -111,6 +135,13 @@ def set_options(solver, inner: str = "auto", net_from_level: int = 1, restart: i
     network (finer levels use the identity) and the FGMRES cycle length."""
     _check(lib().caffe_dev_set_precond_options(solver._h, INNER[inner], int(net_from_level), int(restart)),
            "set_precond_options")
+
+
+def set_net_levels(solver, first_level: int = 1, last_level: int | None = None) -> None:
+    """The pyramid levels that run the network (first_level .. last_level; None: down to the
+    coarsest); the others use the identity."""
+    _check(lib().caffe_dev_set_precond_net_levels(solver._h, int(first_level), -1 if last_level is None else int(last_level)),
+           "set_precond_net_levels")
 
 
 def record_pairs(solver, capacity: int, snapshots: int = 0) -> None:

@@ -82,6 +82,7 @@ def main(argv=None) -> dict:
     n = P.pair_count(store)
     t1 = time.time()
     P.set_options(store, "auto", args.net_from)
+    net_to = len(P.pyramid_dims(dims)) - 1
     before = {m: float(P.evaluate(store, m).mean()) for m in ("jacobi", "levels")}
     params, hist = P.train(store, P.identity_params(0), steps=args.train_steps, batch=args.batch, lr=args.lr, seed=1)
     after = float(P.evaluate(store, "network").mean())
@@ -89,7 +90,7 @@ def main(argv=None) -> dict:
     store.close()
     os.makedirs(os.path.dirname(os.path.abspath(args.out)), exist_ok=True)
     np.save(args.out, params.astype(np.float32))
-    info = {"case": args.case, "form": args.form, "net_from": args.net_from, "pairs": n, "seeds": list(args.seeds), "dims": list(dims),
+    info = {"case": args.case, "form": args.form, "net_from": args.net_from, "net_to": net_to, "pairs": n, "seeds": list(args.seeds), "dims": list(dims),
             "train_steps": args.train_steps, "batch": args.batch, "lr": args.lr, "pair_generation_s": round(t1 - t0, 1),
             "training_s": round(t2 - t1, 1), "loss_jacobi": before["jacobi"], "loss_levels": before["levels"],
             "loss_network": after, "loss_first_steps": [float(v) for v in hist[:5]],

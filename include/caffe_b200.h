@@ -239,6 +239,9 @@ int caffe_dev_set_precond_mode(caffe_dev* h, int mode);
  * identity.  restart: FGMRES cycle length, 1..64 (one cycle per FP64 refinement pass; it
  * cannot grow after the handle's first FGMRES solve). */
 int caffe_dev_set_precond_options(caffe_dev* h, int inner_method, int net_from_level, int restart);
+/* The pyramid levels that run the network: first_level .. last_level (last_level < 0: every
+ * level from first_level down to the coarsest); the others use the identity. */
+int caffe_dev_set_precond_net_levels(caffe_dev* h, int first_level, int last_level);
 /* Training pairs (b, x) with A x = b, kept on the device in FP32.  record_pairs(capacity > 0)
  * stores the right-hand side and solution of every following p' solve until `capacity` pairs
  * are held, plus `snapshots` residual/correction pairs (b - A x_k, x - x_k) per solve from
