@@ -53,6 +53,12 @@
 #include <string>
 #include <vector>
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <array>
+#include <mutex>
+#include <utility>
+
 #include "../../include/caffe_b200.h"
 #include "common.cuh"
 #include "cnn.cuh"
@@ -346,6 +352,212 @@ __global__ void __launch_bounds__(256) restrict_kernel(Dims3 fd, Dims3 cd, const
             }
         }
     }
+}
+
+// ---------------------------------------------------------------- restriction to level 1, TMA-staged
+// The same restriction from the cell lattice (v = fin * invD on active cells) as restrict_kernel,
+// by persistent CTAs (one per SM) that walk the coarse tiles and stream each tile's fine box in
+// by TMA while the previous tile is reduced: two stages, each holding the tile's fin, invD (FP32)
+// and status (byte) boxes.  TMA wants the innermost start coordinate on a 16-byte boundary, so the
+// float boxes start at fine i = 2 I0 - 4 (72 cells) and the status box at 2 I0 - 16 (96 bytes);
+// boxes reaching outside the lattice are zero-filled, and zero fin contributes nothing.
+constexpr int RT_BX = 72, RT_BXS = 96;
+constexpr int RT_F_BYTES = RT_BX * RFJ * RFK * 4;            // 28800
+constexpr int RT_S_BYTES = RT_BXS * RFJ * RFK;               // 9600
+constexpr int RT_STAGE_BYTES = 2 * RT_F_BYTES + RT_S_BYTES;  // 67200
+constexpr int RT_THREADS = 512;
+constexpr long long RT_WAIT_LIMIT = 1ll << 19;               // rounds of at most 2 us each
+
+__device__ __forceinline__ uint32_t rt_smem(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ bool rt_try(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred P1;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2, %3;\n\t"
+        "selp.b32 %0, 1, 0, P1;\n\t}\n"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity), "r"(2000u)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ bool rt_wait(uint32_t bar, uint32_t parity) {
+    for (long long t = 0; t < RT_WAIT_LIMIT; ++t)
+        if (rt_try(bar, parity)) return true;
+    return false;
+}
+__device__ __forceinline__ void rt_load3d(uint32_t dst, const CUtensorMap* map, int x, int y, int z, uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+        :
+        : "r"(dst), "l"((uint64_t)map), "r"(x), "r"(y), "r"(z), "r"(bar)
+        : "memory");
+}
+
+struct RestrictMaps {
+    CUtensorMap fin, invD, st;   // this GPU's own buffers (no cluster multicast)
+};
+
+__global__ void __launch_bounds__(RT_THREADS) restrict_tma_kernel(const __grid_constant__ RestrictMaps maps, Dims3 fd, Dims3 cd, int hasSt,
+                                                                  float scale, float* out, int* err, const Scal* S) {
+    if (S && S->done) return;
+    extern __shared__ __align__(1024) unsigned char rt_raw[];
+    unsigned char* smem = (unsigned char*)(((uintptr_t)rt_raw + 1023) & ~(uintptr_t)1023);
+    __shared__ __align__(8) uint64_t full[2];
+    __shared__ float t1[RFK][RFJ][RCI];
+    __shared__ float t2[RFK][RCJ][RCI];
+    __shared__ float wI[RCI][4], wJ[RCJ][4], wK[RCK][4];
+    const int tI = (cd.n0 + RCI - 1) / RCI, tJ = (cd.n1 + RCJ - 1) / RCJ, tK = (cd.n2 + RCK - 1) / RCK;
+    const int T = tI * tJ * tK;
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(rt_smem(&full[0])));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(rt_smem(&full[1])));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    int issued[2] = {0, 0};   // thread 0: loads issued per stage
+    auto issue = [&](int tile, int stage) {
+        const int ti = tile % tI, tj = (tile / tI) % tJ, tk = tile / (tI * tJ);
+        const int x = 2 * ti * RCI - 4, y = 2 * tj * RCJ - 1, z = 2 * tk * RCK - 1;
+        unsigned char* b = smem + (size_t)stage * RT_STAGE_BYTES;
+        const uint32_t bar = rt_smem(&full[stage]);
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // after the generic writes of this stage's last tile
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
+                     "r"((uint32_t)(hasSt ? RT_STAGE_BYTES : 2 * RT_F_BYTES)) : "memory");
+        rt_load3d(rt_smem(b), &maps.fin, x, y, z, bar);
+        rt_load3d(rt_smem(b + RT_F_BYTES), &maps.invD, x, y, z, bar);
+        if (hasSt) rt_load3d(rt_smem(b + 2 * RT_F_BYTES), &maps.st, x - 12, y, z, bar);
+        ++issued[stage];
+    };
+    if (threadIdx.x == 0 && (int)blockIdx.x < T) issue(blockIdx.x, 0);
+    bool failed = false;
+    int n = 0;
+    for (int tile = blockIdx.x; tile < T; tile += gridDim.x, ++n) {
+        const int stage = n & 1;
+        if (threadIdx.x == 0 && tile + (int)gridDim.x < T) issue(tile + gridDim.x, stage ^ 1);
+        const int ti = tile % tI, tj = (tile / tI) % tJ, tk = tile / (tI * tJ);
+        const int I0 = ti * RCI, J0 = tj * RCJ, K0 = tk * RCK;
+        if (threadIdx.x < 4 * RCI) {
+            int ci = threadIdx.x >> 2, m = threadIdx.x & 3, I = I0 + ci;
+            wI[ci][m] = rweight_in(2 * I - 1 + m, fd.n0, I, cd.n0);
+        } else if (threadIdx.x < 4 * RCI + 4 * RCJ) {
+            int u = threadIdx.x - 4 * RCI, cj = u >> 2, m = u & 3, J = J0 + cj;
+            wJ[cj][m] = rweight_in(2 * J - 1 + m, fd.n1, J, cd.n1);
+        } else if (threadIdx.x < 4 * RCI + 4 * RCJ + 4 * RCK) {
+            int u = threadIdx.x - 4 * RCI - 4 * RCJ, ck = u >> 2, m = u & 3, K = K0 + ck;
+            wK[ck][m] = rweight_in(2 * K - 1 + m, fd.n2, K, cd.n2);
+        }
+        const bool ok = rt_wait(rt_smem(&full[stage]), (uint32_t)((n >> 1) & 1));
+        if (__syncthreads_or(ok ? 0 : 1)) { failed = true; break; }
+        float* sf = reinterpret_cast<float*>(smem + (size_t)stage * RT_STAGE_BYTES);
+        const float* sd = sf + RT_F_BYTES / 4;
+        const unsigned char* ss = smem + (size_t)stage * RT_STAGE_BYTES + 2 * RT_F_BYTES;
+        // v = fin * invD on active cells, in place, for the 66 columns the tile draws on (3 .. 68)
+        for (int e = threadIdx.x; e < RFK * RFJ * RFI; e += RT_THREADS) {
+            const int li = e % RFI, row = e / RFI;
+            const int o = row * RT_BX + 3 + li;
+            const bool act = !hasSt || ss[row * RT_BXS + 15 + li] == ST_ACTIVE;
+            sf[o] = act ? sf[o] * sd[o] : 0.f;
+        }
+        __syncthreads();
+        for (int u = threadIdx.x; u < RFK * RFJ * RCI; u += RT_THREADS) {
+            const int ci = u % RCI, row = u / RCI;
+            const float* v = sf + row * RT_BX + 3 + 2 * ci;
+            t1[row / RFJ][row % RFJ][ci] = wI[ci][0] * v[0] + wI[ci][1] * v[1] + wI[ci][2] * v[2] + wI[ci][3] * v[3];
+        }
+        __syncthreads();
+        for (int u = threadIdx.x; u < RFK * RCJ * RCI; u += RT_THREADS) {
+            const int ci = u % RCI, cj = (u / RCI) % RCJ, lk = u / (RCI * RCJ);
+            t2[lk][cj][ci] = wJ[cj][0] * t1[lk][2 * cj][ci] + wJ[cj][1] * t1[lk][2 * cj + 1][ci] + wJ[cj][2] * t1[lk][2 * cj + 2][ci] +
+                             wJ[cj][3] * t1[lk][2 * cj + 3][ci];
+        }
+        __syncthreads();
+        for (int u = threadIdx.x; u < RCK * RCJ * RCI; u += RT_THREADS) {
+            const int ci = u % RCI, cj = (u / RCI) % RCJ, ck = u / (RCI * RCJ);
+            const int I = I0 + ci, J = J0 + cj, K = K0 + ck;
+            if (I >= cd.n0 || J >= cd.n1 || K >= cd.n2) continue;
+            const float acc = wK[ck][0] * t2[2 * ck][cj][ci] + wK[ck][1] * t2[2 * ck + 1][cj][ci] + wK[ck][2] * t2[2 * ck + 2][cj][ci] +
+                              wK[ck][3] * t2[2 * ck + 3][cj][ci];
+            out[((unsigned)K * (unsigned)cd.n1 + (unsigned)J) * (unsigned)cd.n0 + (unsigned)I] = acc * scale;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        if (failed) atomicExch(err, 1);
+        // every load issued lands before the shared memory is released
+        for (int q = 0; q < 2; ++q)
+            if (issued[q] > 0) rt_wait(rt_smem(&full[q]), (uint32_t)((issued[q] - 1) & 1));
+    }
+    __syncthreads();
+}
+
+// tensor maps of the TMA restriction's inputs, kept per (buffer, lattice, element size)
+PFN_cuTensorMapEncodeTiled_v12000 rt_encode_fn() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess && q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    return fn;
+}
+const CUtensorMap* rt_map(const void* base, const Dims3& fd, int esize) {
+    static std::vector<std::pair<std::array<long long, 5>, CUtensorMap>> cache;
+    static std::mutex lock;
+    std::lock_guard<std::mutex> guard(lock);
+    const std::array<long long, 5> key = {(long long)(uintptr_t)base, fd.n0, fd.n1, fd.n2, esize};
+    for (auto& e : cache)
+        if (e.first == key) return &e.second;
+    PFN_cuTensorMapEncodeTiled_v12000 fn = rt_encode_fn();
+    if (!fn) return nullptr;
+    CUtensorMap m;
+    cuuint64_t dims[3] = {(cuuint64_t)fd.n0, (cuuint64_t)fd.n1, (cuuint64_t)fd.n2};
+    cuuint64_t strides[2] = {(cuuint64_t)fd.n0 * esize, (cuuint64_t)fd.n0 * fd.n1 * esize};
+    cuuint32_t box[3] = {(cuuint32_t)(esize == 4 ? RT_BX : RT_BXS), (cuuint32_t)RFJ, (cuuint32_t)RFK};
+    cuuint32_t estr[3] = {1, 1, 1};
+    CUresult r = fn(&m, esize == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<void*>(base), dims, strides,
+                    box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return nullptr;
+    cache.emplace_back(key, m);
+    return &cache.back().second;
+}
+
+// whether the fine lattice and buffers meet TMA's rules for the staged restriction: rows of 16-byte
+// multiples (status rows of bytes too) and 16-byte aligned bases
+bool restrict_tma_usable(const Dims3& fd, const float* fin, const float* invD, const uint8_t* st) {
+    auto al = [](const void* p) { return ((uintptr_t)p & 15u) == 0; };
+    if (fd.n0 % 4 != 0 || !al(fin) || !al(invD)) return false;
+    if (st && (fd.n0 % 16 != 0 || !al(st))) return false;
+    return rt_encode_fn() != nullptr;
+}
+
+int launch_restrict_tma(const Dims3& fd, const Dims3& cd, const float* fin, const float* invD, const uint8_t* st, float scale, float* out,
+                        int* err, const Scal* S, cudaStream_t stream) {
+    RestrictMaps maps;
+    std::memset(&maps, 0, sizeof(maps));
+    const CUtensorMap* mf = rt_map(fin, fd, 4);
+    const CUtensorMap* md = rt_map(invD, fd, 4);
+    const CUtensorMap* ms = st ? rt_map(st, fd, 1) : nullptr;
+    if (!mf || !md || (st && !ms)) { set_error("tensor map encoding failed for the staged restriction"); return 1; }
+    maps.fin = *mf;
+    maps.invD = *md;
+    if (ms) maps.st = *ms;
+    const size_t smem = 1024 + 2 * (size_t)RT_STAGE_BYTES;
+    static bool attr = false;
+    static int nsm = 0;
+    if (!attr) {
+        CB_CUDA(cudaFuncSetAttribute(restrict_tma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        attr = true;
+    }
+    const long long T = (long long)((cd.n0 + RCI - 1) / RCI) * ((cd.n1 + RCJ - 1) / RCJ) * ((cd.n2 + RCK - 1) / RCK);
+    const int grid = (int)std::min<long long>(T, nsm > 0 ? nsm : 148);
+    restrict_tma_kernel<<<grid, RT_THREADS, smem, stream>>>(maps, fd, cd, st ? 1 : 0, scale, out, err, S);
+    CB_CHECK_LAUNCH();
+    return 0;
 }
 
 inline dim3 restrict_grid(const Dims3& cd) {
@@ -1089,6 +1301,10 @@ int apply_levels(LearnedWork& lw, const float* rfine, const uint8_t* status, int
     for (int l = 1; l < lw.nLev; ++l) {
         Level& c = lw.lev[l];
         const Level& f = lw.lev[l - 1];
+        if (l == 1 && !netAt(1) && lw.rtErr && restrict_tma_usable(dims_of(f), rfine, lw.invD, status)) {
+            if (launch_restrict_tma(dims_of(f), dims_of(c), rfine, lw.invD, status, c.rscale, c.u, lw.rtErr, S, st)) return 1;
+            continue;
+        }
         restrict_kernel<<<restrict_grid(dims_of(c)), 256, 0, st>>>(dims_of(f), dims_of(c), l == 1 ? rfine : f.u, l == 1 ? lw.invD : nullptr,
                                                                    l == 1 ? status : nullptr, c.rscale, c.u, nullptr, 0.f,
                                                                    netAt(l) ? c.net.act[0] : nullptr, netAt(l) ? c.netNeg.act[0] : nullptr,
@@ -1156,6 +1372,7 @@ int learned_alloc(LearnedWork& lw, const Lat& L, void* (*alloc)(size_t, void*), 
     lw.part = static_cast<double*>(alloc(sizeof(double) * 4 * MAXP, ctx));
     lw.scal = alloc(sizeof(Scal), ctx);
     lw.mean = static_cast<double*>(alloc(sizeof(double) * 2, ctx));
+    lw.rtErr = static_cast<int*>(alloc(sizeof(int) * 4, ctx));
     bool ok = lw.r && lw.z && lw.e && lw.p[0] && lw.p[1] && lw.q[0] && lw.q[1] && lw.t && lw.rh && lw.invD && lw.part && lw.scal && lw.mean;
     for (int q = 0; q < 4; ++q) ok = ok && lw.A[q];
     if (!ok) { set_error("learned-solver allocation failed"); return 1; }
@@ -1413,7 +1630,10 @@ int learned_solve(LearnedWork& lw, const OpSym& A, const uint8_t* status, const 
     publish_kernel<<<1, 32, 0, st>>>(S, out);
     CB_CHECK_LAUNCH();
     CB_CUDA(cudaMemcpyAsync(lw.hostScal, S, sizeof(Scal), cudaMemcpyDeviceToHost, st));
+    int rtErr = 0;
+    if (lw.rtErr) CB_CUDA(cudaMemcpyAsync(&rtErr, lw.rtErr, sizeof(int), cudaMemcpyDeviceToHost, st));
     CB_CUDA(cudaStreamSynchronize(st));
+    if (rtErr) { set_error("a TMA load of the staged restriction did not complete"); return 1; }
     lw.lastIters = static_cast<Scal*>(lw.hostScal)->iters;
     lw.lastOuter = static_cast<Scal*>(lw.hostScal)->outer;
     return 0;

@@ -73,6 +73,7 @@ struct LearnedWork {
     void* (*alloc)(size_t, void*) = nullptr;
     void* allocCtx = nullptr;
     int lastIters = 0, lastOuter = 0;
+    int* rtErr = nullptr;        // set by the TMA-staged restriction when a wait ran out
 };
 
 int learned_alloc(LearnedWork& lw, const Lat& L, void* (*alloc)(size_t, void*), void* ctx);
