@@ -124,6 +124,37 @@ __device__ __forceinline__ void totals(const double* part, int nblk, int K, doub
     __syncthreads();
 }
 
+// the same totals read past L1 (the partials were written by other blocks of the running kernel)
+__device__ __forceinline__ void totals_cg(const double* part, int nblk, int K, double* out) {
+    __shared__ double sm[4][LB];
+    for (int q = 0; q < K; ++q) {
+        double t = 0.;
+        for (int b = threadIdx.x; b < nblk; b += blockDim.x) t += __ldcg(part + (size_t)b * 4 + q);
+        sm[q][threadIdx.x] = t;
+    }
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s)
+            for (int q = 0; q < K; ++q) sm[q][threadIdx.x] += sm[q][threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int q = 0; q < K; ++q) out[q] = sm[q][0];
+    __syncthreads();
+}
+
+// after block_sums: true in every thread of the block that finished last (its partial and all
+// the others' are then in memory); that block resets the counter for the next kernel
+__device__ __forceinline__ bool last_block(unsigned* ctr) {
+    __shared__ int amLast;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) amLast = atomicAdd(ctr, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (amLast) __threadfence();
+    return amLast != 0;
+}
+
 inline int nblocks(long long N) {
     long long b = (N + LB - 1) / LB;
     return (int)(b < MAXP ? b : MAXP);
@@ -818,9 +849,33 @@ __global__ void bs_start_finish(const double* part, int nblk, Scal* S, double et
         S->done = !(t[0] > 0.);
     }
 }
+// finishing steps of the flexible BiCGStab reductions (in a one-block kernel, or in the block
+// of the producing kernel that finishes last)
+__device__ __forceinline__ void fin_scale(const double* t, Scal* S) {
+    double sc = S->nact > 0. ? sqrt(t[0] / S->nact) : 1.;
+    S->s = sc > 0. ? sc : 1.;
+}
+__device__ __forceinline__ void fin_alpha(const double* t, Scal* S) {
+    S->rv = t[0];
+    if (t[0] != 0. && t[0] == t[0]) S->alpha = S->rho / t[0];
+    else { S->alpha = 0.; S->done = 1; }
+}
+__device__ __forceinline__ void fin_omega(const double* t, Scal* S) {
+    S->ts = t[0]; S->tt = t[1];
+    S->omega = t[1] > 0. ? t[0] / t[1] : 0.;
+}
+__device__ __forceinline__ void fin_update(const double* t, Scal* S, int max_iters) {
+    S->rr = t[0];
+    S->iters += 1;
+    double rho_new = t[1];
+    bool breakdown = !(S->omega != 0.) || !(S->rho != 0.) || t[1] != t[1];
+    S->beta = breakdown ? 0. : (rho_new / S->rho) * (S->alpha / S->omega);
+    S->rho = rho_new;
+    if (t[0] <= S->tin2 || S->iters >= max_iters || t[0] != t[0] || breakdown) S->done = 1;
+}
 // p = r + beta (p - omega v); partial sum of (D^-1 p)^2 over active cells (scale of M(p))
 __global__ void __launch_bounds__(LB) bs_dir_kernel(long long N, const float* r, const float* v, const float* invD, const uint8_t* st,
-                                                    float* p, double* part, const Scal* S) {
+                                                    float* p, double* part, Scal* S, unsigned* ctr) {
     if (S->done) return;
     const float be = (float)S->beta, om = (float)S->omega;
     const long long T = (long long)gridDim.x * LB, t0 = blockIdx.x * (long long)LB + threadIdx.x, NQ = N >> 2;
@@ -842,15 +897,17 @@ __global__ void __launch_bounds__(LB) bs_dir_kernel(long long N, const float* r,
         if (is_active(st, c)) { double u = (double)__ldg(invD + c) * pv; a[0] += u * u; }
     }
     block_sums(a, 1, part);
+    if (ctr && last_block(ctr)) {
+        double t[1];
+        totals_cg(part, gridDim.x, 1, t);
+        if (threadIdx.x == 0) { fin_scale(t, S); *ctr = 0u; }
+    }
 }
 __global__ void scale_finish(const double* part, int nblk, Scal* S) {
     if (S->done) return;
     double t[1];
     totals(part, nblk, 1, t);
-    if (threadIdx.x == 0) {
-        double sc = S->nact > 0. ? sqrt(t[0] / S->nact) : 1.;
-        S->s = sc > 0. ? sc : 1.;
-    }
+    if (threadIdx.x == 0) fin_scale(t, S);
 }
 // y = M(x) on the cell lattice: D^-1 x + P w_1 on active cells, D^-1 x on ghost rows, 0 on inactive cells
 __global__ void __launch_bounds__(LB) bs_z_kernel(long long N, Dims3 fd, Dims3 cd, const float* x, const float* invD, const uint8_t* st,
@@ -912,7 +969,7 @@ __device__ __forceinline__ void spmv4(const OpSymF32& A, const float* x, long lo
 // out = A x; partial (a1, out), or with b2: (b2, out) and (out, out)
 template <bool V4>
 __global__ void __launch_bounds__(LB) bs_spmv_kernel(OpSymF32 A, long long N, const float* x, float* out, const float* a1, const float* b2,
-                                                     double* part, const Scal* S) {
+                                                     double* part, Scal* S, unsigned* ctr) {
     if (S->done) return;
     double a[2] = {0., 0.};
     long long c0 = 0;
@@ -943,20 +1000,19 @@ __global__ void __launch_bounds__(LB) bs_spmv_kernel(OpSymF32 A, long long N, co
         else a[0] += (double)a1[c] * y;
     }
     block_sums(a, b2 ? 2 : 1, part);
-}
-__global__ void bs_alpha_finish(const double* part, int nblk, Scal* S) {
-    if (S->done) return;
-    double t[1];
-    totals(part, nblk, 1, t);
-    if (threadIdx.x == 0) {
-        S->rv = t[0];
-        if (t[0] != 0. && t[0] == t[0]) S->alpha = S->rho / t[0];
-        else { S->alpha = 0.; S->done = 1; }
+    if (ctr && last_block(ctr)) {
+        double t[2];
+        totals_cg(part, gridDim.x, b2 ? 2 : 1, t);
+        if (threadIdx.x == 0) {
+            if (b2) fin_omega(t, S);
+            else fin_alpha(t, S);
+            *ctr = 0u;
+        }
     }
 }
 // s = r - alpha v; partial sum of (D^-1 s)^2 over active cells
 __global__ void __launch_bounds__(LB) bs_s_kernel(long long N, const float* r, const float* v, const float* invD, const uint8_t* st, float* s,
-                                                  double* part, const Scal* S) {
+                                                  double* part, Scal* S, unsigned* ctr) {
     if (S->done) return;
     const float al = (float)S->alpha;
     const long long T = (long long)gridDim.x * LB, t0 = blockIdx.x * (long long)LB + threadIdx.x, NQ = N >> 2;
@@ -978,19 +1034,15 @@ __global__ void __launch_bounds__(LB) bs_s_kernel(long long N, const float* r, c
         if (is_active(st, c)) { double u = (double)__ldg(invD + c) * sv; a[0] += u * u; }
     }
     block_sums(a, 1, part);
-}
-__global__ void bs_omega_finish(const double* part, int nblk, Scal* S) {
-    if (S->done) return;
-    double t[2];
-    totals(part, nblk, 2, t);
-    if (threadIdx.x == 0) {
-        S->ts = t[0]; S->tt = t[1];
-        S->omega = t[1] > 0. ? t[0] / t[1] : 0.;
+    if (ctr && last_block(ctr)) {
+        double t[1];
+        totals_cg(part, gridDim.x, 1, t);
+        if (threadIdx.x == 0) { fin_scale(t, S); *ctr = 0u; }
     }
 }
 // e += alpha ph + omega sh; r = s - omega t; partials ||r||^2, (rhat, r)
 __global__ void __launch_bounds__(LB) bs_update_kernel(long long N, float* e, float* r, const float* ph, const float* sh, const float* s,
-                                                       const float* t, const float* rh, double* part, const Scal* S) {
+                                                       const float* t, const float* rh, double* part, Scal* S, unsigned* ctr, int max_iters) {
     if (S->done) return;
     const float al = (float)S->alpha, om = (float)S->omega;
     const long long T = (long long)gridDim.x * LB, t0 = blockIdx.x * (long long)LB + threadIdx.x, NQ = N >> 2;
@@ -1016,19 +1068,10 @@ __global__ void __launch_bounds__(LB) bs_update_kernel(long long N, float* e, fl
         a[1] += (double)rh[c] * rn;
     }
     block_sums(a, 2, part);
-}
-__global__ void bs_update_finish(const double* part, int nblk, Scal* S, int max_iters) {
-    if (S->done) return;
-    double t[2];
-    totals(part, nblk, 2, t);
-    if (threadIdx.x == 0) {
-        S->rr = t[0];
-        S->iters += 1;
-        double rho_new = t[1];
-        bool breakdown = !(S->omega != 0.) || !(S->rho != 0.) || t[1] != t[1];
-        S->beta = breakdown ? 0. : (rho_new / S->rho) * (S->alpha / S->omega);
-        S->rho = rho_new;
-        if (t[0] <= S->tin2 || S->iters >= max_iters || t[0] != t[0] || breakdown) S->done = 1;
+    if (ctr && last_block(ctr)) {
+        double tt[2];
+        totals_cg(part, gridDim.x, 2, tt);
+        if (threadIdx.x == 0) { fin_update(tt, S, max_iters); *ctr = 0u; }
     }
 }
 
@@ -1373,7 +1416,9 @@ int learned_alloc(LearnedWork& lw, const Lat& L, void* (*alloc)(size_t, void*), 
     lw.scal = alloc(sizeof(Scal), ctx);
     lw.mean = static_cast<double*>(alloc(sizeof(double) * 2, ctx));
     lw.rtErr = static_cast<int*>(alloc(sizeof(int) * 4, ctx));
-    bool ok = lw.r && lw.z && lw.e && lw.p[0] && lw.p[1] && lw.q[0] && lw.q[1] && lw.t && lw.rh && lw.invD && lw.part && lw.scal && lw.mean;
+    lw.ctr = static_cast<unsigned*>(alloc(sizeof(unsigned) * 4, ctx));
+    bool ok = lw.r && lw.z && lw.e && lw.p[0] && lw.p[1] && lw.q[0] && lw.q[1] && lw.t && lw.rh && lw.invD && lw.part && lw.scal && lw.mean &&
+              lw.rtErr && lw.ctr;
     for (int q = 0; q < 4; ++q) ok = ok && lw.A[q];
     if (!ok) { set_error("learned-solver allocation failed"); return 1; }
     if (cudaMallocHost(&lw.hostScal, sizeof(Scal)) != cudaSuccess) { set_error("pinned allocation failed"); return 1; }
@@ -1575,22 +1620,17 @@ int learned_solve(LearnedWork& lw, const OpSym& A, const uint8_t* status, const 
                         cur ^= 1;
                     } else {
                         // p = p[0], v = q[0], ph = p[1], sh = q[1], s = z, t = t
-                        bs_dir_kernel<<<nb, LB, 0, st>>>(N, lw.r, lw.q[0], lw.invD, status, lw.p[0], lw.part, S);
-                        scale_finish<<<1, LB, 0, st>>>(lw.part, nb, S);
+                        bs_dir_kernel<<<nb, LB, 0, st>>>(N, lw.r, lw.q[0], lw.invD, status, lw.p[0], lw.part, S, lw.ctr);
                         if (apply_levels(lw, lw.p[0], status, mode, S, st)) return 1;
                         bs_z_kernel<<<nb, LB, 0, st>>>(N, fd, cd, lw.p[0], lw.invD, status, w1, lw.p[1], S);
-                        if (v4) bs_spmv_kernel<true><<<nb, LB, 0, st>>>(Af, N, lw.p[1], lw.q[0], lw.rh, nullptr, lw.part, S);
-                        else bs_spmv_kernel<false><<<nb, LB, 0, st>>>(Af, N, lw.p[1], lw.q[0], lw.rh, nullptr, lw.part, S);
-                        bs_alpha_finish<<<1, LB, 0, st>>>(lw.part, nb, S);
-                        bs_s_kernel<<<nb, LB, 0, st>>>(N, lw.r, lw.q[0], lw.invD, status, lw.z, lw.part, S);
-                        scale_finish<<<1, LB, 0, st>>>(lw.part, nb, S);
+                        if (v4) bs_spmv_kernel<true><<<nb, LB, 0, st>>>(Af, N, lw.p[1], lw.q[0], lw.rh, nullptr, lw.part, S, lw.ctr);
+                        else bs_spmv_kernel<false><<<nb, LB, 0, st>>>(Af, N, lw.p[1], lw.q[0], lw.rh, nullptr, lw.part, S, lw.ctr);
+                        bs_s_kernel<<<nb, LB, 0, st>>>(N, lw.r, lw.q[0], lw.invD, status, lw.z, lw.part, S, lw.ctr);
                         if (apply_levels(lw, lw.z, status, mode, S, st)) return 1;
                         bs_z_kernel<<<nb, LB, 0, st>>>(N, fd, cd, lw.z, lw.invD, status, w1, lw.q[1], S);
-                        if (v4) bs_spmv_kernel<true><<<nb, LB, 0, st>>>(Af, N, lw.q[1], lw.t, nullptr, lw.z, lw.part, S);
-                        else bs_spmv_kernel<false><<<nb, LB, 0, st>>>(Af, N, lw.q[1], lw.t, nullptr, lw.z, lw.part, S);
-                        bs_omega_finish<<<1, LB, 0, st>>>(lw.part, nb, S);
-                        bs_update_kernel<<<nb, LB, 0, st>>>(N, lw.e, lw.r, lw.p[1], lw.q[1], lw.z, lw.t, lw.rh, lw.part, S);
-                        bs_update_finish<<<1, LB, 0, st>>>(lw.part, nb, S, maxit);
+                        if (v4) bs_spmv_kernel<true><<<nb, LB, 0, st>>>(Af, N, lw.q[1], lw.t, nullptr, lw.z, lw.part, S, lw.ctr);
+                        else bs_spmv_kernel<false><<<nb, LB, 0, st>>>(Af, N, lw.q[1], lw.t, nullptr, lw.z, lw.part, S, lw.ctr);
+                        bs_update_kernel<<<nb, LB, 0, st>>>(N, lw.e, lw.r, lw.p[1], lw.q[1], lw.z, lw.t, lw.rh, lw.part, S, lw.ctr, maxit);
                     }
                 }
                 CB_CHECK_LAUNCH();

@@ -74,6 +74,7 @@ struct LearnedWork {
     void* allocCtx = nullptr;
     int lastIters = 0, lastOuter = 0;
     int* rtErr = nullptr;        // set by the TMA-staged restriction when a wait ran out
+    unsigned* ctr = nullptr;     // finished-block counter of the kernels that end with their own reduction
 };
 
 int learned_alloc(LearnedWork& lw, const Lat& L, void* (*alloc)(size_t, void*), void* ctx);
