@@ -671,6 +671,109 @@ __device__ __forceinline__ void prolong4(const Dims3& fd, const Dims3& cd, const
     }
 }
 
+// ---------------------------------------------------------------- coarse tail of the pyramid
+// The coarsest levels in one CTA (pyramid mode): u_lt = R u_(lt-1), with u_(lt-1) staged from global
+// memory into shared memory, u_(l+1) = R u_l, then w_last = gain u_last and
+// w_l = gain_l u_l + P w_(l+1) back up to lt, all in shared memory; u_l and w_l of every tail level
+// are written out.  It replaces 2 (levels - lt) launches of a few hundred cells each by one, with
+// the arithmetic of restrict_kernel and prolong_kernel in the same order.
+constexpr int TAIL_MAX_IN = 8192;       // cells of level lt-1 (staged)
+constexpr int TAIL_THREADS = 1024;
+struct TailArgs {
+    int n;                              // tail levels lt .. lt+n-1
+    Dims3 d[LEARN_MAX_LEVELS + 1];      // d[0]: level lt-1; d[1..n]: the tail levels
+    float rscale[LEARN_MAX_LEVELS], gain[LEARN_MAX_LEVELS];
+    const float* uin;                   // u of level lt-1
+    float* u[LEARN_MAX_LEVELS];
+    float* w[LEARN_MAX_LEVELS];
+};
+
+__device__ __forceinline__ float tail_restrict_at(const float* fin, const Dims3& fd, const Dims3& cd, int I, int J, int K, float scale) {
+    float t2[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        const int fk = 2 * K - 1 + c;
+        float t1[4];
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            const int fj = 2 * J - 1 + b;
+            float v[4];
+#pragma unroll
+            for (int a = 0; a < 4; ++a) {
+                const int fi = 2 * I - 1 + a;
+                const bool in = fi >= 0 && fi < fd.n0 && fj >= 0 && fj < fd.n1 && fk >= 0 && fk < fd.n2;
+                v[a] = in ? fin[((unsigned)fk * (unsigned)fd.n1 + (unsigned)fj) * (unsigned)fd.n0 + (unsigned)fi] : 0.f;
+            }
+            t1[b] = rweight_in(2 * I - 1, fd.n0, I, cd.n0) * v[0] + rweight_in(2 * I, fd.n0, I, cd.n0) * v[1] +
+                    rweight_in(2 * I + 1, fd.n0, I, cd.n0) * v[2] + rweight_in(2 * I + 2, fd.n0, I, cd.n0) * v[3];
+        }
+        t2[c] = rweight_in(2 * J - 1, fd.n1, J, cd.n1) * t1[0] + rweight_in(2 * J, fd.n1, J, cd.n1) * t1[1] +
+                rweight_in(2 * J + 1, fd.n1, J, cd.n1) * t1[2] + rweight_in(2 * J + 2, fd.n1, J, cd.n1) * t1[3];
+    }
+    float acc = rweight_in(2 * K - 1, fd.n2, K, cd.n2) * t2[0] + rweight_in(2 * K, fd.n2, K, cd.n2) * t2[1] +
+                rweight_in(2 * K + 1, fd.n2, K, cd.n2) * t2[2] + rweight_in(2 * K + 2, fd.n2, K, cd.n2) * t2[3];
+    acc *= scale;
+    return acc;
+}
+
+// prolong_at on a shared-memory coarse array (plain loads), the same blend order
+__device__ __forceinline__ float tail_prolong_at(const Dims3& fd, const Dims3& cd, const float* wc, long long f) {
+    const unsigned uf = (unsigned)f, n0 = (unsigned)fd.n0, n1 = (unsigned)fd.n1;
+    const unsigned t = uf / n0;
+    const int fi = (int)(uf - t * n0);
+    const int fk = (int)(t / n1);
+    const int fj = (int)(t - (unsigned)fk * n1);
+    int I0 = fi >> 1, I1 = pclamp((fi & 1) ? I0 + 1 : I0 - 1, cd.n0);
+    int J0 = fj >> 1, J1 = pclamp((fj & 1) ? J0 + 1 : J0 - 1, cd.n1);
+    int K0 = fk >> 1, K1 = pclamp((fk & 1) ? K0 + 1 : K0 - 1, cd.n2);
+    const unsigned sJ = (unsigned)cd.n0, sK = (unsigned)cd.n0 * (unsigned)cd.n1;
+    auto row = [&](int K, int J) {
+        const float* w = wc + (unsigned)K * sK + (unsigned)J * sJ;
+        return 0.75f * w[I0] + 0.25f * w[I1];
+    };
+    float k0 = 0.75f * row(K0, J0) + 0.25f * row(K0, J1);
+    float k1 = 0.75f * row(K1, J0) + 0.25f * row(K1, J1);
+    return 0.75f * k0 + 0.25f * k1;
+}
+
+__global__ void __launch_bounds__(TAIL_THREADS) coarse_tail_kernel(const __grid_constant__ TailArgs a, const Scal* S) {
+    if (S && S->done) return;
+    extern __shared__ float tsm[];
+    long long off[LEARN_MAX_LEVELS + 1];
+    long long total = 0;
+    for (int l = 0; l <= a.n; ++l) {
+        off[l] = total;
+        total += (long long)a.d[l].n0 * a.d[l].n1 * a.d[l].n2;
+    }
+    float* U = tsm;                    // u of levels lt-1 .. lt+n-1, packed
+    float* W = tsm + total - off[1];   // w of the tail levels (the same offsets; nothing for lt-1)
+    const long long n0 = off[1];
+    for (long long c = threadIdx.x; c < n0; c += blockDim.x) U[c] = a.uin[c];
+    __syncthreads();
+    for (int l = 1; l <= a.n; ++l) {
+        const Dims3 fd = a.d[l - 1], cd = a.d[l];
+        const long long N = (long long)cd.n0 * cd.n1 * cd.n2;
+        for (long long c = threadIdx.x; c < N; c += blockDim.x) {
+            const int I = (int)(c % cd.n0), J = (int)((c / cd.n0) % cd.n1), K = (int)(c / ((long long)cd.n0 * cd.n1));
+            const float v = tail_restrict_at(U + off[l - 1], fd, cd, I, J, K, a.rscale[l - 1]);
+            U[off[l] + c] = v;
+            a.u[l - 1][c] = v;
+        }
+        __syncthreads();
+    }
+    for (int l = a.n; l >= 1; --l) {
+        const Dims3 fd = a.d[l];
+        const long long N = (long long)fd.n0 * fd.n1 * fd.n2;
+        for (long long c = threadIdx.x; c < N; c += blockDim.x) {
+            float v = a.gain[l - 1] * 1.f * U[off[l] + c];
+            if (l < a.n) v += tail_prolong_at(fd, a.d[l + 1], W + off[l + 1], c);
+            W[off[l] + c] = v;
+            a.w[l - 1][c] = v;
+        }
+        __syncthreads();
+    }
+}
+
 // w_l = gain * (ydiv ? y : s y) + P w_{l+1}   (wc null on the coarsest level); with yn, the
 // network term is odd: y <- (y - yn) / 2 (yn = the network applied to the negated input)
 __global__ void __launch_bounds__(256) prolong_kernel(Dims3 fd, Dims3 cd, const float* wc, const float* y, const float* yn, int ydiv,
@@ -1341,7 +1444,17 @@ Dims3 dims_of(const Level& l) { return Dims3{l.n[0], l.n[1], l.n[2]}; }
 int apply_levels(LearnedWork& lw, const float* rfine, const uint8_t* status, int mode, Scal* S, cudaStream_t st) {
     if (mode == NET_MODE_JACOBI || lw.nLev < 2) return 0;
     auto netAt = [&](int l) { return mode == NET_MODE_NETWORK && l >= lw.netFrom && l <= lw.netTo; };
-    for (int l = 1; l < lw.nLev; ++l) {
+    // the coarse tail: from the first level lt >= 2 whose finer neighbour has at most TAIL_MAX_IN
+    // cells and from which on no level runs the network, one kernel does the rest of the pyramid
+    int lt = lw.nLev;
+    long long tailCells = 0;   // u and w of the tail levels, in shared memory with the staged input
+    for (int l = lw.nLev - 1; l >= 2; --l) {
+        if (netAt(l) || lw.lev[l - 1].N > TAIL_MAX_IN) break;
+        if ((size_t)(lw.lev[l - 1].N + 2 * (tailCells + lw.lev[l].N)) * sizeof(float) > 48 * 1024) break;
+        tailCells += lw.lev[l].N;
+        lt = l;
+    }
+    for (int l = 1; l < lt; ++l) {
         Level& c = lw.lev[l];
         const Level& f = lw.lev[l - 1];
         if (l == 1 && !netAt(1) && lw.rtErr && restrict_tma_usable(dims_of(f), rfine, lw.invD, status)) {
@@ -1362,7 +1475,26 @@ int apply_levels(LearnedWork& lw, const float* rfine, const uint8_t* status, int
             if (netAt(l)) { nets[nn++] = &lw.lev[l].net; nets[nn++] = &lw.lev[l].netNeg; }
         if (nn > 0 && net_forward_group_if(nets, nn, &S->done, st)) return 1;
     }
-    for (int l = lw.nLev - 1; l >= 1; --l) {
+    if (lt < lw.nLev) {
+        TailArgs ta;
+        std::memset(&ta, 0, sizeof(ta));
+        ta.n = lw.nLev - lt;
+        ta.d[0] = dims_of(lw.lev[lt - 1]);
+        ta.uin = lw.lev[lt - 1].u;
+        long long cells = lw.lev[lt - 1].N;
+        for (int q = 0; q < ta.n; ++q) {
+            Level& c = lw.lev[lt + q];
+            ta.d[q + 1] = dims_of(c);
+            ta.rscale[q] = c.rscale;
+            ta.gain[q] = c.gain;
+            ta.u[q] = c.u;
+            ta.w[q] = c.w;
+            cells += 2 * c.N;
+        }
+        coarse_tail_kernel<<<1, TAIL_THREADS, sizeof(float) * (size_t)cells, st>>>(ta, S);
+        CB_CHECK_LAUNCH();
+    }
+    for (int l = lt - 1; l >= 1; --l) {
         Level& f = lw.lev[l];
         const bool top = l + 1 >= lw.nLev;
         prolong_kernel<<<grid_for(f.N, 256), 256, 0, st>>>(dims_of(f), top ? dims_of(f) : dims_of(lw.lev[l + 1]),
