@@ -396,7 +396,7 @@ constexpr int RT_BX = 72, RT_BXS = 96;
 constexpr int RT_F_BYTES = RT_BX * RFJ * RFK * 4;            // 28800
 constexpr int RT_S_BYTES = RT_BXS * RFJ * RFK;               // 9600
 constexpr int RT_STAGE_BYTES = 2 * RT_F_BYTES + RT_S_BYTES;  // 67200
-constexpr int RT_THREADS = 512;
+constexpr int RT_THREADS = 1024;
 constexpr long long RT_WAIT_LIMIT = 1ll << 19;               // rounds of at most 2 us each
 
 __device__ __forceinline__ uint32_t rt_smem(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
