@@ -392,11 +392,18 @@ def run_b200(args, world, rank, local, pg):
     hbm, peak_kind = peaks()
     learned = args.p_form.startswith("learned")
     method = inner_method(spec, args) if learned else ("pcg" if spec.p_method == "cg_jacobi" else "bicgstab64")
+    bytes_total = None
     if learned:
         per_row = LEARNED_BYTES.get(method) if method != "fgmres" else fgmres_bytes_per_cell(args.restart)
         kname = {"bicgstab": "learned inner flexible BiCGStab iteration (FP32, level pyramid)",
                  "fcg": "learned inner flexible CG iteration (FP32, level pyramid)"}.get(
-            method, f"learned inner FGMRES({args.restart}) iteration (FP32, level pyramid + network, CGS2)")
+            method, f"learned inner iterations: FGMRES({args.restart}) with the network (FP32, CGS2), then flexible "
+                    "BiCGStab with the pyramid once the network stage hands over")
+        if method == "fgmres":
+            # the network stage's FGMRES iterations, then the pyramid stage's iterations after a cascade
+            after = LEARNED_BYTES["bicgstab" if spec.kind == "ibpiso" else "fcg"]
+            bytes_total = (per_row * net_iters + after * (p_iters - net_iters)) * N
+            per_row = bytes_total / (N * p_iters) if p_iters > 0 else per_row
     else:
         per_row = PCG_BYTES_PER_ROW if method == "pcg" else BICGSTAB_BYTES_PER_ROW
         kname = "cg1_kernel (persistent Jacobi-PCG, FP64)" if method == "pcg" else "bicgstab_kernel (persistent Jacobi-BiCGStab, FP64)"
@@ -407,6 +414,7 @@ def run_b200(args, world, rank, local, pg):
                 "traffic": (LEARNED_TRAFFIC_PER_CELL[method] * N if learned and method in LEARNED_TRAFFIC_PER_CELL else None),
                 "traffic_unit": "bytes per inner iteration (ncu capture, scaled by cells)",
                 "bytes_per_row_iteration": per_row,
+                "network_stage_iterations_per_step": (net_iters / args.steps) if learned else None,
                 "p_solve_ms_per_step": p_ms / args.steps, "iterations_per_step": p_iters / args.steps}
 
     # end to end through the C ABI with host buffers: per step, upload the solver state

@@ -1716,12 +1716,8 @@ int learned_solve(LearnedWork& lw, const OpSym& A, const uint8_t* status, const 
                     }
                     fg_step_finish<<<1, LB, 0, st>>>(lw.part, nb, j, m, maxit, F, S);
                     fg_scale_kernel<<<G, 256, 0, st>>>(N, lw.t, lw.fgV + (j + 1) * PS + L.H, S);
-                    if ((j & 7) == 7 || j == m - 1) {
-                        CB_CHECK_LAUNCH();
-                        CB_CUDA(cudaMemcpyAsync(lw.hostScal, S, sizeof(Scal), cudaMemcpyDeviceToHost, st));
-                        CB_CUDA(cudaStreamSynchronize(st));
-                        if (static_cast<Scal*>(lw.hostScal)->done) break;
-                    }
+                    // no host wait inside a cycle: once the cycle's `done` is set on the device, the
+                    // remaining iterations' kernels return at once
                 }
                 fg_solve_kernel<<<1, 32, 0, st>>>(F);
                 fg_combine_kernel<<<nb, LB, 0, st>>>(N, lw.fgZ + L.H, PS, F, lw.e);
