@@ -428,8 +428,12 @@ struct RestrictMaps {
     CUtensorMap fin, invD, st;   // this GPU's own buffers (no cluster multicast)
 };
 
+// PRE: the input is already v (D^-1 x on active cells, 0 elsewhere): one FP32 box per tile, no
+// masking pass, half the shared memory (two CTAs per SM)
+template <bool PRE>
 __global__ void __launch_bounds__(RT_THREADS) restrict_tma_kernel(const __grid_constant__ RestrictMaps maps, Dims3 fd, Dims3 cd, int hasSt,
                                                                   float scale, float* out, int* err, const Scal* S) {
+    constexpr int STAGE = PRE ? RT_F_BYTES : RT_STAGE_BYTES;
     if (S && S->done) return;
     extern __shared__ __align__(1024) unsigned char rt_raw[];
     unsigned char* smem = (unsigned char*)(((uintptr_t)rt_raw + 1023) & ~(uintptr_t)1023);
@@ -449,14 +453,16 @@ __global__ void __launch_bounds__(RT_THREADS) restrict_tma_kernel(const __grid_c
     auto issue = [&](int tile, int stage) {
         const int ti = tile % tI, tj = (tile / tI) % tJ, tk = tile / (tI * tJ);
         const int x = 2 * ti * RCI - 4, y = 2 * tj * RCJ - 1, z = 2 * tk * RCK - 1;
-        unsigned char* b = smem + (size_t)stage * RT_STAGE_BYTES;
+        unsigned char* b = smem + (size_t)stage * STAGE;
         const uint32_t bar = rt_smem(&full[stage]);
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // after the generic writes of this stage's last tile
         asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
-                     "r"((uint32_t)(hasSt ? RT_STAGE_BYTES : 2 * RT_F_BYTES)) : "memory");
+                     "r"((uint32_t)(PRE ? RT_F_BYTES : (hasSt ? RT_STAGE_BYTES : 2 * RT_F_BYTES))) : "memory");
         rt_load3d(rt_smem(b), &maps.fin, x, y, z, bar);
-        rt_load3d(rt_smem(b + RT_F_BYTES), &maps.invD, x, y, z, bar);
-        if (hasSt) rt_load3d(rt_smem(b + 2 * RT_F_BYTES), &maps.st, x - 12, y, z, bar);
+        if (!PRE) {
+            rt_load3d(rt_smem(b + RT_F_BYTES), &maps.invD, x, y, z, bar);
+            if (hasSt) rt_load3d(rt_smem(b + 2 * RT_F_BYTES), &maps.st, x - 12, y, z, bar);
+        }
         ++issued[stage];
     };
     if (threadIdx.x == 0 && (int)blockIdx.x < T) issue(blockIdx.x, 0);
@@ -479,17 +485,19 @@ __global__ void __launch_bounds__(RT_THREADS) restrict_tma_kernel(const __grid_c
         }
         const bool ok = rt_wait(rt_smem(&full[stage]), (uint32_t)((n >> 1) & 1));
         if (__syncthreads_or(ok ? 0 : 1)) { failed = true; break; }
-        float* sf = reinterpret_cast<float*>(smem + (size_t)stage * RT_STAGE_BYTES);
-        const float* sd = sf + RT_F_BYTES / 4;
-        const unsigned char* ss = smem + (size_t)stage * RT_STAGE_BYTES + 2 * RT_F_BYTES;
-        // v = fin * invD on active cells, in place, for the 66 columns the tile draws on (3 .. 68)
-        for (int e = threadIdx.x; e < RFK * RFJ * RFI; e += RT_THREADS) {
-            const int li = e % RFI, row = e / RFI;
-            const int o = row * RT_BX + 3 + li;
-            const bool act = !hasSt || ss[row * RT_BXS + 15 + li] == ST_ACTIVE;
-            sf[o] = act ? sf[o] * sd[o] : 0.f;
+        float* sf = reinterpret_cast<float*>(smem + (size_t)stage * STAGE);
+        if (!PRE) {
+            const float* sd = sf + RT_F_BYTES / 4;
+            const unsigned char* ss = smem + (size_t)stage * STAGE + 2 * RT_F_BYTES;
+            // v = fin * invD on active cells, in place, for the 66 columns the tile draws on (3 .. 68)
+            for (int e = threadIdx.x; e < RFK * RFJ * RFI; e += RT_THREADS) {
+                const int li = e % RFI, row = e / RFI;
+                const int o = row * RT_BX + 3 + li;
+                const bool act = !hasSt || ss[row * RT_BXS + 15 + li] == ST_ACTIVE;
+                sf[o] = act ? sf[o] * sd[o] : 0.f;
+            }
+            __syncthreads();
         }
-        __syncthreads();
         for (int u = threadIdx.x; u < RFK * RFJ * RCI; u += RT_THREADS) {
             const int ci = u % RCI, row = u / RCI;
             const float* v = sf + row * RT_BX + 3 + 2 * ci;
@@ -558,35 +566,44 @@ const CUtensorMap* rt_map(const void* base, const Dims3& fd, int esize) {
 // multiples (status rows of bytes too) and 16-byte aligned bases
 bool restrict_tma_usable(const Dims3& fd, const float* fin, const float* invD, const uint8_t* st) {
     auto al = [](const void* p) { return ((uintptr_t)p & 15u) == 0; };
-    if (fd.n0 % 4 != 0 || !al(fin) || !al(invD)) return false;
+    if (fd.n0 % 4 != 0 || !al(fin) || (invD && !al(invD))) return false;
     if (st && (fd.n0 % 16 != 0 || !al(st))) return false;
     return rt_encode_fn() != nullptr;
 }
 
+// invD null: fin is already v (pre-multiplied and masked)
 int launch_restrict_tma(const Dims3& fd, const Dims3& cd, const float* fin, const float* invD, const uint8_t* st, float scale, float* out,
                         int* err, const Scal* S, cudaStream_t stream) {
     RestrictMaps maps;
     std::memset(&maps, 0, sizeof(maps));
+    const bool pre = invD == nullptr;
     const CUtensorMap* mf = rt_map(fin, fd, 4);
-    const CUtensorMap* md = rt_map(invD, fd, 4);
-    const CUtensorMap* ms = st ? rt_map(st, fd, 1) : nullptr;
-    if (!mf || !md || (st && !ms)) { set_error("tensor map encoding failed for the staged restriction"); return 1; }
+    const CUtensorMap* md = pre ? nullptr : rt_map(invD, fd, 4);
+    const CUtensorMap* ms = (!pre && st) ? rt_map(st, fd, 1) : nullptr;
+    if (!mf || (!pre && !md) || (!pre && st && !ms)) { set_error("tensor map encoding failed for the staged restriction"); return 1; }
     maps.fin = *mf;
-    maps.invD = *md;
+    if (md) maps.invD = *md;
     if (ms) maps.st = *ms;
-    const size_t smem = 1024 + 2 * (size_t)RT_STAGE_BYTES;
+    const size_t smemFull = 1024 + 2 * (size_t)RT_STAGE_BYTES, smemPre = 1024 + 2 * (size_t)RT_F_BYTES;
     static bool attr = false;
     static int nsm = 0;
     if (!attr) {
-        CB_CUDA(cudaFuncSetAttribute(restrict_tma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        CB_CUDA(cudaFuncSetAttribute(restrict_tma_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemFull));
+        CB_CUDA(cudaFuncSetAttribute(restrict_tma_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemPre));
         int dev = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
         attr = true;
     }
     const long long T = (long long)((cd.n0 + RCI - 1) / RCI) * ((cd.n1 + RCJ - 1) / RCJ) * ((cd.n2 + RCK - 1) / RCK);
-    const int grid = (int)std::min<long long>(T, nsm > 0 ? nsm : 148);
-    restrict_tma_kernel<<<grid, RT_THREADS, smem, stream>>>(maps, fd, cd, st ? 1 : 0, scale, out, err, S);
+    const int sms = nsm > 0 ? nsm : 148;
+    if (pre) {
+        const int grid = (int)std::min<long long>(T, 2LL * sms);   // two CTAs per SM
+        restrict_tma_kernel<true><<<grid, RT_THREADS, smemPre, stream>>>(maps, fd, cd, 0, scale, out, err, S);
+    } else {
+        const int grid = (int)std::min<long long>(T, sms);
+        restrict_tma_kernel<false><<<grid, RT_THREADS, smemFull, stream>>>(maps, fd, cd, st ? 1 : 0, scale, out, err, S);
+    }
     CB_CHECK_LAUNCH();
     return 0;
 }
@@ -978,7 +995,7 @@ __device__ __forceinline__ void fin_update(const double* t, Scal* S, int max_ite
 }
 // p = r + beta (p - omega v); partial sum of (D^-1 p)^2 over active cells (scale of M(p))
 __global__ void __launch_bounds__(LB) bs_dir_kernel(long long N, const float* r, const float* v, const float* invD, const uint8_t* st,
-                                                    float* p, double* part, Scal* S, unsigned* ctr) {
+                                                    float* p, double* part, Scal* S, unsigned* ctr, float* uo) {
     if (S->done) return;
     const float be = (float)S->beta, om = (float)S->omega;
     const long long T = (long long)gridDim.x * LB, t0 = blockIdx.x * (long long)LB + threadIdx.x, NQ = N >> 2;
@@ -987,17 +1004,21 @@ __global__ void __launch_bounds__(LB) bs_dir_kernel(long long N, const float* r,
         float R[4], V[4], P4[4], D[4];
         uint8_t F[4];
         un4(ld4(r, q), R); un4(ld4(v, q), V); un4(ld4(p, q), P4); un4(ld4(invD, q), D); st_flags4(st, q, F);
+        float U[4];
 #pragma unroll
         for (int m = 0; m < 4; ++m) {
             P4[m] = R[m] + be * (P4[m] - om * V[m]);
+            U[m] = F[m] == ST_ACTIVE ? D[m] * P4[m] : 0.f;
             if (F[m] == ST_ACTIVE) { double u = (double)D[m] * P4[m]; a[0] += u * u; }
         }
         st4(p, q, P4);
+        if (uo) st4(uo, q, U);
     }
     for (long long c = 4 * NQ + t0; c < N; c += T) {
         float pv = r[c] + be * (p[c] - om * v[c]);
         p[c] = pv;
         if (is_active(st, c)) { double u = (double)__ldg(invD + c) * pv; a[0] += u * u; }
+        if (uo) uo[c] = is_active(st, c) ? __ldg(invD + c) * pv : 0.f;
     }
     block_sums(a, 1, part);
     if (ctr && last_block(ctr)) {
@@ -1115,7 +1136,7 @@ __global__ void __launch_bounds__(LB) bs_spmv_kernel(OpSymF32 A, long long N, co
 }
 // s = r - alpha v; partial sum of (D^-1 s)^2 over active cells
 __global__ void __launch_bounds__(LB) bs_s_kernel(long long N, const float* r, const float* v, const float* invD, const uint8_t* st, float* s,
-                                                  double* part, Scal* S, unsigned* ctr) {
+                                                  double* part, Scal* S, unsigned* ctr, float* uo) {
     if (S->done) return;
     const float al = (float)S->alpha;
     const long long T = (long long)gridDim.x * LB, t0 = blockIdx.x * (long long)LB + threadIdx.x, NQ = N >> 2;
@@ -1124,17 +1145,21 @@ __global__ void __launch_bounds__(LB) bs_s_kernel(long long N, const float* r, c
         float R[4], V[4], D[4], O[4];
         uint8_t F[4];
         un4(ld4(r, q), R); un4(ld4(v, q), V); un4(ld4(invD, q), D); st_flags4(st, q, F);
+        float U[4];
 #pragma unroll
         for (int m = 0; m < 4; ++m) {
             O[m] = R[m] - al * V[m];
+            U[m] = F[m] == ST_ACTIVE ? D[m] * O[m] : 0.f;
             if (F[m] == ST_ACTIVE) { double u = (double)D[m] * O[m]; a[0] += u * u; }
         }
         st4(s, q, O);
+        if (uo) st4(uo, q, U);
     }
     for (long long c = 4 * NQ + t0; c < N; c += T) {
         float sv = r[c] - al * v[c];
         s[c] = sv;
         if (is_active(st, c)) { double u = (double)__ldg(invD + c) * sv; a[0] += u * u; }
+        if (uo) uo[c] = is_active(st, c) ? __ldg(invD + c) * sv : 0.f;
     }
     block_sums(a, 1, part);
     if (ctr && last_block(ctr)) {
@@ -1263,11 +1288,14 @@ __global__ void fg_start_finish(Scal* S, double eta, const double* nact) {
 }
 // partial sum of (D^-1 x)^2 over active cells (the network scale of M(x))
 __global__ void __launch_bounds__(LB) scale_partial_kernel(long long N, const float* x, const float* invD, const uint8_t* st, double* part,
-                                                           const Scal* S) {
+                                                           const Scal* S, float* uo) {
     if (S->done) return;
     double a[1] = {0.};
-    for (long long c = blockIdx.x * (long long)LB + threadIdx.x; c < N; c += (long long)gridDim.x * LB)
-        if (is_active(st, c)) { double u = (double)__ldg(invD + c) * x[c]; a[0] += u * u; }
+    for (long long c = blockIdx.x * (long long)LB + threadIdx.x; c < N; c += (long long)gridDim.x * LB) {
+        const bool act = is_active(st, c);
+        if (act) { double u = (double)__ldg(invD + c) * x[c]; a[0] += u * u; }
+        if (uo) uo[c] = act ? __ldg(invD + c) * x[c] : 0.f;
+    }
     block_sums(a, 1, part);
 }
 // w = A z (FP32, with the ghost rows)
@@ -1441,7 +1469,9 @@ Dims3 dims_of(const Level& l) { return Dims3{l.n[0], l.n[1], l.n[2]}; }
 
 // Restriction chain, the network (or the identity) on every coarse level, prolongation chain
 // (result in lev[1].w).  Every kernel is a no-op while S->done is set.
-int apply_levels(LearnedWork& lw, const float* rfine, const uint8_t* status, int mode, Scal* S, cudaStream_t st) {
+// ufine: optional D^-1 rfine on active cells, 0 elsewhere (written by the kernel that produced
+// rfine); with it the restriction to level 1 stages one array instead of three
+int apply_levels(LearnedWork& lw, const float* rfine, const uint8_t* status, int mode, Scal* S, cudaStream_t st, const float* ufine = nullptr) {
     if (mode == NET_MODE_JACOBI || lw.nLev < 2) return 0;
     auto netAt = [&](int l) { return mode == NET_MODE_NETWORK && l >= lw.netFrom && l <= lw.netTo; };
     // the coarse tail: from the first level lt >= 2 whose finer neighbour has at most TAIL_MAX_IN
@@ -1457,6 +1487,10 @@ int apply_levels(LearnedWork& lw, const float* rfine, const uint8_t* status, int
     for (int l = 1; l < lt; ++l) {
         Level& c = lw.lev[l];
         const Level& f = lw.lev[l - 1];
+        if (l == 1 && !netAt(1) && lw.rtErr && ufine && restrict_tma_usable(dims_of(f), ufine, nullptr, nullptr)) {
+            if (launch_restrict_tma(dims_of(f), dims_of(c), ufine, nullptr, nullptr, c.rscale, c.u, lw.rtErr, S, st)) return 1;
+            continue;
+        }
         if (l == 1 && !netAt(1) && lw.rtErr && restrict_tma_usable(dims_of(f), rfine, lw.invD, status)) {
             if (launch_restrict_tma(dims_of(f), dims_of(c), rfine, lw.invD, status, c.rscale, c.u, lw.rtErr, S, st)) return 1;
             continue;
@@ -1539,7 +1573,7 @@ int learned_alloc(LearnedWork& lw, const Lat& L, void* (*alloc)(size_t, void*), 
         float* b = static_cast<float*>(alloc(sizeof(float) * (size_t)L.PS, ctx));
         return b ? b + L.H : nullptr;
     };
-    lw.r = fcell(); lw.z = fcell(); lw.e = fcell();
+    lw.r = fcell(); lw.z = fcell(); lw.e = fcell(); lw.u1 = fcell();
     lw.p[0] = fcell(); lw.p[1] = fcell(); lw.q[0] = fcell(); lw.q[1] = fcell();
     lw.t = fcell(); lw.rh = fcell();
     lw.invD = fcell();
@@ -1550,7 +1584,7 @@ int learned_alloc(LearnedWork& lw, const Lat& L, void* (*alloc)(size_t, void*), 
     lw.rtErr = static_cast<int*>(alloc(sizeof(int) * 4, ctx));
     lw.ctr = static_cast<unsigned*>(alloc(sizeof(unsigned) * 4, ctx));
     bool ok = lw.r && lw.z && lw.e && lw.p[0] && lw.p[1] && lw.q[0] && lw.q[1] && lw.t && lw.rh && lw.invD && lw.part && lw.scal && lw.mean &&
-              lw.rtErr && lw.ctr;
+              lw.rtErr && lw.ctr && lw.u1;
     for (int q = 0; q < 4; ++q) ok = ok && lw.A[q];
     if (!ok) { set_error("learned-solver allocation failed"); return 1; }
     if (cudaMallocHost(&lw.hostScal, sizeof(Scal)) != cudaSuccess) { set_error("pinned allocation failed"); return 1; }
@@ -1696,9 +1730,9 @@ int learned_solve(LearnedWork& lw, const OpSym& A, const uint8_t* status, const 
                 for (int j = 0; j < m; ++j) {
                     float* vj = lw.fgV + j * PS + L.H;
                     float* zj = lw.fgZ + j * PS + L.H;
-                    scale_partial_kernel<<<nb, LB, 0, st>>>(N, vj, lw.invD, status, lw.part, S);
+                    scale_partial_kernel<<<nb, LB, 0, st>>>(N, vj, lw.invD, status, lw.part, S, lw.u1);
                     scale_finish<<<1, LB, 0, st>>>(lw.part, nb, S);
-                    if (apply_levels(lw, vj, status, mode, S, st)) return 1;
+                    if (apply_levels(lw, vj, status, mode, S, st, lw.u1)) return 1;
                     bs_z_kernel<<<nb, LB, 0, st>>>(N, fd, cd, vj, lw.invD, status, w1, zj, S);
                     if (v4) fg_spmv_kernel<true><<<nb, LB, 0, st>>>(Af, N, zj, lw.t, S);
                     else fg_spmv_kernel<false><<<nb, LB, 0, st>>>(Af, N, zj, lw.t, S);
@@ -1748,13 +1782,13 @@ int learned_solve(LearnedWork& lw, const OpSym& A, const uint8_t* status, const 
                         cur ^= 1;
                     } else {
                         // p = p[0], v = q[0], ph = p[1], sh = q[1], s = z, t = t
-                        bs_dir_kernel<<<nb, LB, 0, st>>>(N, lw.r, lw.q[0], lw.invD, status, lw.p[0], lw.part, S, lw.ctr);
-                        if (apply_levels(lw, lw.p[0], status, mode, S, st)) return 1;
+                        bs_dir_kernel<<<nb, LB, 0, st>>>(N, lw.r, lw.q[0], lw.invD, status, lw.p[0], lw.part, S, lw.ctr, lw.u1);
+                        if (apply_levels(lw, lw.p[0], status, mode, S, st, lw.u1)) return 1;
                         bs_z_kernel<<<nb, LB, 0, st>>>(N, fd, cd, lw.p[0], lw.invD, status, w1, lw.p[1], S);
                         if (v4) bs_spmv_kernel<true><<<nb, LB, 0, st>>>(Af, N, lw.p[1], lw.q[0], lw.rh, nullptr, lw.part, S, lw.ctr);
                         else bs_spmv_kernel<false><<<nb, LB, 0, st>>>(Af, N, lw.p[1], lw.q[0], lw.rh, nullptr, lw.part, S, lw.ctr);
-                        bs_s_kernel<<<nb, LB, 0, st>>>(N, lw.r, lw.q[0], lw.invD, status, lw.z, lw.part, S, lw.ctr);
-                        if (apply_levels(lw, lw.z, status, mode, S, st)) return 1;
+                        bs_s_kernel<<<nb, LB, 0, st>>>(N, lw.r, lw.q[0], lw.invD, status, lw.z, lw.part, S, lw.ctr, lw.u1);
+                        if (apply_levels(lw, lw.z, status, mode, S, st, lw.u1)) return 1;
                         bs_z_kernel<<<nb, LB, 0, st>>>(N, fd, cd, lw.z, lw.invD, status, w1, lw.q[1], S);
                         if (v4) bs_spmv_kernel<true><<<nb, LB, 0, st>>>(Af, N, lw.q[1], lw.t, nullptr, lw.z, lw.part, S, lw.ctr);
                         else bs_spmv_kernel<false><<<nb, LB, 0, st>>>(Af, N, lw.q[1], lw.t, nullptr, lw.z, lw.part, S, lw.ctr);

@@ -75,6 +75,7 @@ struct LearnedWork {
     int lastIters = 0, lastOuter = 0;
     int* rtErr = nullptr;        // set by the TMA-staged restriction when a wait ran out
     unsigned* ctr = nullptr;     // finished-block counter of the kernels that end with their own reduction
+    float* u1 = nullptr;         // D^-1 x on active cells of the vector being preconditioned (restriction input)
 };
 
 int learned_alloc(LearnedWork& lw, const Lat& L, void* (*alloc)(size_t, void*), void* ctx);
