@@ -527,7 +527,7 @@ def main():
                     "(default: the one the shipped parameters were trained for)")
     ap.add_argument("--net-to", type=int, default=None, help="last pyramid level that runs the network "
                     "(default: the coarsest level the shipped parameters were trained on)")
-    ap.add_argument("--restart", type=int, default=10)
+    ap.add_argument("--restart", type=int, default=5)
     ap.add_argument("--params", default=None, help="network parameters (.npy); default: the shipped ones")
     ap.add_argument("--size", type=int, default=None)
     ap.add_argument("--compare-fp64", type=int, default=1, help="plain FP64 steps from rest to compare with")

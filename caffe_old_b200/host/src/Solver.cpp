@@ -13,6 +13,7 @@
 //   LearnedPreconditioner.mode         levels | network | jacobi
 //   LearnedPreconditioner.parameters   file of caffe_precond_param_count() floats (raw or .npy)
 //   LearnedPreconditioner.firstNetworkLevel   first pyramid level that runs the network (1)
+//   LearnedPreconditioner.lastNetworkLevel    last pyramid level that runs the network (all)
 //   LearnedPreconditioner.innerMethod  auto | fcg | bicgstab | fgmres
 //   LearnedPreconditioner.restart      FGMRES cycle length (40)
 #include "Solver.h"
@@ -163,6 +164,9 @@ Solver::Solver(const Input& input, const HexaFvmMesh& mesh, int kind) : mesh_(me
         int restart = c.get<int>("LearnedPreconditioner.restart", 40);
         if (caffe_dev_set_precond_options(h_, im, netFrom, restart) != 0)
             Output::raiseException("Solver", "Solver", std::string("cannot set the preconditioner options: ") + caffe_last_error());
+        int netTo = c.get<int>("LearnedPreconditioner.lastNetworkLevel", -1);
+        if (caffe_dev_set_precond_net_levels(h_, netFrom, netTo) != 0)
+            Output::raiseException("Solver", "Solver", std::string("cannot set the network levels: ") + caffe_last_error());
     }
     mesh.attachSolver(this);
 }

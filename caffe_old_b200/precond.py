@@ -95,9 +95,12 @@ def pyramid_dims(dims) -> list:
 
 
 def trained_last_level() -> int | None:
-    """The coarsest pyramid level the shipped parameters were trained on (the network has never
-    seen the level channel of a coarser one), or None when unknown."""
+    """The last pyramid level that runs the network with the shipped parameters: the measured
+    choice recorded with them, else the coarsest level they were trained on (the network has
+    never seen the level channel of a coarser one), or None when unknown."""
     info = default_info()
+    if "net_to_run" in info:
+        return int(info["net_to_run"])
     if "net_to" in info:
         return int(info["net_to"])
     if "dims" in info:
