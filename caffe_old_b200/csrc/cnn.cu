@@ -256,11 +256,14 @@ __global__ void __launch_bounds__(CONV_THREADS) conv3d_tc_kernel(const __grid_co
     asm volatile("tcgen05.fence::after_thread_sync;");
     const uint32_t tmem = tmem_base_sh;
 
-    // bounded wait that also gives up once another role has failed (checked every 16 rounds)
-    auto wait = [&](uint64_t* b, uint32_t parity) -> bool {
+    // bounded wait that also gives up once another role has failed (checked every 16 rounds); the
+    // epilogue warps suspend in hardware while they wait, the single producer and MMA threads poll
+    // so that they resume at once
+    auto wait = [&](uint64_t* b, uint32_t parity, bool sleep) -> bool {
         const uint32_t a = smem_u32(b);
-        for (long long t = 0; t < SLEEP_WAIT_LIMIT; ++t) {
-            if (mbar_try_sleep(a, parity, SLEEP_NS)) return true;
+        const long long limit = sleep ? SLEEP_WAIT_LIMIT : WAIT_LIMIT;
+        for (long long t = 0; t < limit; ++t) {
+            if (sleep ? mbar_try_sleep(a, parity, SLEEP_NS) : mbar_try(a, parity)) return true;
             if ((t & 15) == 15 && fail_sh) return false;
         }
         fail_sh = 1;
@@ -272,7 +275,7 @@ __global__ void __launch_bounds__(CONV_THREADS) conv3d_tc_kernel(const __grid_co
         int issued[NPL] = {};
         for (int q = 0; q < nP; ++q) {
             const int sl = q % NPL;
-            if (q >= NPL && !wait(&empty[sl], (uint32_t)((q / NPL - 1) & 1))) break;
+            if (q >= NPL && !wait(&empty[sl], (uint32_t)((q / NPL - 1) & 1), false)) break;
             const uint32_t fb = smem_u32(&full[sl]);
             mbar_expect_tx(fb, 3 * BUF_BYTES);
             for (int sh = 0; sh < 3; ++sh)
@@ -292,10 +295,10 @@ __global__ void __launch_bounds__(CONV_THREADS) conv3d_tc_kernel(const __grid_co
             const int a = o % NACC;
             bool ok = true;
             while (ok && ready < o + 3) {
-                ok = wait(&full[ready % NPL], (uint32_t)((ready / NPL) & 1));
+                ok = wait(&full[ready % NPL], (uint32_t)((ready / NPL) & 1), false);
                 ++ready;
             }
-            if (ok && o >= NACC) ok = wait(&acce[a], (uint32_t)((o / NACC - 1) & 1));
+            if (ok && o >= NACC) ok = wait(&acce[a], (uint32_t)((o / NACC - 1) & 1), false);
             if (!ok) break;
             asm volatile("tcgen05.fence::after_thread_sync;");
             int t = 0;
@@ -326,7 +329,7 @@ __global__ void __launch_bounds__(CONV_THREADS) conv3d_tc_kernel(const __grid_co
         for (int o = 0; o < nO; ++o) {
             const int a = o % NACC;
             // warp-uniform outcome: the tcgen05.ld below is a warp-wide instruction
-            if (!__all_sync(0xffffffffu, wait(&accf[a], (uint32_t)((o / NACC) & 1)) ? 1 : 0)) break;
+            if (!__all_sync(0xffffffffu, wait(&accf[a], (uint32_t)((o / NACC) & 1), true) ? 1 : 0)) break;
             asm volatile("tcgen05.fence::after_thread_sync;");
             float v[16];
             tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(16 * a), v);

@@ -397,20 +397,22 @@ constexpr int RT_F_BYTES = RT_BX * RFJ * RFK * 4;            // 28800
 constexpr int RT_S_BYTES = RT_BXS * RFJ * RFK;               // 9600
 constexpr int RT_STAGE_BYTES = 2 * RT_F_BYTES + RT_S_BYTES;  // 67200
 constexpr int RT_THREADS = 1024;
-constexpr long long RT_WAIT_LIMIT = 1ll << 19;               // rounds of at most 2 us each
+constexpr long long RT_WAIT_LIMIT = 1ll << 22;               // polls (each at most a short hardware wait)
 
 __device__ __forceinline__ uint32_t rt_smem(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 __device__ __forceinline__ bool rt_try(uint32_t bar, uint32_t parity) {
     uint32_t ok;
     asm volatile(
         "{\n\t.reg .pred P1;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2, %3;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
         "selp.b32 %0, 1, 0, P1;\n\t}\n"
         : "=r"(ok)
-        : "r"(bar), "r"(parity), "r"(2000u)
+        : "r"(bar), "r"(parity)
         : "memory");
     return ok != 0;
 }
+// polled by one warp per CTA (the others wait at the barrier that follows), without a suspend
+// hint, so that a tile starts as soon as its data has landed
 __device__ __forceinline__ bool rt_wait(uint32_t bar, uint32_t parity) {
     for (long long t = 0; t < RT_WAIT_LIMIT; ++t)
         if (rt_try(bar, parity)) return true;
@@ -429,27 +431,27 @@ struct RestrictMaps {
 };
 
 // PRE: the input is already v (D^-1 x on active cells, 0 elsewhere): one FP32 box per tile, no
-// masking pass, half the shared memory (two CTAs per SM)
+// masking pass, three stages in less shared memory (two CTAs per SM)
 template <bool PRE>
-__global__ void __launch_bounds__(RT_THREADS) restrict_tma_kernel(const __grid_constant__ RestrictMaps maps, Dims3 fd, Dims3 cd, int hasSt,
+__global__ void __launch_bounds__(RT_THREADS, 2) restrict_tma_kernel(const __grid_constant__ RestrictMaps maps, Dims3 fd, Dims3 cd, int hasSt,
                                                                   float scale, float* out, int* err, const Scal* S) {
     constexpr int STAGE = PRE ? RT_F_BYTES : RT_STAGE_BYTES;
+    constexpr int NS = PRE ? 3 : 2;   // stages: tiles in flight ahead of the one being reduced = NS - 1
     if (S && S->done) return;
     extern __shared__ __align__(1024) unsigned char rt_raw[];
     unsigned char* smem = (unsigned char*)(((uintptr_t)rt_raw + 1023) & ~(uintptr_t)1023);
-    __shared__ __align__(8) uint64_t full[2];
+    __shared__ __align__(8) uint64_t full[3];
     __shared__ float t1[RFK][RFJ][RCI];
     __shared__ float t2[RFK][RCJ][RCI];
     __shared__ float wI[RCI][4], wJ[RCJ][4], wK[RCK][4];
     const int tI = (cd.n0 + RCI - 1) / RCI, tJ = (cd.n1 + RCJ - 1) / RCJ, tK = (cd.n2 + RCK - 1) / RCK;
     const int T = tI * tJ * tK;
     if (threadIdx.x == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(rt_smem(&full[0])));
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(rt_smem(&full[1])));
+        for (int q = 0; q < NS; ++q) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(rt_smem(&full[q])));
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
-    int issued[2] = {0, 0};   // thread 0: loads issued per stage
+    int issued[3] = {0, 0, 0};   // thread 0: loads issued per stage
     auto issue = [&](int tile, int stage) {
         const int ti = tile % tI, tj = (tile / tI) % tJ, tk = tile / (tI * tJ);
         const int x = 2 * ti * RCI - 4, y = 2 * tj * RCJ - 1, z = 2 * tk * RCK - 1;
@@ -465,12 +467,16 @@ __global__ void __launch_bounds__(RT_THREADS) restrict_tma_kernel(const __grid_c
         }
         ++issued[stage];
     };
-    if (threadIdx.x == 0 && (int)blockIdx.x < T) issue(blockIdx.x, 0);
+    if (threadIdx.x == 0)
+        for (int q = 0; q < NS - 1; ++q)
+            if ((int)blockIdx.x + q * (int)gridDim.x < T) issue(blockIdx.x + q * gridDim.x, q);
     bool failed = false;
     int n = 0;
     for (int tile = blockIdx.x; tile < T; tile += gridDim.x, ++n) {
-        const int stage = n & 1;
-        if (threadIdx.x == 0 && tile + (int)gridDim.x < T) issue(tile + gridDim.x, stage ^ 1);
+        const int stage = n % NS;
+        // the stage of tile n-1, free since the barrier that ended it, takes tile n + NS - 1
+        const int ahead = tile + (NS - 1) * (int)gridDim.x;
+        if (threadIdx.x == 0 && ahead < T) issue(ahead, (n + NS - 1) % NS);
         const int ti = tile % tI, tj = (tile / tI) % tJ, tk = tile / (tI * tJ);
         const int I0 = ti * RCI, J0 = tj * RCJ, K0 = tk * RCK;
         if (threadIdx.x < 4 * RCI) {
@@ -483,7 +489,8 @@ __global__ void __launch_bounds__(RT_THREADS) restrict_tma_kernel(const __grid_c
             int u = threadIdx.x - 4 * RCI - 4 * RCJ, ck = u >> 2, m = u & 3, K = K0 + ck;
             wK[ck][m] = rweight_in(2 * K - 1 + m, fd.n2, K, cd.n2);
         }
-        const bool ok = rt_wait(rt_smem(&full[stage]), (uint32_t)((n >> 1) & 1));
+        bool ok = true;
+        if (threadIdx.x < 32) ok = rt_wait(rt_smem(&full[stage]), (uint32_t)((n / NS) & 1));
         if (__syncthreads_or(ok ? 0 : 1)) { failed = true; break; }
         float* sf = reinterpret_cast<float*>(smem + (size_t)stage * STAGE);
         if (!PRE) {
@@ -523,7 +530,7 @@ __global__ void __launch_bounds__(RT_THREADS) restrict_tma_kernel(const __grid_c
     if (threadIdx.x == 0) {
         if (failed) atomicExch(err, 1);
         // every load issued lands before the shared memory is released
-        for (int q = 0; q < 2; ++q)
+        for (int q = 0; q < NS; ++q)
             if (issued[q] > 0) rt_wait(rt_smem(&full[q]), (uint32_t)((issued[q] - 1) & 1));
     }
     __syncthreads();
@@ -584,7 +591,7 @@ int launch_restrict_tma(const Dims3& fd, const Dims3& cd, const float* fin, cons
     maps.fin = *mf;
     if (md) maps.invD = *md;
     if (ms) maps.st = *ms;
-    const size_t smemFull = 1024 + 2 * (size_t)RT_STAGE_BYTES, smemPre = 1024 + 2 * (size_t)RT_F_BYTES;
+    const size_t smemFull = 1024 + 2 * (size_t)RT_STAGE_BYTES, smemPre = 1024 + 3 * (size_t)RT_F_BYTES;
     static bool attr = false;
     static int nsm = 0;
     if (!attr) {
