@@ -642,17 +642,24 @@ __device__ __forceinline__ float prolong_at(const Dims3& fd, const Dims3& cd, co
 
 // (P wc) for the 4 consecutive cells 4q..4q+3 of the fine lattice fd: the (j, k) part of the
 // index and the four coarse rows are computed once when the 4 cells share a row
+__device__ __forceinline__ void prolong4_ijk(const Dims3& fd, const Dims3& cd, const float* wc, unsigned f0, int fi, int fj, int fk,
+                                             float (&out)[4]);
 __device__ __forceinline__ void prolong4(const Dims3& fd, const Dims3& cd, const float* wc, long long q, float (&out)[4]) {
     const unsigned f0 = (unsigned)(4 * q), n0 = (unsigned)fd.n0, n1 = (unsigned)fd.n1;
     const unsigned t = f0 / n0;
     const int fi = (int)(f0 - t * n0);
+    const int fk = (int)(t / n1);
+    const int fj = (int)(t - (unsigned)fk * n1);
+    prolong4_ijk(fd, cd, wc, f0, fi, fj, fk, out);
+}
+// the same for the 4 cells from f0 = (fk nJ + fj) nI + fi, whose coordinates the caller knows
+__device__ __forceinline__ void prolong4_ijk(const Dims3& fd, const Dims3& cd, const float* wc, unsigned f0, int fi, int fj, int fk,
+                                             float (&out)[4]) {
     if (fi + 3 >= fd.n0) {   // the 4 cells span a row end
 #pragma unroll
         for (int m = 0; m < 4; ++m) out[m] = prolong_at(fd, cd, wc, (long long)f0 + m);
         return;
     }
-    const int fk = (int)(t / n1);
-    const int fj = (int)(t - (unsigned)fk * n1);
     const int J0 = fj >> 1, J1 = pclamp((fj & 1) ? J0 + 1 : J0 - 1, cd.n1);
     const int K0 = fk >> 1, K1 = pclamp((fk & 1) ? K0 + 1 : K0 - 1, cd.n2);
     const unsigned sJ = (unsigned)cd.n0, sK = (unsigned)cd.n0 * (unsigned)cd.n1;
@@ -1045,12 +1052,30 @@ __global__ void __launch_bounds__(LB) bs_z_kernel(long long N, Dims3 fd, Dims3 c
                                                   const float* w1, float* y, const Scal* S) {
     if (S->done) return;
     const long long T = (long long)gridDim.x * LB, t0 = blockIdx.x * (long long)LB + threadIdx.x, NQ = N >> 2;
+    // lattice coordinates of cell 4q, stepped with the loop (no division inside it)
+    const unsigned n0 = (unsigned)fd.n0, n1 = (unsigned)fd.n1;
+    const unsigned step = (unsigned)(4 * T), stepRows = step / n0, dI = step - stepRows * n0;
+    const unsigned dK = stepRows / n1, dJ = stepRows - dK * n1;
+    int fi, fj, fk;
+    {
+        const unsigned f0 = (unsigned)(4 * t0), rows = f0 / n0;
+        fi = (int)(f0 - rows * n0);
+        fk = (int)(rows / n1);
+        fj = (int)(rows - (unsigned)fk * n1);
+    }
     for (long long q = t0; q < NQ; q += T) {
         float X[4], D[4], Y[4];
         uint8_t F[4];
         un4(ld4(x, q), X); un4(ld4(invD, q), D); st_flags4(st, q, F);
         float PW[4] = {0.f, 0.f, 0.f, 0.f};
-        if (w1) prolong4(fd, cd, w1, q, PW);
+        if (w1) prolong4_ijk(fd, cd, w1, (unsigned)(4 * q), fi, fj, fk, PW);
+        fi += (int)dI;
+        const int carry = fi >= fd.n0;
+        if (carry) fi -= fd.n0;
+        fj += (int)dJ + carry;
+        const int carryJ = fj >= fd.n1;
+        if (carryJ) fj -= fd.n1;
+        fk += (int)dK + carryJ;
 #pragma unroll
         for (int m = 0; m < 4; ++m) {
             if (F[m] == ST_INACTIVE) Y[m] = 0.f;
