@@ -1179,97 +1179,6 @@ __global__ void __launch_bounds__(LB) bs_spmv_kernel(OpSymF32 A, long long N, co
         }
     }
 }
-// The same v = A x and dots as bs_spmv_kernel<true>, by CTAs that own 128 (i) x 8 (j) cells and
-// walk a slab of KZ planes along k: x of planes k-1 and k and the top coefficients of plane k-1
-// stay in registers from one plane to the next, the j neighbours' x and north coefficients come
-// from the tile staged in shared memory (global loads only on the tile's edge rows), the i
-// neighbours from the adjacent lanes (shuffles).  Six float4 loads per 4 cells and plane instead
-// of eleven.  The stencil sum keeps spmv4's order.
-constexpr int KM_QX = 32, KM_RY = 8;
-// a one-dimensional grid of gx * gy * gz tiles (block b: tile b mod gx along i, (b / gx) mod gy along
-// j, b / (gx gy) along k), so that the partial sums and the last-block test see one block index
-__global__ void __launch_bounds__(256, 4) bs_spmv_km_kernel(OpSymF32 A, int nI, int nJ, int nK, int KZ, int gx, int gy, const float* x,
-                                                         float* out, const float* a1, const float* b2, double* part, Scal* S, unsigned* ctr) {
-    if (S->done) return;
-    __shared__ float4 sx[KM_RY][KM_QX];
-    __shared__ float4 sn[KM_RY][KM_QX];
-    const int lane = threadIdx.x & 31, row = threadIdx.x >> 5;
-    const int nQ = nI >> 2;
-    const int bx = (int)(blockIdx.x % (unsigned)gx), by = (int)((blockIdx.x / (unsigned)gx) % (unsigned)gy);
-    const int bz = (int)(blockIdx.x / ((unsigned)gx * (unsigned)gy));
-    const int iq = bx * KM_QX + lane;
-    const int j = by * KM_RY + row;
-    const int k0 = bz * KZ, k1 = min(k0 + KZ, nK);
-    const bool in = iq < nQ && j < nJ;
-    const long long qI = nQ, qIJ = (long long)nQ * nJ;
-    const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
-    const float4* X4 = reinterpret_cast<const float4*>(x);
-    double a[2] = {0., 0.};
-    long long q = in ? ((long long)k0 * nJ + j) * qI + iq : 0;
-    float4 xm = in ? X4[q - qIJ] : z4, xc = in ? X4[q] : z4, tm = in ? ld4(A.aT, q - qIJ) : z4;
-    for (int k = k0; k < k1; ++k, q += qIJ) {
-        float4 P = z4, E = z4, Nn = z4, T = z4, xp = z4;
-        if (in) { P = ld4(A.aP, q); E = ld4(A.aE, q); Nn = ld4(A.aN, q); T = ld4(A.aT, q); xp = X4[q + qIJ]; }
-        sx[row][lane] = xc;
-        sn[row][lane] = Nn;
-        __syncthreads();
-        float4 XN = z4, XS = z4, SN = z4;
-        if (in) {
-            XN = row + 1 < KM_RY ? sx[row + 1][lane] : X4[q + qI];
-            XS = row > 0 ? sx[row - 1][lane] : X4[q - qI];
-            SN = row > 0 ? sn[row - 1][lane] : ld4(A.aN, q - qI);
-        }
-        float xl = __shfl_up_sync(0xffffffffu, xc.w, 1), wl = __shfl_up_sync(0xffffffffu, E.w, 1);
-        float xr = __shfl_down_sync(0xffffffffu, xc.x, 1);
-        const long long c = 4 * q;
-        if (in && lane == 0) { xl = x[c - 1]; wl = __ldg(A.aE + c - 1); }
-        if (in && (lane == 31 || iq + 1 >= nQ)) xr = x[c + 4];
-        float Pv[4], Ev[4], Nv[4], Tv[4], Sv[4], Bv[4], Xv[4], XNv[4], XSv[4], XTv[4], XBv[4];
-        un4(P, Pv); un4(E, Ev); un4(Nn, Nv); un4(T, Tv); un4(SN, Sv); un4(tm, Bv); un4(xc, Xv); un4(XN, XNv); un4(XS, XSv);
-        un4(xp, XTv); un4(xm, XBv);
-        const float W[4] = {wl, Ev[0], Ev[1], Ev[2]};
-        const float xL[4] = {xl, Xv[0], Xv[1], Xv[2]};
-        const float xR[4] = {Xv[1], Xv[2], Xv[3], xr};
-        float Y[4];
-#pragma unroll
-        for (int m = 0; m < 4; ++m)
-            Y[m] = Pv[m] * Xv[m] + Ev[m] * xR[m] + W[m] * xL[m] + Nv[m] * XNv[m] + Sv[m] * XSv[m] + Tv[m] * XTv[m] + Bv[m] * XBv[m];
-        if (in) {
-            if (A.gh.n > 0) {
-                const uint32_t bits = (__ldg(A.gh.bits + (c >> 5)) >> (c & 31)) & 0xFu;
-                if (bits)
-#pragma unroll
-                    for (int m = 0; m < 4; ++m)
-                        if ((bits >> m) & 1u) Y[m] = applyF(A, c + m, [&](long long e_) { return x[e_]; });
-            }
-            st4(out, q, Y);
-            if (b2) {
-                float Bb[4];
-                un4(ld4(b2, q), Bb);
-#pragma unroll
-                for (int m = 0; m < 4; ++m) { a[0] += (double)Bb[m] * Y[m]; a[1] += (double)Y[m] * Y[m]; }
-            } else {
-                float Av[4];
-                un4(ld4(a1, q), Av);
-#pragma unroll
-                for (int m = 0; m < 4; ++m) a[0] += (double)Av[m] * Y[m];
-            }
-        }
-        __syncthreads();
-        xm = xc; xc = xp; tm = T;
-    }
-    block_sums(a, b2 ? 2 : 1, part);
-    if (ctr && last_block(ctr)) {
-        double t[2];
-        totals_cg(part, gridDim.x, b2 ? 2 : 1, t);
-        if (threadIdx.x == 0) {
-            if (b2) fin_omega(t, S);
-            else fin_alpha(t, S);
-            *ctr = 0u;
-        }
-    }
-}
-
 // s = r - alpha v; partial sum of (D^-1 s)^2 over active cells
 __global__ void __launch_bounds__(LB) bs_s_kernel(long long N, const float* r, const float* v, const float* invD, const uint8_t* st, float* s,
                                                   double* part, Scal* S, unsigned* ctr, float* uo) {
@@ -1808,22 +1717,6 @@ int learned_solve(LearnedWork& lw, const OpSym& A, const uint8_t* status, const 
     const bool nonsym = A.gh.n > 0;
     // 4-cell vector rows: neighbouring groups of 4 cells stay 16-byte aligned
     const bool v4 = (L.nI % 4) == 0 && (L.nIJ % 4) == 0;
-    // the k-marching SpMV: tiles of 128 x 8 cells, slabs of planes sized so that the blocks fit the
-    // MAXP partial slots (at least 8 planes per slab, so that the carried planes pay)
-    struct { bool ok; int gx, gy, KZ, blocks; } km = {false, 0, 0, 0, 0};
-    if (v4) {
-        km.gx = (L.nI / 4 + KM_QX - 1) / KM_QX;
-        km.gy = (L.nJ + KM_RY - 1) / KM_RY;
-        const long long gxy = (long long)km.gx * km.gy;
-        if (gxy <= MAXP) {
-            long long gz = std::min<long long>((L.nK + 7) / 8, MAXP / gxy);
-            if (gz < 1) gz = 1;
-            km.KZ = (int)((L.nK + gz - 1) / gz);
-            gz = (L.nK + km.KZ - 1) / km.KZ;
-            km.blocks = (int)(gxy * gz);
-            km.ok = km.blocks <= MAXP;
-        }
-    }
     int method = lw.inner;
     if (method == LEARN_INNER_AUTO)
         method = !nonsym ? LEARN_INNER_FCG : (mode == NET_MODE_NETWORK ? LEARN_INNER_FGMRES : LEARN_INNER_BICGSTAB);
@@ -1937,16 +1830,12 @@ int learned_solve(LearnedWork& lw, const OpSym& A, const uint8_t* status, const 
                         bs_dir_kernel<<<nb, LB, 0, st>>>(N, lw.r, lw.q[0], lw.invD, status, lw.p[0], lw.part, S, lw.ctr, lw.u1);
                         if (apply_levels(lw, lw.p[0], status, mode, S, st, lw.u1)) return 1;
                         bs_z_kernel<<<nb, LB, 0, st>>>(N, fd, cd, lw.p[0], lw.invD, status, w1, lw.p[1], S, lw.u1);
-                        if (km.ok) bs_spmv_km_kernel<<<km.blocks, 256, 0, st>>>(Af, L.nI, L.nJ, L.nK, km.KZ, km.gx, km.gy, lw.p[1], lw.q[0],
-                                                                                lw.rh, nullptr, lw.part, S, lw.ctr);
-                        else if (v4) bs_spmv_kernel<true><<<nb, LB, 0, st>>>(Af, N, lw.p[1], lw.q[0], lw.rh, nullptr, lw.part, S, lw.ctr);
+                        if (v4) bs_spmv_kernel<true><<<nb, LB, 0, st>>>(Af, N, lw.p[1], lw.q[0], lw.rh, nullptr, lw.part, S, lw.ctr);
                         else bs_spmv_kernel<false><<<nb, LB, 0, st>>>(Af, N, lw.p[1], lw.q[0], lw.rh, nullptr, lw.part, S, lw.ctr);
                         bs_s_kernel<<<nb, LB, 0, st>>>(N, lw.r, lw.q[0], lw.invD, status, lw.z, lw.part, S, lw.ctr, lw.u1);
                         if (apply_levels(lw, lw.z, status, mode, S, st, lw.u1)) return 1;
                         bs_z_kernel<<<nb, LB, 0, st>>>(N, fd, cd, lw.z, lw.invD, status, w1, lw.q[1], S, lw.u1);
-                        if (km.ok) bs_spmv_km_kernel<<<km.blocks, 256, 0, st>>>(Af, L.nI, L.nJ, L.nK, km.KZ, km.gx, km.gy, lw.q[1], lw.t,
-                                                                                nullptr, lw.z, lw.part, S, lw.ctr);
-                        else if (v4) bs_spmv_kernel<true><<<nb, LB, 0, st>>>(Af, N, lw.q[1], lw.t, nullptr, lw.z, lw.part, S, lw.ctr);
+                        if (v4) bs_spmv_kernel<true><<<nb, LB, 0, st>>>(Af, N, lw.q[1], lw.t, nullptr, lw.z, lw.part, S, lw.ctr);
                         else bs_spmv_kernel<false><<<nb, LB, 0, st>>>(Af, N, lw.q[1], lw.t, nullptr, lw.z, lw.part, S, lw.ctr);
                         bs_update_kernel<<<nb, LB, 0, st>>>(N, lw.e, lw.r, lw.p[1], lw.q[1], lw.z, lw.t, lw.rh, lw.part, S, lw.ctr, maxit);
                     }
