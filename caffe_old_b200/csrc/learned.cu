@@ -1048,10 +1048,8 @@ __global__ void scale_finish(const double* part, int nblk, Scal* S) {
     if (threadIdx.x == 0) fin_scale(t, S);
 }
 // y = M(x) on the cell lattice: D^-1 x + P w_1 on active cells, D^-1 x on ghost rows, 0 on inactive cells
-// u (optional): D^-1 x on active cells, 0 elsewhere, as the kernel that produced x wrote it; then
-// x and 1/diag are read for ghost rows only
 __global__ void __launch_bounds__(LB) bs_z_kernel(long long N, Dims3 fd, Dims3 cd, const float* x, const float* invD, const uint8_t* st,
-                                                  const float* w1, float* y, const Scal* S, const float* u) {
+                                                  const float* w1, float* y, const Scal* S) {
     if (S->done) return;
     const long long T = (long long)gridDim.x * LB, t0 = blockIdx.x * (long long)LB + threadIdx.x, NQ = N >> 2;
     // lattice coordinates of cell 4q, stepped with the loop (no division inside it)
@@ -1068,18 +1066,7 @@ __global__ void __launch_bounds__(LB) bs_z_kernel(long long N, Dims3 fd, Dims3 c
     for (long long q = t0; q < NQ; q += T) {
         float X[4], D[4], Y[4];
         uint8_t F[4];
-        st_flags4(st, q, F);
-        if (u) {
-            float U[4];
-            un4(ld4(u, q), U);
-            const bool ghost = F[0] == ST_GHOST || F[1] == ST_GHOST || F[2] == ST_GHOST || F[3] == ST_GHOST;
-            if (ghost) { un4(ld4(x, q), X); un4(ld4(invD, q), D); }
-#pragma unroll
-            for (int m = 0; m < 4; ++m)
-                if (F[m] == ST_ACTIVE || !ghost) { X[m] = U[m]; D[m] = 1.f; }
-        } else {
-            un4(ld4(x, q), X); un4(ld4(invD, q), D);
-        }
+        un4(ld4(x, q), X); un4(ld4(invD, q), D); st_flags4(st, q, F);
         float PW[4] = {0.f, 0.f, 0.f, 0.f};
         if (w1) prolong4_ijk(fd, cd, w1, (unsigned)(4 * q), fi, fj, fk, PW);
         fi += (int)dI;
@@ -1778,7 +1765,7 @@ int learned_solve(LearnedWork& lw, const OpSym& A, const uint8_t* status, const 
                     scale_partial_kernel<<<nb, LB, 0, st>>>(N, vj, lw.invD, status, lw.part, S, lw.u1);
                     scale_finish<<<1, LB, 0, st>>>(lw.part, nb, S);
                     if (apply_levels(lw, vj, status, mode, S, st, lw.u1)) return 1;
-                    bs_z_kernel<<<nb, LB, 0, st>>>(N, fd, cd, vj, lw.invD, status, w1, zj, S, lw.u1);
+                    bs_z_kernel<<<nb, LB, 0, st>>>(N, fd, cd, vj, lw.invD, status, w1, zj, S);
                     if (v4) fg_spmv_kernel<true><<<nb, LB, 0, st>>>(Af, N, zj, lw.t, S);
                     else fg_spmv_kernel<false><<<nb, LB, 0, st>>>(Af, N, zj, lw.t, S);
                     // classical Gram-Schmidt with one re-orthogonalisation (CGS2): FP32 vectors lose
@@ -1829,12 +1816,12 @@ int learned_solve(LearnedWork& lw, const OpSym& A, const uint8_t* status, const 
                         // p = p[0], v = q[0], ph = p[1], sh = q[1], s = z, t = t
                         bs_dir_kernel<<<nb, LB, 0, st>>>(N, lw.r, lw.q[0], lw.invD, status, lw.p[0], lw.part, S, lw.ctr, lw.u1);
                         if (apply_levels(lw, lw.p[0], status, mode, S, st, lw.u1)) return 1;
-                        bs_z_kernel<<<nb, LB, 0, st>>>(N, fd, cd, lw.p[0], lw.invD, status, w1, lw.p[1], S, lw.u1);
+                        bs_z_kernel<<<nb, LB, 0, st>>>(N, fd, cd, lw.p[0], lw.invD, status, w1, lw.p[1], S);
                         if (v4) bs_spmv_kernel<true><<<nb, LB, 0, st>>>(Af, N, lw.p[1], lw.q[0], lw.rh, nullptr, lw.part, S, lw.ctr);
                         else bs_spmv_kernel<false><<<nb, LB, 0, st>>>(Af, N, lw.p[1], lw.q[0], lw.rh, nullptr, lw.part, S, lw.ctr);
                         bs_s_kernel<<<nb, LB, 0, st>>>(N, lw.r, lw.q[0], lw.invD, status, lw.z, lw.part, S, lw.ctr, lw.u1);
                         if (apply_levels(lw, lw.z, status, mode, S, st, lw.u1)) return 1;
-                        bs_z_kernel<<<nb, LB, 0, st>>>(N, fd, cd, lw.z, lw.invD, status, w1, lw.q[1], S, lw.u1);
+                        bs_z_kernel<<<nb, LB, 0, st>>>(N, fd, cd, lw.z, lw.invD, status, w1, lw.q[1], S);
                         if (v4) bs_spmv_kernel<true><<<nb, LB, 0, st>>>(Af, N, lw.q[1], lw.t, nullptr, lw.z, lw.part, S, lw.ctr);
                         else bs_spmv_kernel<false><<<nb, LB, 0, st>>>(Af, N, lw.q[1], lw.t, nullptr, lw.z, lw.part, S, lw.ctr);
                         bs_update_kernel<<<nb, LB, 0, st>>>(N, lw.e, lw.r, lw.p[1], lw.q[1], lw.z, lw.t, lw.rh, lw.part, S, lw.ctr, maxit);
