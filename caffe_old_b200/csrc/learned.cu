@@ -397,6 +397,7 @@ constexpr int RT_F_BYTES = RT_BX * RFJ * RFK * 4;            // 28800
 constexpr int RT_S_BYTES = RT_BXS * RFJ * RFK;               // 9600
 constexpr int RT_STAGE_BYTES = 2 * RT_F_BYTES + RT_S_BYTES;  // 67200
 constexpr int RT_THREADS = 1024;
+static_assert(RT_THREADS % (RCI * RCJ) == 0 && RT_THREADS >= RCK * RCJ * RCI, "restriction thread layout");
 constexpr long long RT_WAIT_LIMIT = 1ll << 22;               // polls (each at most a short hardware wait)
 
 __device__ __forceinline__ uint32_t rt_smem(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -505,25 +506,34 @@ __global__ void __launch_bounds__(RT_THREADS, 2) restrict_tma_kernel(const __gri
             }
             __syncthreads();
         }
-        for (int u = threadIdx.x; u < RFK * RFJ * RCI; u += RT_THREADS) {
-            const int ci = u % RCI, row = u / RCI;
-            const float* v = sf + row * RT_BX + 3 + 2 * ci;
-            t1[row / RFJ][row % RFJ][ci] = wI[ci][0] * v[0] + wI[ci][1] * v[1] + wI[ci][2] * v[2] + wI[ci][3] * v[3];
+        // each thread keeps one coarse column ci (RT_THREADS is a multiple of RCI * RCJ * 8), so its
+        // weights stay in registers; the four fine values of pass 1 come as three aligned float2
+        const int ci = threadIdx.x & (RCI - 1);
+        {
+            const float w0 = wI[ci][0], w1 = wI[ci][1], w2 = wI[ci][2], w3 = wI[ci][3];
+            float* T1 = &t1[0][0][0];
+            for (int row = threadIdx.x >> 5; row < RFK * RFJ; row += RT_THREADS / RCI) {
+                const float2* v2 = reinterpret_cast<const float2*>(sf + row * RT_BX + 2 + 2 * ci);   // fine 2I-2 .. 2I+3
+                const float2 a = v2[0], b = v2[1], c = v2[2];
+                T1[row * RCI + ci] = w0 * a.y + w1 * b.x + w2 * b.y + w3 * c.x;
+            }
         }
         __syncthreads();
-        for (int u = threadIdx.x; u < RFK * RCJ * RCI; u += RT_THREADS) {
-            const int ci = u % RCI, cj = (u / RCI) % RCJ, lk = u / (RCI * RCJ);
-            t2[lk][cj][ci] = wJ[cj][0] * t1[lk][2 * cj][ci] + wJ[cj][1] * t1[lk][2 * cj + 1][ci] + wJ[cj][2] * t1[lk][2 * cj + 2][ci] +
-                             wJ[cj][3] * t1[lk][2 * cj + 3][ci];
+        {
+            const int cj = (threadIdx.x >> 5) & (RCJ - 1);
+            const float w0 = wJ[cj][0], w1 = wJ[cj][1], w2 = wJ[cj][2], w3 = wJ[cj][3];
+            for (int lk = threadIdx.x / (RCI * RCJ); lk < RFK; lk += RT_THREADS / (RCI * RCJ))
+                t2[lk][cj][ci] = w0 * t1[lk][2 * cj][ci] + w1 * t1[lk][2 * cj + 1][ci] + w2 * t1[lk][2 * cj + 2][ci] + w3 * t1[lk][2 * cj + 3][ci];
         }
         __syncthreads();
-        for (int u = threadIdx.x; u < RCK * RCJ * RCI; u += RT_THREADS) {
-            const int ci = u % RCI, cj = (u / RCI) % RCJ, ck = u / (RCI * RCJ);
+        if (threadIdx.x < RCK * RCJ * RCI) {
+            const int cj = (threadIdx.x >> 5) & (RCJ - 1), ck = threadIdx.x / (RCI * RCJ);
             const int I = I0 + ci, J = J0 + cj, K = K0 + ck;
-            if (I >= cd.n0 || J >= cd.n1 || K >= cd.n2) continue;
-            const float acc = wK[ck][0] * t2[2 * ck][cj][ci] + wK[ck][1] * t2[2 * ck + 1][cj][ci] + wK[ck][2] * t2[2 * ck + 2][cj][ci] +
-                              wK[ck][3] * t2[2 * ck + 3][cj][ci];
-            out[((unsigned)K * (unsigned)cd.n1 + (unsigned)J) * (unsigned)cd.n0 + (unsigned)I] = acc * scale;
+            if (I < cd.n0 && J < cd.n1 && K < cd.n2) {
+                const float acc = wK[ck][0] * t2[2 * ck][cj][ci] + wK[ck][1] * t2[2 * ck + 1][cj][ci] + wK[ck][2] * t2[2 * ck + 2][cj][ci] +
+                                  wK[ck][3] * t2[2 * ck + 3][cj][ci];
+                out[((unsigned)K * (unsigned)cd.n1 + (unsigned)J) * (unsigned)cd.n0 + (unsigned)I] = acc * scale;
+            }
         }
         __syncthreads();
     }
