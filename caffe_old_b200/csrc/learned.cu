@@ -1134,7 +1134,7 @@ __device__ __forceinline__ void spmv4(const OpSymF32& A, const float* x, long lo
 
 // out = A x; partial (a1, out), or with b2: (b2, out) and (out, out)
 template <bool V4>
-__global__ void __launch_bounds__(LB) bs_spmv_kernel(OpSymF32 A, long long N, const float* x, float* out, const float* a1, const float* b2,
+__global__ void __launch_bounds__(LB, 5) bs_spmv_kernel(OpSymF32 A, long long N, const float* x, float* out, const float* a1, const float* b2,
                                                      double* part, Scal* S, unsigned* ctr) {
     if (S->done) return;
     double a[2] = {0., 0.};
