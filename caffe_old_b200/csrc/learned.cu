@@ -625,6 +625,9 @@ int launch_restrict_tma(const Dims3& fd, const Dims3& cd, const float* fin, cons
     return 0;
 }
 
+inline long long restrict_tiles(const Dims3& cd) {
+    return (long long)((cd.n0 + RCI - 1) / RCI) * ((cd.n1 + RCJ - 1) / RCJ) * ((cd.n2 + RCK - 1) / RCK);
+}
 inline dim3 restrict_grid(const Dims3& cd) {
     return dim3((unsigned)((cd.n0 + RCI - 1) / RCI), (unsigned)((cd.n1 + RCJ - 1) / RCJ), (unsigned)((cd.n2 + RCK - 1) / RCK));
 }
@@ -1535,6 +1538,13 @@ int apply_levels(LearnedWork& lw, const float* rfine, const uint8_t* status, int
         }
         if (l == 1 && !netAt(1) && lw.rtErr && restrict_tma_usable(dims_of(f), rfine, lw.invD, status)) {
             if (launch_restrict_tma(dims_of(f), dims_of(c), rfine, lw.invD, status, c.rscale, c.u, lw.rtErr, S, st)) return 1;
+            continue;
+        }
+        // deeper levels: the input is already plain values, the staged form of the restriction
+        // applies where the level has tiles enough for two per SM
+        if (l >= 2 && !netAt(l) && lw.rtErr && restrict_tiles(dims_of(c)) >= 2 * 148 &&
+            restrict_tma_usable(dims_of(f), f.u, nullptr, nullptr)) {
+            if (launch_restrict_tma(dims_of(f), dims_of(c), f.u, nullptr, nullptr, c.rscale, c.u, lw.rtErr, S, st)) return 1;
             continue;
         }
         restrict_kernel<<<restrict_grid(dims_of(c)), 256, 0, st>>>(dims_of(f), dims_of(c), l == 1 ? rfine : f.u, l == 1 ? lw.invD : nullptr,
