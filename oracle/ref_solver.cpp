@@ -1,5 +1,6 @@
 // Driver of the reference's own solver code (test infrastructure): src/Solvers/Simple.cpp,
-// Piso.cpp and IbPiso.cpp with the mesh, fields, schemes and math they use, compiled from the
+// Piso.cpp, IbPiso.cpp, Coupled.cpp and Diffusion.cpp with the mesh, fields, schemes and math they
+// use, compiled from the
 // reference's sources where they lie (oracle/Makefile, target refsolver) against the stand-in
 // headers in refshim/include.  A case is set up the way the reference's module mains do it
 // (Modules/caffeSimple.cpp:13-30): Input reads case/case.info, the mesh is built from a node
@@ -15,6 +16,8 @@
 #include <string>
 #include <vector>
 
+#include "Coupled.h"
+#include "Diffusion.h"
 #include "IbPiso.h"
 #include "Interpolation.h"
 #include "Parallel.h"
@@ -36,6 +39,22 @@ struct Open : B {
     Field<Vector3D>& gradP() { return this->gradPField_; }
 };
 
+// the Coupled and Diffusion solvers' fields (protected members)
+struct OpenCoupled : Coupled {
+    OpenCoupled(const Input& in, const HexaFvmMesh& m) : Coupled(in, m) {}
+    Field<Vector3D>& u() { return uField_; }
+    Field<double>& p() { return pField_; }
+    Field<double>& d() { return dField_; }
+    Field<double>& mf() { return massFlowField_; }
+    Field<Vector3D>& gradP() { return gradPField_; }
+    Field<Vector3D>& h() { return hField_; }
+};
+struct OpenDiffusion : Diffusion {
+    OpenDiffusion(const Input& in, const HexaFvmMesh& m) : Diffusion(in, m) {}
+    Field<double>& phi() { return phiField_; }
+    Field<Vector3D>& gradPhi() { return gradPhiField_; }
+};
+
 struct Run {
     std::unique_ptr<Input> input;
     std::unique_ptr<HexaFvmMesh> mesh;
@@ -43,7 +62,7 @@ struct Run {
     int kind = 0;
     int nI = 0, nJ = 0, nK = 0;
     template <class F>
-    auto with(F&& f) {
+    auto with(F&& f) {   // kinds 0-2: the flow solvers
         if (kind == 0) return f(*static_cast<Open<Simple>*>(solver.get()));
         if (kind == 1) return f(*static_cast<Open<Piso>*>(solver.get()));
         return f(*static_cast<Open<IbPiso>*>(solver.get()));
@@ -108,7 +127,9 @@ void* refsolver_create(const char* casedir, const double* nodes, int nNI, int nN
         r->mesh->initialize(pts);
         if (kind == 0) r->solver.reset(new Open<Simple>(*r->input, *r->mesh));
         else if (kind == 1) r->solver.reset(new Open<Piso>(*r->input, *r->mesh));
-        else r->solver.reset(new Open<IbPiso>(*r->input, *r->mesh));
+        else if (kind == 2) r->solver.reset(new Open<IbPiso>(*r->input, *r->mesh));
+        else if (kind == 3) r->solver.reset(new OpenCoupled(*r->input, *r->mesh));
+        else r->solver.reset(new OpenDiffusion(*r->input, *r->mesh));
         r->nI = nNI - 1; r->nJ = nNJ - 1; r->nK = nNK - 1;
     } catch (const char* msg) {
         g_err = msg;
@@ -135,6 +156,22 @@ void refsolver_destroy(void* h) { delete static_cast<Run*>(h); }
 int refsolver_zero_pressure_patch(void* h, int face) {
     Run* r = static_cast<Run*>(h);
     if (face < 0 || face > 5) return 1;
+    if (r->kind == 3) {
+        Field<double>& p = static_cast<OpenCoupled*>(r->solver.get())->p();
+        Array3D<double>* patch[6] = {&p.eastBoundaryPatch, &p.westBoundaryPatch, &p.northBoundaryPatch,
+                                     &p.southBoundaryPatch, &p.topBoundaryPatch, &p.bottomBoundaryPatch};
+        patch[face]->assign(0.);
+        switch (face) {
+            case 0: p.setEastFacesFromPatch(); break;
+            case 1: p.setWestFacesFromPatch(); break;
+            case 2: p.setNorthFacesFromPatch(); break;
+            case 3: p.setSouthFacesFromPatch(); break;
+            case 4: p.setTopFacesFromPatch(); break;
+            default: p.setBottomFacesFromPatch(); break;
+        }
+        return 0;
+    }
+    if (r->kind > 3) return 1;
     return r->with([&](auto& s) -> int {
         Field<double>& p = s.p();
         Array3D<double>* patch[6] = {&p.eastBoundaryPatch, &p.westBoundaryPatch, &p.northBoundaryPatch,
@@ -165,7 +202,8 @@ double refsolver_solve(void* h, double dt) {
     return std::nan("");
 }
 
-// "u" (N x 3), "gradP" (N x 3), "p", "pCorr", "d", "massFlow" (cells), "massFlowI/J/K" (faces)
+// "u" (N x 3), "gradP" (N x 3), "p", "pCorr", "d", "massFlow" (cells), "massFlowI/J/K" (faces); the
+// Coupled solver: "u", "gradP", "h", "p", "d", "massFlowI/J/K"; Diffusion: "phi", "gradPhi", "phiFaceI/J/K"
 long refsolver_field(void* h, const char* name, double* out, long count) {
     Run* r = static_cast<Run*>(h);
     std::string n(name);
@@ -196,6 +234,27 @@ long refsolver_field(void* h, const char* name, double* out, long count) {
                     }
         return need;
     };
+    if (r->kind == 3) {
+        OpenCoupled& s = *static_cast<OpenCoupled*>(r->solver.get());
+        if (n == "u") return cells(s.u(), 3);
+        if (n == "gradP") return cells(s.gradP(), 3);
+        if (n == "h") return cells(s.h(), 3);
+        if (n == "p") return cells(s.p(), 1);
+        if (n == "d") return cells(s.d(), 1);
+        if (n == "massFlowI") return faces(s.mf(), 0);
+        if (n == "massFlowJ") return faces(s.mf(), 1);
+        if (n == "massFlowK") return faces(s.mf(), 2);
+        return -1L;
+    }
+    if (r->kind == 4) {
+        OpenDiffusion& s = *static_cast<OpenDiffusion*>(r->solver.get());
+        if (n == "phi") return cells(s.phi(), 1);
+        if (n == "gradPhi") return cells(s.gradPhi(), 3);
+        if (n == "phiFaceI") return faces(s.phi(), 0);
+        if (n == "phiFaceJ") return faces(s.phi(), 1);
+        if (n == "phiFaceK") return faces(s.phi(), 2);
+        return -1L;
+    }
     return r->with([&](auto& s) -> long {
         if (n == "u") return cells(s.u(), 3);
         if (n == "gradP") return cells(s.gradP(), 3);

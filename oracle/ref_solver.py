@@ -2,8 +2,9 @@
 LAPACKE / Boost headers (oracle/Makefile target ``refsolver`` -> oracle/_ref/libref_solver.so).
 
 Test infrastructure: it pins the oracle's restatement of Simple / Piso / IbPiso
-(src/Solvers/Simple.cpp:78-449, Piso.cpp:12-29, IbPiso.cpp:43-190) to the reference's own
-arithmetic.  The library exists only where the reference's sources do (it is built from them
+(src/Solvers/Simple.cpp:78-449, Piso.cpp:12-29, IbPiso.cpp:43-190), Coupled
+(src/Solvers/Coupled.cpp:5-339) and Diffusion (src/Solvers/Diffusion.cpp:35-131) to the
+reference's own arithmetic.  The library exists only where the reference's sources do (it is built from them
 where they lie); tests skip when it is absent and fall back to the committed golden vectors.
 
 A case is written as the reference's case/case.info and case/initialConditions.info, the way
@@ -26,7 +27,7 @@ LIB_PATH = os.path.join(_HERE, "_ref", "libref_solver.so")
 _lib = None
 
 FACES = ("east", "west", "north", "south", "top", "bottom")
-KINDS = {"simple": 0, "piso": 1, "ibpiso": 2}
+KINDS = {"simple": 0, "piso": 1, "ibpiso": 2, "coupled": 3, "diffusion": 4}
 
 
 def available() -> bool:
@@ -92,25 +93,46 @@ def case_files(spec, directory: str) -> None:
         fh.write("\n".join(ic) + "\n")
 
 
-class RefSolver:
-    """The reference's Simple / Piso / IbPiso on a node array (nK+1, nJ+1, nI+1, 3)."""
+def diffusion_case_files(types, refs, time_accurate: bool, phi0: float, directory: str) -> None:
+    """case/case.info and case/initialConditions.info of the reference's Diffusion solver: face
+    types fixed / zeroGradient / empty with their reference values, a uniform phi."""
+    os.makedirs(os.path.join(directory, "case"), exist_ok=True)
+    lines = ["Solver", "{", f"  timeAccurate {'ON' if time_accurate else 'OFF'}", "}", "Boundaries", "{"]
+    for f, name in enumerate(FACES):
+        lines += [f"  {name}", "  {", f"    type {types[f]}", f"    refValue {float(refs[f])!r}", "  }"]
+    lines.append("}")
+    with open(os.path.join(directory, "case", "case.info"), "w") as fh:
+        fh.write("\n".join(lines) + "\n")
+    with open(os.path.join(directory, "case", "initialConditions.info"), "w") as fh:
+        fh.write("\n".join(["phi", "{", "  type uniform", f"  value {float(phi0)!r}", "}"]) + "\n")
 
-    def __init__(self, nodes: np.ndarray, spec, rtol: float = 1e-13, maxit: int = 200000, record: bool = False):
+
+class RefSolver:
+    """The reference's Simple / Piso / IbPiso (the spec's kind), Coupled (kind="coupled") or
+    Diffusion (kind="diffusion", with `diffusion` = (types, refs, time_accurate, phi0)) on a
+    node array (nK+1, nJ+1, nI+1, 3)."""
+
+    def __init__(self, nodes: np.ndarray, spec, rtol: float = 1e-13, maxit: int = 200000, record: bool = False,
+                 kind: str | None = None, diffusion=None):
         L = lib()
         L.refsolver_set_tolerance(float(rtol), int(maxit))
         L.refsolver_record(1 if record else 0)
         self.spec = spec
+        self.kind = kind or spec.kind
         self.nodes = np.ascontiguousarray(nodes, dtype=np.float64)
         self.shape = (self.nodes.shape[2] - 1, self.nodes.shape[1] - 1, self.nodes.shape[0] - 1)
         self._dir = tempfile.TemporaryDirectory(prefix="caffe_ref_case_")
-        case_files(spec, self._dir.name)
+        if self.kind == "diffusion":
+            diffusion_case_files(*diffusion, self._dir.name)
+        else:
+            case_files(spec, self._dir.name)
         self._h = L.refsolver_create(self._dir.name.encode(), self.nodes.ctypes.data_as(ctypes.c_void_p),
-                                     self.nodes.shape[2], self.nodes.shape[1], self.nodes.shape[0], KINDS[spec.kind])
+                                     self.nodes.shape[2], self.nodes.shape[1], self.nodes.shape[0], KINDS[self.kind])
         if not self._h:
             raise RuntimeError("reference solver set-up failed: " + L.refsolver_last_error().decode())
         # faces without a fixed pressure start from the zero that zero-initialised memory gives in
         # place of the reference's uninitialised refValues_ (see refsolver_zero_pressure_patch)
-        if any(t == "outlet" for t in spec.bc):
+        if self.kind != "diffusion" and any(t == "outlet" for t in spec.bc):
             for f, t in enumerate(spec.bc):
                 if t != "outlet":
                     L.refsolver_zero_pressure_patch(self._h, f)
@@ -128,7 +150,7 @@ class RefSolver:
             pass
 
     def solve(self, dt: float | None = None) -> float:
-        v = lib().refsolver_solve(self._h, float(self.spec.dt if dt is None else dt))
+        v = lib().refsolver_solve(self._h, float(self.spec.dt if (dt is None and self.spec is not None) else (dt or 1.0)))
         if not np.isfinite(v) and lib().refsolver_last_error():
             raise RuntimeError("reference solve failed: " + lib().refsolver_last_error().decode())
         return float(v)
