@@ -302,7 +302,7 @@ def fgmres_bytes_per_cell(m: int) -> float:
 # DRAM bytes per cell and inner BiCGStab iteration of the fine-lattice kernels, from one ncu
 # capture (dram__bytes_read.sum + dram__bytes_write.sum of the 240x160x160 case, per cell);
 # traffic grows with the cell count
-LEARNED_TRAFFIC_PER_CELL = {"bicgstab": 154.0}
+LEARNED_TRAFFIC_PER_CELL = {"bicgstab": 143.0}
 
 
 def configure_precond(dev, args):
