@@ -65,7 +65,8 @@ class StepStats(ctypes.Structure):
 
 EXPORTS = (
     "caffe_last_error", "caffe_dev_create", "caffe_dev_destroy", "caffe_dev_solve", "caffe_dev_phase",
-    "caffe_dev_array", "caffe_dev_stats", "caffe_dev_stream", "caffe_dev_synchronize",
+    "caffe_dev_array", "caffe_dev_stats", "caffe_dev_stream", "caffe_dev_synchronize", "caffe_dev_set_stream",
+    "caffe_slab_set_owned", "caffe_slab_halo", "caffe_slab_ksp", "caffe_slab_phase", "caffe_slab_reduce",
     "caffe_ksp7_solve", "caffe_ksp7_solve_device", "caffe_ksp7_solve_device_noalloc", "caffe_csr_solve", "caffe_csr_matvec",
     "caffe_diffusion_create", "caffe_diffusion_destroy", "caffe_diffusion_solve", "caffe_diffusion_phase", "caffe_diffusion_array",
     "caffe_coupled_create", "caffe_coupled_destroy", "caffe_coupled_solve", "caffe_coupled_phase", "caffe_coupled_stats",
@@ -98,6 +99,13 @@ def lib():
     L.caffe_dev_stream.restype = vp
     L.caffe_dev_stream.argtypes = [vp]
     L.caffe_dev_synchronize.argtypes = [vp]
+    L.caffe_dev_set_stream.argtypes = [vp, vp]
+    L.caffe_slab_set_owned.argtypes = [vp, ci, ci]
+    L.caffe_slab_halo.restype = ctypes.c_long
+    L.caffe_slab_halo.argtypes = [vp, ctypes.c_char_p, ci, ci, ci, vp]
+    L.caffe_slab_ksp.argtypes = [vp, ci, ci, vp, vp]
+    L.caffe_slab_phase.argtypes = [vp, ctypes.c_char_p, cd]
+    L.caffe_slab_reduce.argtypes = [vp, ctypes.c_char_p, cd, vp]
     L.caffe_ksp7_solve.argtypes = [ci, ci, ci, vp, vp, vp, ci, cd, ci, ctypes.POINTER(ci), ctypes.POINTER(cd)]
     L.caffe_ksp7_solve_device.argtypes = [ci, ci, ci, vp, vp, vp, ci, cd, ci, vp, ctypes.POINTER(ci), ctypes.POINTER(cd)]
     L.caffe_ksp7_solve_device_noalloc.argtypes = [ci, ci, ci, vp, vp, vp, ci, cd, ci, vp, ctypes.POINTER(ci),

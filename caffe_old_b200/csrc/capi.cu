@@ -14,6 +14,7 @@
 #include "ib.cuh"
 #include "cnn.cuh"
 #include "learned.cuh"
+#include "slab.cuh"
 
 namespace cb {
 
@@ -177,6 +178,14 @@ struct caffe_dev {
     // event pairs around every linear solve of a step (device time of each solve)
     std::vector<cudaEvent_t> evP, evM;
     int nPTimed = 0, nMTimed = 0;
+    // k-slab decomposition: the owned cells [o0, o1) and the vectors of the distributed
+    // Krylov phases (set by caffe_slab_set_owned)
+    bool slab = false;
+    long long o0 = 0, o1 = 0;
+    double* slabPh = nullptr;
+    double* slabSh = nullptr;
+    double* slabPart = nullptr;
+    bool ownStream = true;   // false once the caller has handed in its own stream
 
     template <class T>
     T* dalloc(size_t count) {
@@ -273,7 +282,7 @@ struct caffe_dev {
         learned_free_host(lw);
         cudaFree(pairB); cudaFree(pairX);
         if (accHost) cudaFreeHost(accHost);
-        if (st) cudaStreamDestroy(st);
+        if (st && ownStream) cudaStreamDestroy(st);
     }
 };
 
@@ -456,7 +465,8 @@ int ph_solve_pcorr(caffe_dev* h) {
 int ph_correct(caffe_dev* h) {
     if (launch_correct(h->geo(), h->bc, h->fields(), h->P, h->st)) return 1;
     for (int q = 0; q < 3; ++q) std::swap(h->F[q], h->Fb[q]);
-    return launch_correct_post(h->geo(), h->bc, h->fields(), h->st);
+    // a slab forms grad u separately, after its u halo planes are exchanged
+    return launch_correct_post(h->geo(), h->bc, h->fields(), h->st, !h->slab);
 }
 int ph_continuity(caffe_dev* h) {
     return launch_continuity(h->L, h->mfc, h->vol, h->ib ? h->status : nullptr, h->chunkMax, &h->acc->continuity, h->st);
@@ -854,6 +864,145 @@ int caffe_dev_synchronize(caffe_dev* h) {
     if (!h) { set_error("handle is NULL"); return 1; }
     CB_CUDA(cudaStreamSynchronize(h->st));
     return 0;
+}
+
+int caffe_dev_set_stream(caffe_dev* h, void* stream) {
+    g_err.clear();
+    if (!h || !stream) { set_error("NULL argument"); return 1; }
+    CB_CUDA(cudaSetDevice(h->device));
+    CB_CUDA(cudaStreamSynchronize(h->st));
+    if (h->ownStream) CB_CUDA(cudaStreamDestroy(h->st));
+    h->st = static_cast<cudaStream_t>(stream);
+    h->ownStream = false;
+    return 0;
+}
+
+// ------------------------------------------------------------------ k-slab decomposition
+int caffe_slab_set_owned(caffe_dev* h, int k0, int k1) {
+    g_err.clear();
+    if (!h) { set_error("handle is NULL"); return 1; }
+    if (h->ib) { set_error("slab: the immersed-boundary solver is not decomposed"); return 1; }
+    if (h->cs.p_form != CAFFE_P_FP64) { set_error("slab: only the plain FP64 pressure-correction solve is decomposed"); return 1; }
+    if (k0 < 0 || k1 > h->L.nK || k0 >= k1) { set_error("slab: owned planes must satisfy 0 <= k0 < k1 <= nK"); return 1; }
+    CB_CUDA(cudaSetDevice(h->device));
+    if (!h->slabPh && !(h->slabPh = h->cell(3))) { set_error("allocation failed"); return 1; }
+    if (!h->slabSh && !(h->slabSh = h->cell(3))) { set_error("allocation failed"); return 1; }
+    if (!h->slabPart && !(h->slabPart = h->dalloc<double>((size_t)SLAB_MAX_BLOCKS * 8))) { set_error("allocation failed"); return 1; }
+    h->slab = true;
+    h->o0 = (long long)k0 * h->L.nIJ;
+    h->o1 = (long long)k1 * h->L.nIJ;
+    return 0;
+}
+
+namespace {
+int slab_array(caffe_dev* h, const std::string& n, double** base, int* planes) {
+    *base = nullptr; *planes = 0;
+    if (n == "u") { *base = h->u; *planes = 3; }
+    else if (n == "p") { *base = h->p; *planes = 1; }
+    else if (n == "pCorr") { *base = h->pc; *planes = 1; }
+    else if (n == "d") { *base = h->d; *planes = 1; }
+    else if (n == "gradP") { *base = h->gradP; *planes = 3; }
+    else if (n == "gradPCorr") { *base = h->gradPC; *planes = 3; }
+    else if (n == "gradU" && h->gradU) { *base = h->gradU; *planes = 9; }
+    else if (n == "kspPh") { *base = h->slabPh; *planes = 3; }
+    else if (n == "kspSh") { *base = h->slabSh; *planes = 3; }
+    return *base ? 0 : 1;
+}
+}  // namespace
+
+long caffe_slab_halo(caffe_dev* h, const char* name, int planes, int side, int dir, double* buf) {
+    g_err.clear();
+    if (!h || !name) { set_error("NULL argument"); return -1; }
+    if (!h->slab) { set_error("slab: caffe_slab_set_owned has not been called"); return -1; }
+    double* base;
+    int np;
+    if (slab_array(h, name, &base, &np)) { set_error(std::string("slab: no halo exchange for array ") + name); return -1; }
+    if (planes <= 0) planes = np;
+    if (planes > np) { set_error("slab: more planes than the array has"); return -1; }
+    const long long nIJ = h->L.nIJ;
+    const int k0 = (int)(h->o0 / nIJ), k1 = (int)(h->o1 / nIJ);
+    int own, halo;
+    if (side == 0) {
+        if (k0 == 0) { set_error("slab: no halo below the first plane of the lattice"); return -1; }
+        own = k0; halo = k0 - 1;
+    } else if (side == 1) {
+        if (k1 == h->L.nK) { set_error("slab: no halo above the last plane of the lattice"); return -1; }
+        own = k1 - 1; halo = k1;
+    } else {
+        set_error("slab: side is 0 (below) or 1 (above)");
+        return -1;
+    }
+    const long count = (long)planes * (long)nIJ;
+    if (!buf) return count;
+    CB_CUDA(cudaSetDevice(h->device));
+    const size_t row = (size_t)nIJ * sizeof(double), pitch = (size_t)h->L.PS * sizeof(double);
+    if (dir == 0) {
+        if (cudaMemcpy2DAsync(buf, row, base + (long long)own * nIJ, pitch, row, planes, cudaMemcpyDeviceToDevice, h->st) != cudaSuccess) {
+            set_error("slab: halo pack failed"); return -1;
+        }
+    } else if (dir == 1) {
+        if (cudaMemcpy2DAsync(base + (long long)halo * nIJ, pitch, buf, row, row, planes, cudaMemcpyDeviceToDevice, h->st) != cudaSuccess) {
+            set_error("slab: halo unpack failed"); return -1;
+        }
+    } else {
+        set_error("slab: dir is 0 (pack the owned plane) or 1 (unpack into the halo plane)");
+        return -1;
+    }
+    return count;
+}
+
+int caffe_slab_ksp(caffe_dev* h, int sys, int phase, const double* scal, double* red) {
+    g_err.clear();
+    if (!h || !red) { set_error("NULL argument"); return -1; }
+    if (!h->slab) { set_error("slab: caffe_slab_set_owned has not been called"); return -1; }
+    CB_CUDA(cudaSetDevice(h->device));
+    SlabKsp k;
+    k.L = h->L; k.o0 = h->o0; k.o1 = h->o1;
+    k.w = h->kw; k.ph = h->slabPh; k.sh = h->slabSh; k.part = h->slabPart; k.red = red;
+    SlabScal s;
+    for (int q = 0; q < 3; ++q) {
+        s.alpha[q] = scal ? scal[4 * q] : 0.;
+        s.beta[q] = scal ? scal[4 * q + 1] : 0.;
+        s.omega[q] = scal ? scal[4 * q + 2] : 0.;
+        s.flags[q] = scal ? (int)scal[4 * q + 3] : 0;
+    }
+    if (sys == 0) { k.b = h->mb; k.x = h->u; return slab_ksp_phase(h->momOp(), 3, phase, k, s, h->st); }
+    if (sys == 1) { k.b = h->pb; k.x = h->pc; return slab_ksp_phase(h->pOp(), 1, phase, k, s, h->st); }
+    set_error("slab: system 0 (momentum) or 1 (pressure correction)");
+    return -1;
+}
+
+int caffe_slab_phase(caffe_dev* h, const char* name, double dt) {
+    g_err.clear();
+    if (!h || !name) { set_error("NULL argument"); return 1; }
+    if (!h->slab) { set_error("slab: caffe_slab_set_owned has not been called"); return 1; }
+    CB_CUDA(cudaSetDevice(h->device));
+    std::string n(name);
+    if (n == "save_u0") return ph_save_u0(h);
+    if (n == "assemble_momentum") return ph_assemble_momentum(h, dt);
+    if (n == "momentum_post") return ph_momentum_post(h);
+    if (n == "assemble_pcorr") return ph_assemble_pcorr(h);
+    if (n == "correct") return ph_correct(h);
+    if (n == "grad_u") return launch_grad_u(h->geo(), h->bc, h->fields(), h->st);
+    set_error("slab: unknown phase " + n);
+    return 1;
+}
+
+int caffe_slab_reduce(caffe_dev* h, const char* what, double dt, double* red) {
+    g_err.clear();
+    if (!h || !what || !red) { set_error("NULL argument"); return 1; }
+    if (!h->slab) { set_error("slab: caffe_slab_set_owned has not been called"); return 1; }
+    CB_CUDA(cudaSetDevice(h->device));
+    std::string n(what);
+    if (n == "continuity") {
+        // Simple.cpp:358-380 on this slab's cells, in their k-j-i order
+        Lat Lo = h->L;
+        Lo.N = h->o1 - h->o0;
+        return launch_continuity(Lo, h->mfc + h->o0, h->vol + h->o0, nullptr, h->chunkMax, red, h->st);
+    }
+    if (n == "courant") return launch_courant(h->geo(), h->fields(), dt, reinterpret_cast<unsigned long long*>(red), h->st, h->o0, h->o1);
+    set_error("slab: unknown reduction " + n);
+    return 1;
 }
 
 int caffe_dev_set_precond(caffe_dev* h, const float* params) {

@@ -505,14 +505,15 @@ __global__ void __launch_bounds__(256) grad_u_kernel(Geo g, Bc bc, FlowFields f)
 }
 
 // ---------------------------------------------------------------------------
-// Courant number (Simple.cpp:382-408): max over all cells.  Non-negative doubles order
+// Courant number (Simple.cpp:382-408): max over the cells [c0, c1) (all cells, or a slab's own).  Non-negative doubles order
 // like their bit patterns, so the maximum is an atomicMax on the bits.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) courant_kernel(Geo g, FlowFields f, double dt, unsigned long long* out) {
+__global__ void __launch_bounds__(256) courant_kernel(Geo g, FlowFields f, double dt, unsigned long long* out, long long c0,
+                                                      long long c1) {
     const Lat& L = g.L;
-    long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    long long c = c0 + blockIdx.x * (long long)blockDim.x + threadIdx.x;
     double co = 0.;
-    if (c < L.N) {
+    if (c < c1) {
         int i, j, k;
         L.ijk(c, i, j, k);
         long long N = L.PS;   // plane stride of cell vectors
@@ -675,19 +676,30 @@ int launch_correct(const Geo& g, const Bc& bc, const FlowFields& f, const FlowPa
     return 0;
 }
 
-int launch_correct_post(const Geo& g, const Bc& bc, const FlowFields& f, cudaStream_t st) {
+int launch_correct_post(const Geo& g, const Bc& bc, const FlowFields& f, cudaStream_t st, bool gradU) {
     const int B = 256;
     int G = grid_for(g.L.N, B);
     correct_post_kernel<<<G, B, 0, st>>>(g, bc, f);
-    if (f.nonorth) grad_u_kernel<<<G, B, 0, st>>>(g, bc, f);
+    if (f.nonorth && gradU) grad_u_kernel<<<G, B, 0, st>>>(g, bc, f);
     CB_CHECK_LAUNCH();
     return 0;
 }
 
-int launch_courant(const Geo& g, const FlowFields& f, double dt, unsigned long long* d_out, cudaStream_t st) {
-    CB_CUDA(cudaMemsetAsync(d_out, 0, sizeof(unsigned long long), st));
+int launch_grad_u(const Geo& g, const Bc& bc, const FlowFields& f, cudaStream_t st) {
+    if (!f.nonorth) return 0;
     const int B = 256;
-    courant_kernel<<<grid_for(g.L.N, B), B, 0, st>>>(g, f, dt, d_out);
+    grad_u_kernel<<<grid_for(g.L.N, B), B, 0, st>>>(g, bc, f);
+    CB_CHECK_LAUNCH();
+    return 0;
+}
+
+int launch_courant(const Geo& g, const FlowFields& f, double dt, unsigned long long* d_out, cudaStream_t st, long long c0,
+                   long long c1) {
+    CB_CUDA(cudaMemsetAsync(d_out, 0, sizeof(unsigned long long), st));
+    if (c1 < 0) c1 = g.L.N;
+    if (c1 <= c0) return 0;
+    const int B = 256;
+    courant_kernel<<<grid_for(c1 - c0, B), B, 0, st>>>(g, f, dt, d_out, c0, c1);
     CB_CHECK_LAUNCH();
     return 0;
 }

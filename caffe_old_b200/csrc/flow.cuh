@@ -47,8 +47,13 @@ int launch_momentum_assemble(const Geo& g, const Bc& bc, const FlowFields& f, co
 int launch_rhie_chow(const Geo& g, const Bc& bc, const FlowFields& f, const FlowParams& P, cudaStream_t st);
 int launch_pcorr_assemble(const Geo& g, const Bc& bc, const FlowFields& f, const PcSys& s, const FlowParams& P, cudaStream_t st);
 int launch_correct(const Geo& g, const Bc& bc, const FlowFields& f, const FlowParams& P, cudaStream_t st);
-int launch_correct_post(const Geo& g, const Bc& bc, const FlowFields& f, cudaStream_t st);
-int launch_courant(const Geo& g, const FlowFields& f, double dt, unsigned long long* d_out, cudaStream_t st);
+// gradU = false leaves grad u (non-orthogonal extension) to launch_grad_u, for a slab whose u
+// halo planes must be exchanged in between
+int launch_correct_post(const Geo& g, const Bc& bc, const FlowFields& f, cudaStream_t st, bool gradU = true);
+int launch_grad_u(const Geo& g, const Bc& bc, const FlowFields& f, cudaStream_t st);
+// max over the cells [c0, c1); c1 < 0: all cells
+int launch_courant(const Geo& g, const FlowFields& f, double dt, unsigned long long* d_out, cudaStream_t st, long long c0 = 0,
+                   long long c1 = -1);
 int launch_continuity(const Lat& L, const double* mfc, const double* vol, const uint8_t* status, double* chunkMax, double* d_out,
                       cudaStream_t st);
 

@@ -130,6 +130,57 @@ int caffe_dev_stats(caffe_dev* h, caffe_step_stats* stats);
  * events with the solver's kernels. */
 void* caffe_dev_stream(caffe_dev* h);
 int caffe_dev_synchronize(caffe_dev* h);
+/* Run the handle's work on the caller's CUDA stream from now on (after finishing what the
+ * handle's own stream holds); the caller keeps ownership of the stream and must keep it
+ * alive until caffe_dev_destroy. */
+int caffe_dev_set_stream(caffe_dev* h, void* stream);
+
+/* ---- k-slab decomposition (replaces ParallelHexaFvmMesh::initializeSubDomains,
+ * src/Domains/HexaFvmMesh/ParallelHexaFvmMesh.cpp:119-307, the halo exchange of
+ * PrimitiveBoundaryCondition::setBoundaries for PARALLEL faces,
+ * src/Domains/Field/PrimitiveBoundaryCondition.tpp:54-141, and the Parallel::sum / max
+ * reductions of src/Parallel/Parallel.cpp).
+ *
+ * One rank owns the cell planes [k0, k1) of the global lattice.  Its handle is created by
+ * caffe_dev_create on the node planes of the cells [max(k0-1, 0), min(k1+1, nK)): the owned
+ * planes plus one halo plane on each side that has a neighbouring slab, with the global case
+ * (its six boundary types and values) unchanged.  Every finite-volume phase then runs on the
+ * slab exactly as on the whole lattice for the owned cells, provided the halo planes hold the
+ * neighbours' values of the arrays the phase reads; the caller exchanges them with
+ * caffe_slab_halo (through NCCL, or any transport) and runs the linear solves as distributed
+ * Krylov phases (caffe_slab_ksp) whose sums it adds over the ranks.  Plain FP64 solves of
+ * Simple and Piso only (no immersed boundary, no mixed or learned pressure solve). */
+
+/* Declare the owned planes [k0, k1) in the handle's own k numbering. */
+int caffe_slab_set_owned(caffe_dev* h, int k0, int k1);
+
+/* Copy one plane of `planes` planes of a cell array between the slab and a device buffer
+ * of planes x nI*nJ doubles, on the handle's stream.  side 0: the plane below the owned
+ * ones; side 1: above.  dir 0 packs the owned boundary plane into buf; dir 1 unpacks buf into
+ * the halo plane.  Arrays: "u", "p", "pCorr", "d", "gradP", "gradPCorr", "gradU", and the
+ * Krylov vectors "kspPh", "kspSh".  planes 0 means all of the array's.  Returns the buffer's
+ * length in doubles (buf == NULL only queries it), -1 on error. */
+long caffe_slab_halo(caffe_dev* h, const char* name, int planes, int side, int dir, double* buf);
+
+/* One phase of a distributed Krylov solve on the owned cells (sys 0: the momentum system,
+ * three right-hand sides, solution u; sys 1: the pressure correction, solution p').  Phases:
+ * BiCGStab 0 init, 1 p, 2 v = A D^-1 p, 3 s, 4 t = A D^-1 s, 5 update, 6 true residual;
+ * CG 10 init, 11 w = A D^-1 r, 12 update, 13 true residual, 14 restart; mean projection
+ * 20 sum b, 21 b -= c, 22 sum x, 23 x -= c.  scal: 12 host doubles (alpha, beta, omega,
+ * flags per right-hand side; flags 1 run, 2 fresh start, 4 true residual).  red: device
+ * buffer of 8 doubles that receives this slab's sums.  Returns how many sums it wrote, -1
+ * on error.  Replaces SparseMatrix::solve (src/Math/SparseMatrix.cpp:86-106) on one rank. */
+int caffe_slab_ksp(caffe_dev* h, int sys, int phase, const double* scal, double* red);
+
+/* The phases of the step that run on the slab without a reduction, asynchronously on its
+ * stream: "save_u0", "assemble_momentum", "momentum_post", "assemble_pcorr", "correct"
+ * (without grad u) and "grad_u" (non-orthogonal extension). */
+int caffe_slab_phase(caffe_dev* h, const char* name, double dt);
+
+/* This slab's share of a step's reductions into red[0] (device): "continuity", the
+ * reference's scan over the owned cells (Simple.cpp:358-380; ranks combine by max, as its
+ * Parallel::max does), or "courant", the max over the owned cells (Simple.cpp:382-408). */
+int caffe_slab_reduce(caffe_dev* h, const char* what, double dt, double* red);
 
 /* Stand-alone Krylov solve of a 7-point system on an nI x nJ x nK lattice: coef7 holds
  * 7 host arrays of N = nI*nJ*nK doubles (aP, aE, aW, aN, aS, aT, aB; a coefficient whose
