@@ -306,30 +306,41 @@ __global__ void __launch_bounds__(256) restrict_kernel(Dims3 fd, Dims3 cd, const
         wK[ck][m] = rweight_in(2 * K - 1 + m, fd.n2, K, cd.n2);
     }
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarp = blockDim.x >> 5;
-    // stage the fine tile: one warp per (j, k) row of RFI cells, lanes along i; all loads of a row's
-    // three 32-cell chunks are issued before any is stored
-    for (int row = warp; row < RFJ * RFK; row += nwarp) {
-        const int lj = row % RFJ, lk = row / RFJ;
-        const int fj = fj0 + lj, fk = fk0 + lk;
-        const bool rowIn = fj >= 0 && fj < fd.n1 && fk >= 0 && fk < fd.n2;
-        const unsigned rowBase = rowIn ? (unsigned)fk * fsK + (unsigned)fj * fsJ : 0u;
-        constexpr int CH = (RFI + 31) / 32;
-        float fv[CH], dv[CH];
-        uint8_t sv[CH];
-        bool in[CH];
+    // stage the fine tile: one warp per (j, k) row of RFI cells, lanes along i; a warp issues the
+    // loads of RB rows (three 32-cell chunks each) before it stores any, so that on the small
+    // coarse levels, where a few CTAs stage everything, each warp has RB rows in flight
+    constexpr int CH = (RFI + 31) / 32, RB = 4;
+    for (int row0 = warp; row0 < RFJ * RFK; row0 += RB * nwarp) {
+        float fv[RB][CH], dv[RB][CH];
+        uint8_t sv[RB][CH];
+        bool in[RB][CH];
 #pragma unroll
-        for (int u = 0; u < CH; ++u) {
-            const int li = lane + 32 * u, fi = fi0 + li;
-            in[u] = rowIn && li < RFI && fi >= 0 && fi < fd.n0;
-            const unsigned f = in[u] ? rowBase + (unsigned)fi : 0u;
-            fv[u] = (in[u] && fin) ? __ldg(fin + f) : 1.f;
-            dv[u] = (in[u] && invD) ? __ldg(invD + f) : 1.f;
-            sv[u] = (in[u] && st) ? __ldg(st + f) : (uint8_t)ST_ACTIVE;
+        for (int b = 0; b < RB; ++b) {
+            const int row = row0 + b * nwarp;
+            const int lj = row % RFJ, lk = row / RFJ;
+            const int fj = fj0 + lj, fk = fk0 + lk;
+            const bool rowIn = row < RFJ * RFK && fj >= 0 && fj < fd.n1 && fk >= 0 && fk < fd.n2;
+            const unsigned rowBase = rowIn ? (unsigned)fk * fsK + (unsigned)fj * fsJ : 0u;
+#pragma unroll
+            for (int u = 0; u < CH; ++u) {
+                const int li = lane + 32 * u, fi = fi0 + li;
+                in[b][u] = rowIn && li < RFI && fi >= 0 && fi < fd.n0;
+                const unsigned f = in[b][u] ? rowBase + (unsigned)fi : 0u;
+                fv[b][u] = (in[b][u] && fin) ? __ldg(fin + f) : 1.f;
+                dv[b][u] = (in[b][u] && invD) ? __ldg(invD + f) : 1.f;
+                sv[b][u] = (in[b][u] && st) ? __ldg(st + f) : (uint8_t)ST_ACTIVE;
+            }
         }
 #pragma unroll
-        for (int u = 0; u < CH; ++u) {
-            const int li = lane + 32 * u;
-            if (li < RFI) s0[lk][lj][li] = (in[u] && sv[u] == ST_ACTIVE) ? fv[u] * dv[u] : 0.f;
+        for (int b = 0; b < RB; ++b) {
+            const int row = row0 + b * nwarp;
+            if (row >= RFJ * RFK) continue;
+            const int lj = row % RFJ, lk = row / RFJ;
+#pragma unroll
+            for (int u = 0; u < CH; ++u) {
+                const int li = lane + 32 * u;
+                if (li < RFI) s0[lk][lj][li] = (in[b][u] && sv[b][u] == ST_ACTIVE) ? fv[b][u] * dv[b][u] : 0.f;
+            }
         }
     }
     __syncthreads();
@@ -831,6 +842,34 @@ __global__ void __launch_bounds__(256) prolong_kernel(Dims3 fd, Dims3 cd, const 
     float v = gain * sy * yv;
     if (wc) v += prolong_at(fd, cd, wc, f);
     out[f] = v;
+}
+
+// prolong_kernel on 4 consecutive fine cells per thread (cell count a multiple of 4, 16-byte
+// aligned arrays): one index division per 4 cells and each coarse row loaded once (prolong4),
+// every value formed as prolong_kernel forms it
+__global__ void __launch_bounds__(256) prolong4_kernel(Dims3 fd, Dims3 cd, const float* wc, const float* y, const float* yn, int ydiv,
+                                                       float gain, float* out, const Scal* S) {
+    if (S->done) return;
+    const long long NQ = ((long long)fd.n0 * fd.n1 * fd.n2) >> 2;
+    const long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (q >= NQ) return;
+    const float sy = ydiv ? 1.f : (float)S->s;
+    float Y[4], PW[4] = {0.f, 0.f, 0.f, 0.f}, V[4];
+    un4(ld4(y, q), Y);
+    if (yn) {
+        float Yn[4];
+        un4(ld4(yn, q), Yn);
+#pragma unroll
+        for (int m = 0; m < 4; ++m) Y[m] = 0.5f * (Y[m] - Yn[m]);
+    }
+    if (wc) prolong4(fd, cd, wc, q, PW);
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+        float v = gain * sy * Y[m];
+        if (wc) v += PW[m];
+        V[m] = v;
+    }
+    st4(out, q, V);
 }
 
 // z = D^-1 r + P w_1 (active), D^-1 r (ghost), 0 (inactive); partial (z, q_prev)
@@ -1583,9 +1622,16 @@ int apply_levels(LearnedWork& lw, const float* rfine, const uint8_t* status, int
     for (int l = lt - 1; l >= 1; --l) {
         Level& f = lw.lev[l];
         const bool top = l + 1 >= lw.nLev;
-        prolong_kernel<<<grid_for(f.N, 256), 256, 0, st>>>(dims_of(f), top ? dims_of(f) : dims_of(lw.lev[l + 1]),
-                                                           top ? nullptr : lw.lev[l + 1].w, netAt(l) ? f.net.y : f.u,
-                                                           netAt(l) ? f.netNeg.y : nullptr, netAt(l) ? 0 : 1, f.gain, f.w, S);
+        const float* y = netAt(l) ? f.net.y : f.u;
+        const float* yn = netAt(l) ? f.netNeg.y : nullptr;
+        auto a16 = [](const void* p) { return ((uintptr_t)p & 15u) == 0; };
+        if ((f.N & 3) == 0 && a16(y) && a16(f.w) && (!yn || a16(yn)))
+            prolong4_kernel<<<grid_for(f.N / 4, 256), 256, 0, st>>>(dims_of(f), top ? dims_of(f) : dims_of(lw.lev[l + 1]),
+                                                                    top ? nullptr : lw.lev[l + 1].w, y, yn, netAt(l) ? 0 : 1, f.gain,
+                                                                    f.w, S);
+        else
+            prolong_kernel<<<grid_for(f.N, 256), 256, 0, st>>>(dims_of(f), top ? dims_of(f) : dims_of(lw.lev[l + 1]),
+                                                               top ? nullptr : lw.lev[l + 1].w, y, yn, netAt(l) ? 0 : 1, f.gain, f.w, S);
     }
     CB_CHECK_LAUNCH();
     return 0;

@@ -485,3 +485,50 @@ class SlabSolver:
         """A cell field on this process's slabs, in the global lattice's cell order (all of
         it with ``LocalTransport``)."""
         return np.concatenate([s.owned(name) for s in self.slabs], axis=0).ravel()
+
+
+def main(argv=None) -> None:
+    """Times the lid-driven cavity (PISO, Re 400, n^3 cells) on the whole lattice and as `slabs`
+    slabs driven from this process on one GPU, from the same state, and prints one JSON line:
+    seconds per step, Krylov iterations and the largest field difference."""
+    import argparse
+    import json
+    import time
+
+    import torch
+
+    from .solver import make_solver
+    ap = argparse.ArgumentParser(description=main.__doc__)
+    ap.add_argument("--size", type=int, default=128)
+    ap.add_argument("--slabs", type=int, default=2)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=1)
+    a = ap.parse_args(argv)
+    nodes, spec, _ = C.config2_cavity3d(n=a.size)
+    whole = make_solver(nodes, spec)
+    sl = SlabSolver(nodes, spec, a.slabs)
+    out = {"workload": f"piso_lid_cavity3d_{a.size}^3_re400_cg_jacobi_fp64", "slabs": a.slabs, "transport": "in-process, one GPU"}
+    try:
+        for name, run in (("whole", lambda: whole.solve()), ("slabs", lambda: sl.solve())):
+            for _ in range(a.warmup):
+                run()
+            torch.cuda.synchronize()
+            iters = []
+            t0 = time.perf_counter()
+            for _ in range(a.steps):
+                run()
+                st = whole.last_stats if name == "whole" else sl.last_stats
+                iters.append(st["p_iters_total"])
+            torch.cuda.synchronize()
+            out[f"{name}_s_per_step"] = (time.perf_counter() - t0) / a.steps
+            out[f"{name}_p_iters"] = iters
+        out["slab_over_whole"] = out["slabs_s_per_step"] / out["whole_s_per_step"]
+        out["max_abs_du"] = float(np.max(np.abs(sl.field("u") - whole.field("u"))))
+    finally:
+        sl.close()
+        whole.close()
+    print(json.dumps(out))
+
+
+if __name__ == "__main__":
+    main()
