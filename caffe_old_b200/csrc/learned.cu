@@ -455,9 +455,16 @@ __global__ void __launch_bounds__(RT_THREADS, 2) restrict_tma_kernel(const __gri
     __shared__ __align__(8) uint64_t full[3];
     __shared__ float t1[RFK][RFJ][RCI];
     __shared__ float t2[RFK][RCJ][RCI];
-    __shared__ float wI[RCI][4], wJ[RCJ][4], wK[RCK][4];
+    // weights of the tile being reduced, double-buffered by tile parity: tile n writes its set while
+    // the last readers of tile n-1's pass 3 may still run, so no barrier ends a tile
+    __shared__ float wI[2][RCI][4], wJ[2][RCJ][4], wK[2][RCK][4];
     const int tI = (cd.n0 + RCI - 1) / RCI, tJ = (cd.n1 + RCJ - 1) / RCJ, tK = (cd.n2 + RCK - 1) / RCK;
     const int T = tI * tJ * tK;
+    // the tile's coordinates are stepped by gridDim.x = dI + tI (dJ + tJ dK) per iteration, with
+    // carries, instead of divided every iteration
+    const int G = (int)gridDim.x;
+    const int dI = G % tI, dJ = (G / tI) % tJ, dK = G / (tI * tJ);
+    int ti = (int)blockIdx.x % tI, tj = ((int)blockIdx.x / tI) % tJ, tk = (int)blockIdx.x / (tI * tJ);
     if (threadIdx.x == 0) {
         for (int q = 0; q < NS; ++q) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(rt_smem(&full[q])));
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -486,21 +493,28 @@ __global__ void __launch_bounds__(RT_THREADS, 2) restrict_tma_kernel(const __gri
     int n = 0;
     for (int tile = blockIdx.x; tile < T; tile += gridDim.x, ++n) {
         const int stage = n % NS;
-        // the stage of tile n-1, free since the barrier that ended it, takes tile n + NS - 1
+        // the stage of tile n-1 is free once every thread has passed tile n-1's second barrier (its
+        // last read of the stage is pass 1): it takes tile n + NS - 1
         const int ahead = tile + (NS - 1) * (int)gridDim.x;
         if (threadIdx.x == 0 && ahead < T) issue(ahead, (n + NS - 1) % NS);
-        const int ti = tile % tI, tj = (tile / tI) % tJ, tk = tile / (tI * tJ);
         const int I0 = ti * RCI, J0 = tj * RCJ, K0 = tk * RCK;
+        const int wb = n & 1;
         if (threadIdx.x < 4 * RCI) {
             int ci = threadIdx.x >> 2, m = threadIdx.x & 3, I = I0 + ci;
-            wI[ci][m] = rweight_in(2 * I - 1 + m, fd.n0, I, cd.n0);
+            wI[wb][ci][m] = rweight_in(2 * I - 1 + m, fd.n0, I, cd.n0);
         } else if (threadIdx.x < 4 * RCI + 4 * RCJ) {
             int u = threadIdx.x - 4 * RCI, cj = u >> 2, m = u & 3, J = J0 + cj;
-            wJ[cj][m] = rweight_in(2 * J - 1 + m, fd.n1, J, cd.n1);
+            wJ[wb][cj][m] = rweight_in(2 * J - 1 + m, fd.n1, J, cd.n1);
         } else if (threadIdx.x < 4 * RCI + 4 * RCJ + 4 * RCK) {
             int u = threadIdx.x - 4 * RCI - 4 * RCJ, ck = u >> 2, m = u & 3, K = K0 + ck;
-            wK[ck][m] = rweight_in(2 * K - 1 + m, fd.n2, K, cd.n2);
+            wK[wb][ck][m] = rweight_in(2 * K - 1 + m, fd.n2, K, cd.n2);
         }
+        // the next tile's coordinates
+        ti += dI;
+        if (ti >= tI) { ti -= tI; ++tj; }
+        tj += dJ;
+        if (tj >= tJ) { tj -= tJ; ++tk; }
+        tk += dK;
         bool ok = true;
         if (threadIdx.x < 32) ok = rt_wait(rt_smem(&full[stage]), (uint32_t)((n / NS) & 1));
         if (__syncthreads_or(ok ? 0 : 1)) { failed = true; break; }
@@ -521,7 +535,7 @@ __global__ void __launch_bounds__(RT_THREADS, 2) restrict_tma_kernel(const __gri
         // weights stay in registers; the four fine values of pass 1 come as three aligned float2
         const int ci = threadIdx.x & (RCI - 1);
         {
-            const float w0 = wI[ci][0], w1 = wI[ci][1], w2 = wI[ci][2], w3 = wI[ci][3];
+            const float w0 = wI[wb][ci][0], w1 = wI[wb][ci][1], w2 = wI[wb][ci][2], w3 = wI[wb][ci][3];
             float* T1 = &t1[0][0][0];
             for (int row = threadIdx.x >> 5; row < RFK * RFJ; row += RT_THREADS / RCI) {
                 const float2* v2 = reinterpret_cast<const float2*>(sf + row * RT_BX + 2 + 2 * ci);   // fine 2I-2 .. 2I+3
@@ -532,7 +546,7 @@ __global__ void __launch_bounds__(RT_THREADS, 2) restrict_tma_kernel(const __gri
         __syncthreads();
         {
             const int cj = (threadIdx.x >> 5) & (RCJ - 1);
-            const float w0 = wJ[cj][0], w1 = wJ[cj][1], w2 = wJ[cj][2], w3 = wJ[cj][3];
+            const float w0 = wJ[wb][cj][0], w1 = wJ[wb][cj][1], w2 = wJ[wb][cj][2], w3 = wJ[wb][cj][3];
             for (int lk = threadIdx.x / (RCI * RCJ); lk < RFK; lk += RT_THREADS / (RCI * RCJ))
                 t2[lk][cj][ci] = w0 * t1[lk][2 * cj][ci] + w1 * t1[lk][2 * cj + 1][ci] + w2 * t1[lk][2 * cj + 2][ci] + w3 * t1[lk][2 * cj + 3][ci];
         }
@@ -541,12 +555,14 @@ __global__ void __launch_bounds__(RT_THREADS, 2) restrict_tma_kernel(const __gri
             const int cj = (threadIdx.x >> 5) & (RCJ - 1), ck = threadIdx.x / (RCI * RCJ);
             const int I = I0 + ci, J = J0 + cj, K = K0 + ck;
             if (I < cd.n0 && J < cd.n1 && K < cd.n2) {
-                const float acc = wK[ck][0] * t2[2 * ck][cj][ci] + wK[ck][1] * t2[2 * ck + 1][cj][ci] + wK[ck][2] * t2[2 * ck + 2][cj][ci] +
-                                  wK[ck][3] * t2[2 * ck + 3][cj][ci];
+                const float acc = wK[wb][ck][0] * t2[2 * ck][cj][ci] + wK[wb][ck][1] * t2[2 * ck + 1][cj][ci] +
+                                  wK[wb][ck][2] * t2[2 * ck + 2][cj][ci] + wK[wb][ck][3] * t2[2 * ck + 3][cj][ci];
                 out[((unsigned)K * (unsigned)cd.n1 + (unsigned)J) * (unsigned)cd.n0 + (unsigned)I] = acc * scale;
             }
         }
-        __syncthreads();
+        // no barrier here: tile n+1 writes t1 after its first barrier (all of tile n's pass 2 is
+        // done by then), t2 after its second (all of tile n's pass 3 reads come before the first
+        // barrier of tile n+1 is passed), and weights into the other buffer
     }
     if (threadIdx.x == 0) {
         if (failed) atomicExch(err, 1);
