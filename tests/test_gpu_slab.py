@@ -13,6 +13,10 @@ sums as ranks on separate GPUs, with copies in place of the point-to-point messa
   PISO with two correctors, central convection with the non-orthogonal term on a sheared
   mesh, and a channel with a fixed-pressure outlet; the continuity error is the max over the
   slabs of the reference's scan of each slab's cells (its Parallel::max).
+* Slabs of one plane each (halo planes on both sides of every owned plane) match the whole
+  lattice too.
+* The NCCL form of the transport (``DistTransport`` over a one-rank process group: the sums
+  all-reduced on device tensors on the slabs' stream) takes the same steps.
 * The immersed boundary and the mixed / learned pressure solves are refused.
 """
 import numpy as np
@@ -235,3 +239,62 @@ def test_unsupported_forms_are_refused():
         S.SlabSolver(nodes, spec.replace(kind="ibpiso", ib_radius=0.2, ib_center=(0.5, 0.5, 0.5)), 2)
     with pytest.raises(CaffeError):
         S.SlabSolver(nodes, spec.replace(p_form="mixed"), 2)
+
+
+def test_one_plane_slabs_match_the_whole_lattice():
+    """Every slab owns a single plane, so every interior slab has halo planes on both sides of it."""
+    nodes, spec = _cavity3d(n=(6, 5, 6))
+    P = Pair(nodes, spec, 6)
+    try:
+        for _ in range(3):
+            P.S.solve()
+            P.g.solve()
+        vol = P.g.field("vol")
+        assert rel_l2(P.S.field("u"), P.g.field("u")) < SLAB_RTOL
+        assert rel_l2(demean(P.S.field("p"), vol), demean(P.g.field("p"), vol)) < SLAB_RTOL
+    finally:
+        P.close()
+
+
+def _nccl_one_rank(q):
+    import os
+    from datetime import timedelta
+
+    import torch
+    import torch.distributed as dist
+    port = q.get()
+    dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1, timeout=timedelta(seconds=60))
+    try:
+        torch.cuda.set_device(0)
+        nodes, spec = _cavity3d(n=(6, 5, 8))
+        sol = S.SlabSolver(nodes, spec, 1, ranks=[0], transport=S.DistTransport(), device=0)
+        ref = make_solver(nodes, spec)
+        for _ in range(2):
+            c1 = sol.solve()
+            c2 = ref.solve()
+        q.put((c1, c2, rel_l2(sol.field("u"), ref.field("u"))))
+        sol.close()
+        ref.close()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_dist_transport_over_nccl_single_rank():
+    """The NCCL form of the transport (all-reduce of the slab sums on device tensors, on the
+    slabs' stream) in a one-rank process group: the same step as the whole-lattice solver."""
+    import socket
+
+    import torch.multiprocessing as mp
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    q.put(port)
+    p = ctx.Process(target=_nccl_one_rank, args=(q,))
+    p.start()
+    p.join(timeout=300)
+    assert p.exitcode == 0
+    c1, c2, du = q.get(timeout=10)
+    # the continuity errors are round-off sized (a few 1e-15) after these steps: compared absolutely
+    assert du < SLAB_RTOL and abs(c1 - c2) <= 1e-12
