@@ -734,6 +734,12 @@ int caffe_dev_destroy(caffe_dev* h) {
 int caffe_dev_solve(caffe_dev* h, double dt, caffe_step_stats* stats) {
     g_err.clear();
     if (!h) { set_error("handle is NULL"); return 1; }
+    if (h->slab) {
+        // a slab's step needs its halo planes exchanged between phases and its solves summed over
+        // the slabs: the caller runs it through caffe_slab_phase / caffe_slab_ksp / caffe_slab_halo
+        set_error("the handle is one slab of a decomposition: its step runs through the caffe_slab_* phases");
+        return 1;
+    }
     if (!(dt > 0.) && h->cs.time_accurate) { set_error("time step must be positive"); return 1; }
     CB_CUDA(cudaSetDevice(h->device));
     if (do_step(h, dt)) return 1;

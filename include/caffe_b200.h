@@ -151,7 +151,8 @@ int caffe_dev_set_stream(caffe_dev* h, void* stream);
  * Krylov phases (caffe_slab_ksp) whose sums it adds over the ranks.  Plain FP64 solves of
  * Simple and Piso only (no immersed boundary, no mixed or learned pressure solve). */
 
-/* Declare the owned planes [k0, k1) in the handle's own k numbering. */
+/* Declare the owned planes [k0, k1) in the handle's own k numbering.  From then on the handle's
+ * step runs through the caffe_slab_* calls; caffe_dev_solve refuses it. */
 int caffe_slab_set_owned(caffe_dev* h, int k0, int k1);
 
 /* Copy one plane of `planes` planes of a cell array between the slab and a device buffer

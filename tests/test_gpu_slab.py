@@ -239,6 +239,12 @@ def test_unsupported_forms_are_refused():
         S.SlabSolver(nodes, spec.replace(kind="ibpiso", ib_radius=0.2, ib_center=(0.5, 0.5, 0.5)), 2)
     with pytest.raises(CaffeError):
         S.SlabSolver(nodes, spec.replace(p_form="mixed"), 2)
+    sol = S.SlabSolver(nodes, spec, 2)
+    try:
+        with pytest.raises(CaffeError):
+            sol.slabs[0].solver.solve()      # a slab's step runs through the slab phases only
+    finally:
+        sol.close()
 
 
 def test_one_plane_slabs_match_the_whole_lattice():
