@@ -263,7 +263,6 @@ def test_one_plane_slabs_match_the_whole_lattice():
 
 
 def _nccl_one_rank(q):
-    import os
     from datetime import timedelta
 
     import torch
