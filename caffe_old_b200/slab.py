@@ -404,7 +404,10 @@ class SlabSolver:
 
     FIELD_ARRAYS = (("u", 3), ("p", 1), ("pCorr", 1), ("d", 1), ("gradP", 3), ("gradPCorr", 3))
 
-    def __init__(self, nodes: np.ndarray, spec: C.CaseSpec, nslabs: int, ranks=None, transport=None, device: int = 0):
+    def __init__(self, nodes: np.ndarray, spec: C.CaseSpec, nslabs: int, ranks=None, transport=None, device: int = 0,
+                 slab_factory=None):
+        """slab_factory(nodes, spec, parts, rank) builds a slab with DeviceSlab's interface in
+        place of a device slab (the host-side tests use CPU stand-ins)."""
         if spec.kind not in ("simple", "piso"):
             raise ValueError("the slab decomposition runs Simple and Piso")
         nodes = np.ascontiguousarray(nodes, dtype=np.float64)
@@ -414,9 +417,13 @@ class SlabSolver:
         self.parts = partition(self.nK, nslabs)
         self.ranks = list(range(nslabs)) if ranks is None else list(ranks)
         self.transport = transport if transport is not None else LocalTransport(nslabs)
-        import torch
-        self.stream = torch.cuda.Stream(torch.device("cuda", device))   # shared by this process's slabs
-        self.slabs = [DeviceSlab(nodes, spec, self.parts, r, device, self.stream) for r in self.ranks]
+        if slab_factory is None:
+            import torch
+            self.stream = torch.cuda.Stream(torch.device("cuda", device))   # shared by this process's slabs
+            self.slabs = [DeviceSlab(nodes, spec, self.parts, r, device, self.stream) for r in self.ranks]
+        else:
+            self.stream = None
+            self.slabs = [slab_factory(nodes, spec, self.parts, r) for r in self.ranks]
         self.singular = not any(t == "outlet" for t in spec.bc)
         self.last_stats: dict = {}
         self.sync_halos()

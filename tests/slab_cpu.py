@@ -190,3 +190,65 @@ class NumpySlab:
 
     def owned_x(self):
         return self._own(self.x).copy()
+
+
+class StepSlab:
+    """A CPU stand-in for a whole device slab of SlabSolver: the momentum system (three
+    right-hand sides) and the p' system are random 7-point systems solved by NumpySlab engines;
+    the finite-volume phases only record their names; every cell array the step exchanges is a
+    plain array whose owned boundary planes are exchanged for real.  `log` receives
+    ("phase", name), ("ksp", sys, phase) and ("exchange", names) in call order."""
+
+    CELL_ARRAYS = {"u": 3, "p": 1, "d": 1, "gradP": 3, "gradPCorr": 3, "gradU": 9}
+
+    def __init__(self, shape, parts, rank: int, seed: int = 5):
+        am, bm = random_system(shape, 3, False, seed)
+        ap, bp = random_system(shape, 1, True, seed + 1)
+        self.mom = NumpySlab(am, bm, parts, rank)
+        self.pc = NumpySlab(ap, bp, parts, rank)
+        self.sides = self.mom.sides
+        self.nIJ = self.mom.nIJ
+        self.k0, self.k1 = self.mom.k0, self.mom.k1
+        nKe = self.mom.a.shape[1]
+        rng = np.random.default_rng(seed + 10 + rank)
+        self.cells = {n: rng.normal(size=(c, nKe) + self.mom.a.shape[2:]) for n, c in self.CELL_ARRAYS.items()}
+        self.red = torch.zeros(8, dtype=torch.float64)
+        self.log = []
+        self._cur = self.mom
+
+    def close(self):
+        pass
+
+    def phase(self, name: str, dt: float) -> None:
+        self.log.append(("phase", name))
+
+    def ksp(self, sys: int, phase: int, scal=None) -> int:
+        self.log.append(("ksp", sys, phase))
+        self._cur = self.mom if sys == 0 else self.pc
+        n = self._cur.ksp(sys, phase, scal)
+        self.red.copy_(self._cur.red)
+        return n
+
+    def reduce(self, what: str, dt: float) -> None:
+        self.log.append(("reduce", what))
+        self.red[0] = float(self.k1) if what == "continuity" else 0.5 * float(self.k0)
+
+    def buffers(self, arrays, side: int):
+        if side == self.sides[0]:
+            self.log.append(("exchange", tuple(name for name, _ in arrays)))
+        return self.mom.buffers(arrays, side)
+
+    def halo(self, name: str, planes: int, side: int, dir: int, buf, offset: int) -> int:
+        if name in ("kspPh", "kspSh"):
+            return self._cur.halo(name, planes, side, dir, buf, offset)
+        # u and p' are the solutions of the two systems; the rest are plain arrays
+        arr = self.mom.x if name == "u" else (self.pc.x if name == "pCorr" else self.cells[name])
+        lo, hi = self.mom.lo, self.mom.hi
+        plane = (lo if side == 0 else hi - 1) if dir == 0 else (lo - 1 if side == 0 else hi)
+        n = planes * self.nIJ
+        view = buf[offset:offset + n].numpy().reshape(planes, -1)
+        if dir == 0:
+            view[...] = arr[:planes, plane].reshape(planes, -1)
+        else:
+            arr[:planes, plane] = view.reshape(arr[:planes, plane].shape)
+        return n

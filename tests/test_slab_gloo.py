@@ -9,6 +9,10 @@
   the sums) the solve is bit-identical to the same two slabs driven in one process
   (``LocalTransport``), for BiCGStab on three right-hand sides, CG, and CG on a singular
   system with the mean projection.
+* The whole step (``SlabSolver.solve`` over CPU stand-ins of the device slabs): it takes the
+  phases and halo exchanges of the documented halo set, in order, for SIMPLE, PISO with two
+  inner iterations and the non-orthogonal extension; under gloo two ranks take exactly the
+  steps of the same two slabs in one process, with bit-identical solutions.
 """
 import os
 import socket
@@ -133,3 +137,104 @@ def test_gloo_two_ranks_match_two_local_slabs_bit_for_bit(kind):
     x_loc, out_loc, _, _ = _local(kind, 2)
     assert got[0][2]["iters"] == out_loc["iters"]
     assert np.array_equal(x_dist, x_loc)
+
+
+# ---------------------------------------------------------------- the whole step's orchestration
+STEP_SHAPE = (5, 4, 8)
+
+
+def _step_spec(kind, nonorth=False):
+    from caffe_old_b200 import cases as C
+    bc, ref = C.lid_cavity_bcs("north")
+    return C.CaseSpec(kind=kind, bc=bc, ref_vec=ref, time_accurate=kind == "piso", n_inner=2 if kind == "piso" else 1,
+                      n_pcorr=2, nonorth=nonorth, convection="central" if nonorth else "upwind", p_method="cg_jacobi",
+                      mom_rtol=1e-10, p_rtol=1e-10, maxit=500, dt=0.01)
+
+
+def _step_factory():
+    from slab_cpu import StepSlab
+    return lambda nodes, spec, parts, rank: StepSlab(STEP_SHAPE, parts, rank)
+
+
+def _nodes():
+    from caffe_old_b200 import cases as C
+    return C.cartesian_nodes(STEP_SHAPE, (1.0, 1.0, 1.0))
+
+
+def _outline(log):
+    """Phases, reductions and exchanges in order, without the Krylov phases and their vector
+    exchanges, and with repeated exchanges of a solve's solution merged."""
+    out = []
+    for ev in log:
+        if ev[0] == "ksp" or (ev[0] == "exchange" and ev[1][0] in ("kspPh", "kspSh")):
+            continue
+        if out and ev[0] == "exchange" and out[-1] == ev:
+            continue
+        out.append(ev)
+    return out
+
+
+def _expected_outline(spec):
+    """The halo set of the step: which arrays each phase leaves to be exchanged."""
+    ev = [("phase", "save_u0")]
+    n_inner = spec.n_inner if spec.time_accurate else 1
+    n_pc = 1 if spec.kind == "simple" else spec.n_pcorr
+    for _ in range(n_inner):
+        ev += [("phase", "assemble_momentum"), ("exchange", ("d",)), ("exchange", ("u",)), ("phase", "momentum_post")]
+        for _ in range(n_pc):
+            ev += [("phase", "assemble_pcorr"), ("exchange", ("pCorr",)), ("phase", "correct"),
+                   ("exchange", ("u", "p", "gradP", "gradPCorr"))]
+            if spec.nonorth:
+                ev += [("phase", "grad_u"), ("exchange", ("gradU",))]
+    return ev + [("reduce", "courant"), ("reduce", "continuity")]
+
+
+@pytest.mark.parametrize("kind,nonorth", [("simple", False), ("piso", False), ("piso", True)])
+def test_step_takes_the_documented_phases_and_exchanges(kind, nonorth):
+    spec = _step_spec(kind, nonorth)
+    sol = S.SlabSolver(_nodes(), spec, 3, slab_factory=_step_factory())
+    for s in sol.slabs:
+        s.log.clear()
+    cont = sol.solve()
+    for s in sol.slabs:
+        assert _outline(s.log) == _expected_outline(spec), s.k0
+    assert cont == float(STEP_SHAPE[2])                   # the max of the slabs' values
+    assert sol.last_stats["courant"] == 0.5 * sol.parts[-1][0]
+    assert sol.last_stats["status"] == 0
+
+
+def _step_worker(rank, world, port, q):
+    sys.path[:0] = [ROOT, HERE]
+    import torch.distributed as dist
+    import test_slab_gloo as T
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world,
+                            timeout=timedelta(seconds=60))
+    try:
+        spec = T._step_spec("piso", True)
+        sol = S.SlabSolver(T._nodes(), spec, world, ranks=[rank], transport=S.DistTransport(), slab_factory=T._step_factory())
+        conts = [sol.solve() for _ in range(2)]
+        s = sol.slabs[0]
+        q.put((rank, conts, s.log, s.mom.owned_x(), s.pc.owned_x()))
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_gloo_two_ranks_take_the_same_steps_as_two_local_slabs():
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_step_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    got = sorted((q.get(timeout=120) for _ in range(2)), key=lambda t: t[0])
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    spec = _step_spec("piso", True)
+    loc = S.SlabSolver(_nodes(), spec, 2, slab_factory=_step_factory())
+    conts = [loc.solve() for _ in range(2)]
+    assert got[0][1] == got[1][1] == conts
+    for (rank, _, log, xm, xp), s in zip(got, loc.slabs):
+        assert log == s.log, rank              # the same phases, solves and exchanges, in order
+        assert np.array_equal(xm, s.mom.owned_x()) and np.array_equal(xp, s.pc.owned_x())
