@@ -47,6 +47,9 @@ def lockstep_cases():
         "cavity3d": H.small_cavity3d(central=False),
         "skewed": (skewed_nodes, skewed_spec.replace(convection="upwind")),
         "channel": H.small_channel_sphere(),
+        "piso_inner": H.small_piso_inner(),
+        "simple_transient": H.small_simple_transient(),
+        "outlet_top": H.small_outlet_top(),
     }
 
 

@@ -109,3 +109,31 @@ def oracle_dmet_to_faces(oracle, shape):
     out["W_check"] = np.array_equal(d[1][:, :, 1:], d[0][:, :, :-1]) and np.array_equal(d[3][:, 1:, :], d[2][:, :-1, :]) \
         and np.array_equal(d[5][1:], d[4][:-1])
     return out
+
+
+def small_piso_inner(n=(8, 6, 5)):
+    """PISO with two inner iterations and three correctors per step (Piso.cpp:12-29)."""
+    nodes, spec = small_cavity3d(n, central=False, cg=True)
+    return nodes, spec.replace(n_inner=2, n_pcorr=3)
+
+
+def small_simple_transient(n=(7, 6, 5)):
+    """Time-accurate SIMPLE: two inner iterations per step (Simple.cpp:78-91)."""
+    nodes = C.cartesian_nodes(n, (1.0, 1.0, 1.0))
+    bc, ref = C.lid_cavity_bcs("north")
+    spec = C.CaseSpec(kind="simple", bc=bc, ref_vec=ref, rho=1.0, mu=0.01, time_accurate=True, n_inner=2, omega_u=0.7,
+                      omega_p=0.3, convection="upwind", mom_method="bicgstab_jacobi", p_method="bicgstab_jacobi",
+                      mom_rtol=KSP_RTOL, p_rtol=KSP_RTOL, maxit=5000, dt=0.05)
+    return nodes, spec
+
+
+def small_outlet_top(n=(6, 5, 10)):
+    """SIMPLE channel along k: inlet at the bottom, fixed-pressure outlet at the top."""
+    nodes = C.cartesian_nodes(n, (1.0, 1.0, 3.0))
+    bc = ("wall", "wall", "wall", "wall", "outlet", "inlet")
+    ref = ((0.0, 0.0, 0.0),) * 5 + ((0.0, 0.0, 1.0),)
+    spec = C.CaseSpec(kind="simple", bc=bc, ref_vec=ref, ref_val=(0.0, 0.0, 0.0, 0.0, 0.25, 0.0), rho=1.0, mu=0.05,
+                      time_accurate=False, omega_u=0.7, omega_p=0.3, convection="upwind", mom_method="bicgstab_jacobi",
+                      p_method="bicgstab_jacobi", mom_rtol=KSP_RTOL, p_rtol=KSP_RTOL, maxit=5000, dt=1.0,
+                      u_init=(0.0, 0.0, 1.0))
+    return nodes, spec

@@ -30,7 +30,7 @@ import ref_pin as P
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "reference_solver.npz")
 FIELDS = ("u", "p", "massFlowI", "massFlowJ", "massFlowK")
-CASES = ("cavity2d", "cavity3d", "skewed", "channel")
+CASES = ("cavity2d", "cavity3d", "skewed", "channel", "piso_inner", "simple_transient", "outlet_top")
 
 
 def _case(name):
@@ -41,6 +41,12 @@ def _case(name):
     if name == "skewed":
         nodes, spec = H.small_skewed(nonorth=False)
         return nodes, spec.replace(convection="upwind")
+    if name == "piso_inner":
+        return H.small_piso_inner()
+    if name == "simple_transient":
+        return H.small_simple_transient()
+    if name == "outlet_top":
+        return H.small_outlet_top()
     return H.small_channel_sphere()
 
 
