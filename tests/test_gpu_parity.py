@@ -13,7 +13,8 @@ from caffe_old_b200.solver import make_solver
 from caffe_old_b200 import cases as C
 
 from helpers import (FIELD_RTOL, STATE_NAMES, c1_parity, copy_state, demean, oracle_dmet_to_faces, rel_l2,
-                     small_cavity2d, small_cavity3d, small_channel_sphere, small_skewed)
+                     small_cavity2d, small_cavity3d, small_channel_sphere, small_outlet_top, small_piso_inner,
+                     small_simple_transient, small_skewed)
 
 pytestmark = pytest.mark.gpu
 
@@ -38,7 +39,8 @@ def _advance_oracle(o, steps):
 
 
 @pytest.mark.parametrize("maker,steps", [(small_cavity2d, 3), (small_cavity3d, 2), (small_skewed, 2),
-                                         (small_channel_sphere, 3)])
+                                         (small_channel_sphere, 3), (small_piso_inner, 2), (small_simple_transient, 2),
+                                         (small_outlet_top, 3)])
 def test_phases_bit_exact(maker, steps):
     """Every phase outside the Krylov solves, from the same state: bit for bit.  The skewed mesh
     runs with the non-orthogonal correction (its cell velocity gradient is part of the state);
@@ -97,7 +99,8 @@ def test_phases_bit_exact(maker, steps):
 
 
 @pytest.mark.parametrize("maker,steps", [(small_cavity2d, 12), (small_cavity3d, 4), (small_skewed, 3),
-                                         (small_channel_sphere, 3)])
+                                         (small_channel_sphere, 3), (small_piso_inner, 3), (small_simple_transient, 4),
+                                         (small_outlet_top, 6)])
 def test_steps_match_oracle(maker, steps):
     nodes, spec = maker()
     o = OracleSolver(nodes, spec)
