@@ -238,3 +238,19 @@ def test_gloo_two_ranks_take_the_same_steps_as_two_local_slabs():
     for (rank, _, log, xm, xp), s in zip(got, loc.slabs):
         assert log == s.log, rank              # the same phases, solves and exchanges, in order
         assert np.array_equal(xm, s.mom.owned_x()) and np.array_equal(xp, s.pc.owned_x())
+
+
+def test_mean_projection_only_for_singular_pressure_systems():
+    """All walls: the p' system is singular and each p' solve projects b and x (two sums and two
+    shifts); with a fixed-pressure outlet there is no projection."""
+    from caffe_old_b200 import cases as C
+    proj = {S.SS_SUM_B, S.SS_SUB_B, S.SS_SUM_X, S.SS_SUB_X}
+    for bc, singular in ((C.lid_cavity_bcs("north")[0], True), (("wall",) * 4 + ("outlet", "inlet"), False)):
+        spec = _step_spec("simple").replace(bc=bc)
+        sol = S.SlabSolver(_nodes(), spec, 2, slab_factory=_step_factory())
+        assert sol.singular is singular
+        for s in sol.slabs:
+            s.log.clear()
+        sol.solve()
+        got = [ev[2] for ev in sol.slabs[0].log if ev[0] == "ksp" and ev[1] == 1 and ev[2] in proj]
+        assert got == ([S.SS_SUM_B, S.SS_SUB_B, S.SS_SUM_X, S.SS_SUB_X] if singular else [])
