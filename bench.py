@@ -419,11 +419,18 @@ def run_b200(args, world, rank, local, pg):
         per_row = PCG_BYTES_PER_ROW if method == "pcg" else BICGSTAB_BYTES_PER_ROW
         kname = "cg1_kernel (persistent Jacobi-PCG, FP64)" if method == "pcg" else "bicgstab_kernel (persistent Jacobi-BiCGStab, FP64)"
     achieved = per_row * N * p_iters / (p_ms / 1e3) / 1e9 if (p_ms > 0 and per_row) else None
+    # DRAM traffic from the ncu capture of the pyramid BiCGStab iteration; with the network stage
+    # it describes the iterations after the hand-over, which are most of them
+    traffic_key = "bicgstab" if (method == "fgmres" and spec.kind == "ibpiso") else method
+    traffic_unit = ("bytes per pyramid-stage BiCGStab iteration (the iterations after the network stage hands over; "
+                    "ncu capture, scaled by cells)" if method == "fgmres"
+                    else "bytes per inner iteration (ncu capture, scaled by cells)")
     roofline = {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": hbm, "unit": "GB/s",
                 "frac": (achieved / hbm) if achieved else None,
                 "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
-                "traffic": (LEARNED_TRAFFIC_PER_CELL[method] * N if learned and method in LEARNED_TRAFFIC_PER_CELL else None),
-                "traffic_unit": "bytes per inner iteration (ncu capture, scaled by cells)",
+                "traffic": (LEARNED_TRAFFIC_PER_CELL[traffic_key] * N if learned and traffic_key in LEARNED_TRAFFIC_PER_CELL
+                            else None),
+                "traffic_unit": traffic_unit,
                 "bytes_per_row_iteration": per_row,
                 "network_stage_iterations_per_step": (net_iters / args.steps) if learned else None,
                 "p_solve_ms_per_step": p_ms / args.steps, "iterations_per_step": p_iters / args.steps}
